@@ -1,0 +1,575 @@
+// The extern "C" entry points of include/plfbs.h: context lifetime, device
+// memory, the CUDA-graph time step and the host loop around it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "plfbs.h"
+#include "plfbs_internal.hpp"
+
+using plfbs::DevStats;
+using plfbs::KernelArgs;
+using plfbs::Layout;
+
+struct plfbs_ctx {
+  int device = 0;
+  plfbs_config cfg{};
+  Layout L;
+  int N = 0;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t step_exec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  KernelArgs args{};
+  std::vector<void*> allocs;
+  int64_t bytes = 0;
+  DevStats* stats_host = nullptr;  // pinned copy of the stats header
+  long long stages_done = 0;       // stages run through plfbs_run_stages in the current step
+  bool debug = false;
+  bool have_state = false;
+  std::string err;
+};
+
+namespace {
+
+std::string g_err;  // errors without a context
+
+const char* kVersion = "plfbs-b200 0.1 (sm_100a)";
+
+int set_err(plfbs_ctx* c, int code, const std::string& m) {
+  if (c)
+    c->err = m;
+  else
+    g_err = m;
+  return code;
+}
+
+#define CK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return set_err(ctx, PLFBS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T>
+int dev_upload(plfbs_ctx* ctx, void** dst, const std::vector<T>& src) {
+  const size_t n = std::max<size_t>(src.size(), 1) * sizeof(T);
+  CK(cudaMalloc(dst, n));
+  ctx->allocs.push_back(*dst);
+  ctx->bytes += (int64_t)n;
+  if (!src.empty()) CK(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return PLFBS_OK;
+}
+
+int dev_alloc(plfbs_ctx* ctx, void** dst, size_t n) {
+  n = std::max<size_t>(n, 16);
+  CK(cudaMalloc(dst, n));
+  ctx->allocs.push_back(*dst);
+  ctx->bytes += (int64_t)n;
+  CK(cudaMemset(*dst, 0, n));
+  return PLFBS_OK;
+}
+
+#define TRY(x)                \
+  do {                        \
+    int r_ = (x);             \
+    if (r_ != PLFBS_OK) return r_; \
+  } while (0)
+
+// One time step: IBM, then 4 x (gradient, flux, update) (Solver_gpu.cu:667-833).
+void enqueue_step(const KernelArgs& a, int prec, cudaStream_t s) {
+  plfbs::launch_ibm(a, prec, s);
+  for (int rk = 0; rk < 4; rk++) {
+    plfbs::launch_gradient(a, prec, s);
+    plfbs::launch_flux(a, prec, s);
+    plfbs::launch_update(a, prec, rk, s);
+  }
+}
+
+int capture_step(plfbs_ctx* ctx) {
+  if (ctx->step_exec) {
+    cudaGraphExecDestroy(ctx->step_exec);
+    ctx->step_exec = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  enqueue_step(ctx->args, ctx->cfg.precision, ctx->stream);
+  CK(cudaStreamEndCapture(ctx->stream, &g));
+  cudaError_t e = cudaGraphInstantiate(&ctx->step_exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess)
+    return set_err(ctx, PLFBS_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  return PLFBS_OK;
+}
+
+int reset_force(plfbs_ctx* ctx) {
+  if (!ctx->args.force_x) return PLFBS_OK;
+  const int C = ctx->L.C;
+  std::vector<double> base(C, ctx->cfg.pressure_gradient);
+  CK(cudaMemcpyAsync(ctx->args.force_x, base.data(), C * sizeof(double), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaMemsetAsync(ctx->args.force_y, 0, C * sizeof(double), ctx->stream));
+  CK(cudaMemsetAsync(ctx->args.force_z, 0, C * sizeof(double), ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PLFBS_OK;
+}
+
+int read_stats(plfbs_ctx* ctx) {
+  CK(cudaMemcpyAsync(ctx->stats_host, ctx->args.stats, offsetof(DevStats, history),
+                     cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PLFBS_OK;
+}
+
+int check_ctx(plfbs_ctx* ctx) {
+  if (!ctx) return set_err(nullptr, PLFBS_ERR_ARG, "null context");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess)
+    return set_err(ctx, PLFBS_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  return PLFBS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* plfbs_version(void) { return kVersion; }
+
+const char* plfbs_last_error(const plfbs_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : g_err.c_str();
+}
+
+int plfbs_ls_weights(const plfbs_mesh_view* mesh, int32_t gradient_mode, double* lhs_inv,
+                     double* rhs) {
+  if (!mesh || !lhs_inv || !rhs) return set_err(nullptr, PLFBS_ERR_ARG, "null argument");
+  std::string err;
+  int rc = plfbs::ls_weights(*mesh, gradient_mode, lhs_inv, rhs, err);
+  if (rc) g_err = err;
+  return rc;
+}
+
+int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plfbs_bc_view* bc,
+                 const plfbs_ibm_view* ibm, int device, plfbs_ctx** out) {
+  if (!cfg || !mesh || !bc || !out) return set_err(nullptr, PLFBS_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (cfg->precision != PLFBS_FP64 && cfg->precision != PLFBS_FP32_DEVIATION)
+    return set_err(nullptr, PLFBS_ERR_ARG, "unknown precision mode");
+  if (cfg->precision == PLFBS_FP32_DEVIATION)
+    return set_err(nullptr, PLFBS_ERR_ARG, "the FP32 deviation form is not built in this library");
+  if (!(cfg->time_marching_step > 0) || !(cfg->gamma > 0) || !(cfg->ref_rho > 0) ||
+      !(cfg->max_velocity > 0) || !std::isfinite(cfg->visc))
+    return set_err(nullptr, PLFBS_ERR_ARG,
+                   "config needs time_marching_step, gamma, ref_rho, max_velocity > 0");
+  plfbs_ctx* ctx = new (std::nothrow) plfbs_ctx();
+  if (!ctx) return set_err(nullptr, PLFBS_ERR_ARG, "out of host memory");
+  ctx->device = device;
+  ctx->cfg = *cfg;
+  std::string err;
+  int rc = plfbs::build_layout(*cfg, *mesh, *bc, ctx->L, err);
+  if (rc) {
+    delete ctx;
+    return set_err(nullptr, rc, err);
+  }
+  const Layout& L = ctx->L;
+  const int N = (ibm && ibm->n_nodes > 0) ? ibm->n_nodes : 0;
+  if (N > 0) {
+    if (!ibm->x || !ibm->x_ref || ibm->object_nodes <= 0 || !(cfg->domain_dt > 0) ||
+        !(cfg->lengths[0] > 0) || !(cfg->lengths[1] > 0)) {
+      delete ctx;
+      return set_err(nullptr, PLFBS_ERR_ARG,
+                     "IBM needs node arrays, object_nodes > 0, domain_dt > 0 and lengths > 0");
+    }
+  }
+  // validation and layout need no GPU; the device is checked last
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) {
+    delete ctx;
+    return set_err(nullptr, PLFBS_ERR_NO_DEVICE, "no CUDA device with that index");
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+    delete ctx;
+    return set_err(nullptr, PLFBS_ERR_NO_DEVICE,
+                   "this library is built for sm_100a (B200); device major != 10");
+  }
+  ctx->N = N;
+  auto fail = [&](int code) {
+    std::string m = ctx->err;
+    plfbs_destroy(ctx);
+    g_err = m;
+    return code;
+  };
+  if (cudaSetDevice(device) != cudaSuccess) return fail(set_err(ctx, PLFBS_ERR_CUDA, "cudaSetDevice"));
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
+    return fail(set_err(ctx, PLFBS_ERR_CUDA, "stream/event creation failed"));
+  if (cudaMallocHost(&ctx->stats_host, sizeof(DevStats)) != cudaSuccess)
+    return fail(set_err(ctx, PLFBS_ERR_CUDA, "cudaMallocHost failed"));
+
+  KernelArgs& a = ctx->args;
+  const long long T = (long long)L.C + L.B;
+  a.C = L.C;
+  a.F = L.F;
+  a.B = L.B;
+  a.K = L.K;
+  a.K2 = L.K2;
+  a.quirk_b = L.quirk_b;
+  a.N = N;
+  a.nblk_update = (L.C + plfbs::kBlock - 1) / plfbs::kBlock;
+  a.dt = cfg->time_marching_step;
+  a.pg = 1.0 / cfg->gamma;
+  a.visc3 = cfg->visc * 3;
+  a.pressure_gradient = cfg->pressure_gradient;
+  a.tolerance = cfg->tolerance;
+  a.inv_ref_rho = 1.0 / cfg->ref_rho;
+  a.inv_ref_mom = 1.0 / (cfg->ref_rho * cfg->max_velocity);
+  a.rho0 = cfg->ref_rho;
+  a.uref = cfg->max_velocity;
+  for (int c = 0; c < 3; c++) a.origin[c] = cfg->origin[c];
+
+  void* p = nullptr;
+  if ((rc = dev_alloc(ctx, &p, (size_t)T * 32))) return fail(rc);
+  a.state = p;
+  if ((rc = dev_alloc(ctx, &p, (size_t)L.C * 32))) return fail(rc);
+  a.t0 = p;
+  if ((rc = dev_alloc(ctx, &p, (size_t)L.C * 32))) return fail(rc);
+  a.t1 = p;
+  if ((rc = dev_alloc(ctx, &p, (size_t)L.C * 96))) return fail(rc);
+  a.grad = p;
+  if ((rc = dev_alloc(ctx, &p, (size_t)L.F * 32))) return fail(rc);
+  a.flux = p;
+  if ((rc = dev_upload(ctx, &p, L.face0))) return fail(rc);
+  a.face0 = p;
+  if ((rc = dev_upload(ctx, &p, L.face1))) return fail(rc);
+  a.face1 = p;
+  if ((rc = dev_upload(ctx, &p, L.face2))) return fail(rc);
+  a.face2 = p;
+  if ((rc = dev_upload(ctx, &p, L.bc0))) return fail(rc);
+  a.bc0 = p;
+  if ((rc = dev_upload(ctx, &p, L.bc1))) return fail(rc);
+  a.bc1 = p;
+  if ((rc = dev_upload(ctx, &p, L.bc2))) return fail(rc);
+  a.bc2 = p;
+  if ((rc = dev_upload(ctx, &p, L.bc3))) return fail(rc);
+  a.bc3 = p;
+  if ((rc = dev_upload(ctx, &p, L.st_nbr))) return fail(rc);
+  a.st_nbr = static_cast<const int32_t*>(p);
+  if ((rc = dev_upload(ctx, &p, L.st_wx))) return fail(rc);
+  a.st_wx = p;
+  if ((rc = dev_upload(ctx, &p, L.st_wy))) return fail(rc);
+  a.st_wy = p;
+  if ((rc = dev_upload(ctx, &p, L.st_wz))) return fail(rc);
+  a.st_wz = p;
+  if ((rc = dev_upload(ctx, &p, L.gather))) return fail(rc);
+  a.gather = static_cast<const int32_t*>(p);
+  if ((rc = dev_upload(ctx, &p, L.inv_volume))) return fail(rc);
+  a.inv_volume = p;
+  if ((rc = dev_alloc(ctx, &p, (size_t)a.nblk_update * 4 * sizeof(double)))) return fail(rc);
+  a.partial = static_cast<double*>(p);
+  if ((rc = dev_alloc(ctx, &p, sizeof(DevStats)))) return fail(rc);
+  a.stats = static_cast<DevStats*>(p);
+  a.res_debug = nullptr;
+  a.force_x = a.force_y = a.force_z = nullptr;
+  if (N > 0) {
+    const double dx = cfg->domain_dt * 2;  // Solver_gpu.cu:517
+    a.ibm_dx = dx;
+    a.ibm_inv_dx3 = 1 / dx / dx / dx;
+    a.ibm_xc = (int)(cfg->lengths[0] / dx);
+    a.ibm_yc = (int)(cfg->lengths[1] / dx);
+    a.ibm_area_k = ibm->stiffness * (2 * std::acos(-1.0) * ibm->radius / ibm->object_nodes * ibm->depth);
+    for (double** f : {&a.force_x, &a.force_y, &a.force_z}) {
+      if ((rc = dev_alloc(ctx, &p, (size_t)L.C * sizeof(double)))) return fail(rc);
+      *f = static_cast<double*>(p);
+    }
+    std::vector<double> x(ibm->x, ibm->x + 3 * (size_t)N), xr(ibm->x_ref, ibm->x_ref + 3 * (size_t)N);
+    if ((rc = dev_upload(ctx, &p, x))) return fail(rc);
+    a.node_x = static_cast<double*>(p);
+    if ((rc = dev_upload(ctx, &p, x))) return fail(rc);
+    a.node_x0 = static_cast<double*>(p);
+    if ((rc = dev_upload(ctx, &p, xr))) return fail(rc);
+    a.node_ref = static_cast<const double*>(p);
+    if ((rc = dev_alloc(ctx, &p, 3 * (size_t)N * sizeof(double)))) return fail(rc);
+    a.node_vel = static_cast<double*>(p);
+    if ((rc = dev_alloc(ctx, &p, 3 * (size_t)N * sizeof(double)))) return fail(rc);
+    a.node_force = static_cast<double*>(p);
+    if ((rc = dev_upload(ctx, &p, L.cell_new_of_old))) return fail(rc);
+    a.ibm_map = static_cast<const int32_t*>(p);
+    if ((rc = reset_force(ctx))) return fail(rc);
+  }
+  if ((rc = capture_step(ctx))) return fail(rc);
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(set_err(ctx, PLFBS_ERR_CUDA, "setup failed"));
+  *out = ctx;
+  return PLFBS_OK;
+}
+
+void plfbs_destroy(plfbs_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
+  for (void* p : ctx->allocs) cudaFree(p);
+  if (ctx->stats_host) cudaFreeHost(ctx->stats_host);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int plfbs_set_state(plfbs_ctx* ctx, const double* rho, const double* u, const double* v,
+                    const double* w, int64_t n_total) {
+  TRY(check_ctx(ctx));
+  const Layout& L = ctx->L;
+  const int64_t T = (int64_t)L.C + L.B;
+  if (!rho || !u || !v || !w || n_total != T)
+    return set_err(ctx, PLFBS_ERR_ARG, "set_state needs 4 arrays of n_cells + n_boundary values");
+  std::vector<double> q(4 * (size_t)T);
+  for (int64_t o = 0; o < T; o++) {
+    const int64_t n = o < L.C ? L.cell_new_of_old[o] : L.C + L.bc_new_of_old[o - L.C];
+    q[4 * n] = u[o];
+    q[4 * n + 1] = v[o];
+    q[4 * n + 2] = w[o];
+    q[4 * n + 3] = rho[o];
+  }
+  CK(cudaMemcpyAsync(ctx->args.state, q.data(), q.size() * sizeof(double), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaMemsetAsync(ctx->args.stats, 0, sizeof(DevStats), ctx->stream));
+  plfbs::launch_seed(ctx->args, ctx->cfg.precision, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(reset_force(ctx));
+  ctx->stages_done = 0;
+  ctx->have_state = true;
+  return PLFBS_OK;
+}
+
+int plfbs_run(plfbs_ctx* ctx, int64_t max_steps, plfbs_stats* stats, double* history) {
+  TRY(check_ctx(ctx));
+  if (!ctx->have_state) return set_err(ctx, PLFBS_ERR_STATE, "run before set_state");
+  if (ctx->stages_done != 0)
+    return set_err(ctx, PLFBS_ERR_STATE, "run in the middle of a step (after run_stages)");
+  if (max_steps < 0) return set_err(ctx, PLFBS_ERR_ARG, "negative step count");
+  TRY(read_stats(ctx));
+  const long long start = ctx->stats_host->steps;
+  long long done = 0;
+  float ms_total = 0.f;
+  const long long batch = plfbs::kHistoryCap / 2;
+  bool halt = ctx->stats_host->halt != 0;
+  while (done < max_steps && !halt) {
+    const long long n = std::min<long long>(batch, max_steps - done);
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (long long k = 0; k < n; k++) CK(cudaGraphLaunch(ctx->step_exec, ctx->stream));
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    TRY(read_stats(ctx));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ms_total += ms;
+    const long long now = ctx->stats_host->steps;
+    if (history) {
+      // the batch's records sit in the device ring buffer: at most two spans
+      long long t = start + done;
+      while (t < now) {
+        const long long slot = t % plfbs::kHistoryCap;
+        const long long span = std::min(now - t, (long long)plfbs::kHistoryCap - slot);
+        CK(cudaMemcpyAsync(history + 6 * (t - start), ctx->args.stats->history[slot],
+                           6 * sizeof(double) * span, cudaMemcpyDeviceToHost, ctx->stream));
+        t += span;
+      }
+      CK(cudaStreamSynchronize(ctx->stream));
+    }
+    done = now - start;
+    halt = ctx->stats_host->halt != 0;
+  }
+  CK(cudaGetLastError());
+  if (stats) {
+    const DevStats* s = ctx->stats_host;
+    stats->steps_done = s->steps;
+    stats->converged = s->converged;
+    stats->status = s->diverged ? PLFBS_ERR_DIVERGED : PLFBS_OK;
+    stats->max_error = s->last[1];
+    stats->rho_rms = s->last[2];
+    stats->u_rms = s->last[3];
+    stats->v_rms = s->last[4];
+    stats->w_rms = s->last[5];
+    stats->kernel_ms = ms_total;
+    stats->steps_run = s->steps - start;
+  }
+  if (ctx->stats_host->diverged)
+    return set_err(ctx, PLFBS_ERR_DIVERGED, "residual is NaN or rho exceeded 1000");
+  return PLFBS_OK;
+}
+
+int plfbs_get_state(plfbs_ctx* ctx, double* rho, double* u, double* v, double* w,
+                    int64_t n_total) {
+  TRY(check_ctx(ctx));
+  const Layout& L = ctx->L;
+  const int64_t T = (int64_t)L.C + L.B;
+  if (!rho || !u || !v || !w || n_total != T)
+    return set_err(ctx, PLFBS_ERR_ARG, "get_state needs 4 arrays of n_cells + n_boundary values");
+  std::vector<double> q(4 * (size_t)T);
+  CK(cudaMemcpyAsync(q.data(), ctx->args.state, q.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int64_t o = 0; o < T; o++) {
+    const int64_t n = o < L.C ? L.cell_new_of_old[o] : L.C + L.bc_new_of_old[o - L.C];
+    u[o] = q[4 * n];
+    v[o] = q[4 * n + 1];
+    w[o] = q[4 * n + 2];
+    rho[o] = q[4 * n + 3];
+  }
+  return PLFBS_OK;
+}
+
+int plfbs_get_nodes(plfbs_ctx* ctx, double* x, double* vel, double* force, int32_t n_nodes) {
+  TRY(check_ctx(ctx));
+  if (n_nodes != ctx->N) return set_err(ctx, PLFBS_ERR_ARG, "node count mismatch");
+  if (ctx->N == 0) return PLFBS_OK;
+  const size_t n = 3 * (size_t)ctx->N * sizeof(double);
+  if (x) CK(cudaMemcpyAsync(x, ctx->args.node_x, n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (vel) CK(cudaMemcpyAsync(vel, ctx->args.node_vel, n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (force) CK(cudaMemcpyAsync(force, ctx->args.node_force, n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PLFBS_OK;
+}
+
+int plfbs_get_body_force(plfbs_ctx* ctx, double frontal_area, double* cd, double* cl) {
+  TRY(check_ctx(ctx));
+  if (ctx->N == 0) return set_err(ctx, PLFBS_ERR_STATE, "no immersed body");
+  if (!(frontal_area > 0) || !cd || !cl) return set_err(ctx, PLFBS_ERR_ARG, "bad argument");
+  std::vector<double> f(3 * (size_t)ctx->N);
+  CK(cudaMemcpyAsync(f.data(), ctx->args.node_force, f.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  double sx = 0.0, sy = 0.0;
+  for (int n = 0; n < ctx->N; n++) {
+    sx += f[3 * n];
+    sy += f[3 * n + 1];
+  }
+  const double q = 0.5 * ctx->cfg.ref_rho * ctx->cfg.max_velocity * ctx->cfg.max_velocity * frontal_area;
+  *cd = -sx / q;
+  *cl = -sy / q;
+  return PLFBS_OK;
+}
+
+int plfbs_set_debug(plfbs_ctx* ctx, int enable) {
+  TRY(check_ctx(ctx));
+  if ((enable != 0) == ctx->debug) return PLFBS_OK;
+  if (enable) {
+    void* p = nullptr;
+    TRY(dev_alloc(ctx, &p, (size_t)ctx->L.C * 32));
+    ctx->args.res_debug = p;
+  } else {
+    ctx->args.res_debug = nullptr;
+  }
+  ctx->debug = enable != 0;
+  return capture_step(ctx);
+}
+
+int plfbs_run_stages(plfbs_ctx* ctx, int64_t n_stages) {
+  TRY(check_ctx(ctx));
+  if (!ctx->have_state) return set_err(ctx, PLFBS_ERR_STATE, "run_stages before set_state");
+  for (int64_t g = 0; g < n_stages; g++) {
+    const int rk = (int)(ctx->stages_done % 4);
+    if (rk == 0) plfbs::launch_ibm(ctx->args, ctx->cfg.precision, ctx->stream);
+    plfbs::launch_gradient(ctx->args, ctx->cfg.precision, ctx->stream);
+    plfbs::launch_flux(ctx->args, ctx->cfg.precision, ctx->stream);
+    plfbs::launch_update(ctx->args, ctx->cfg.precision, rk, ctx->stream);
+    CK(cudaGetLastError());
+    ctx->stages_done = (ctx->stages_done + 1) % 4;
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PLFBS_OK;
+}
+
+int plfbs_get_gradients(plfbs_ctx* ctx, double* grad, int32_t n_cells) {
+  TRY(check_ctx(ctx));
+  const Layout& L = ctx->L;
+  if (!grad || n_cells != L.C) return set_err(ctx, PLFBS_ERR_ARG, "gradients: need 12 n_cells");
+  std::vector<double> g(12 * (size_t)L.C);
+  CK(cudaMemcpyAsync(g.data(), ctx->args.grad, g.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int o = 0; o < L.C; o++)
+    std::memcpy(grad + 12 * (size_t)o, &g[12 * (size_t)L.cell_new_of_old[o]], 12 * sizeof(double));
+  return PLFBS_OK;
+}
+
+int plfbs_get_face_flux(plfbs_ctx* ctx, double* flux, int32_t n_faces) {
+  TRY(check_ctx(ctx));
+  const Layout& L = ctx->L;
+  if (!flux || n_faces != L.F) return set_err(ctx, PLFBS_ERR_ARG, "face flux: need 4 n_faces");
+  std::vector<double> g(4 * (size_t)L.F);
+  CK(cudaMemcpyAsync(g.data(), ctx->args.flux, g.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int f = 0; f < L.F; f++)
+    std::memcpy(flux + 4 * (size_t)f, &g[4 * (size_t)L.face_new_of_old[f]], 4 * sizeof(double));
+  return PLFBS_OK;
+}
+
+int plfbs_get_residual(plfbs_ctx* ctx, double* res, int32_t n_cells) {
+  TRY(check_ctx(ctx));
+  const Layout& L = ctx->L;
+  if (!ctx->args.res_debug) return set_err(ctx, PLFBS_ERR_STATE, "enable plfbs_set_debug first");
+  if (!res || n_cells != L.C) return set_err(ctx, PLFBS_ERR_ARG, "residual: need 4 n_cells");
+  std::vector<double> g(4 * (size_t)L.C);
+  CK(cudaMemcpyAsync(g.data(), ctx->args.res_debug, g.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int o = 0; o < L.C; o++)
+    std::memcpy(res + 4 * (size_t)o, &g[4 * (size_t)L.cell_new_of_old[o]], 4 * sizeof(double));
+  return PLFBS_OK;
+}
+
+int plfbs_profile_steps(plfbs_ctx* ctx, int64_t n_steps, double* ms) {
+  TRY(check_ctx(ctx));
+  if (!ms) return set_err(ctx, PLFBS_ERR_ARG, "null output");
+  if (!ctx->have_state || ctx->stages_done != 0)
+    return set_err(ctx, PLFBS_ERR_STATE, "profile needs a state at a step boundary");
+  for (int k = 0; k < 4; k++) ms[k] = 0.0;
+  cudaEvent_t ev[13];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  const KernelArgs& a = ctx->args;
+  const int prec = ctx->cfg.precision;
+  for (int64_t t = 0; t < n_steps; t++) {
+    CK(cudaEventRecord(ev[0], ctx->stream));
+    plfbs::launch_ibm(a, prec, ctx->stream);
+    CK(cudaEventRecord(ev[1], ctx->stream));
+    for (int rk = 0; rk < 4; rk++) {
+      plfbs::launch_gradient(a, prec, ctx->stream);
+      CK(cudaEventRecord(ev[2 + 3 * rk], ctx->stream));
+      plfbs::launch_flux(a, prec, ctx->stream);
+      CK(cudaEventRecord(ev[3 + 3 * rk], ctx->stream));
+      plfbs::launch_update(a, prec, rk, ctx->stream);
+      CK(cudaEventRecord(ev[4 + 3 * rk], ctx->stream));
+    }
+    CK(cudaEventSynchronize(ev[12]));
+    float x = 0.f;
+    CK(cudaEventElapsedTime(&x, ev[0], ev[1]));
+    ms[0] += x;
+    for (int rk = 0; rk < 4; rk++) {
+      cudaEvent_t prev = ev[1 + 3 * rk];
+      CK(cudaEventElapsedTime(&x, prev, ev[2 + 3 * rk]));
+      ms[1] += x;
+      CK(cudaEventElapsedTime(&x, ev[2 + 3 * rk], ev[3 + 3 * rk]));
+      ms[2] += x;
+      CK(cudaEventElapsedTime(&x, ev[3 + 3 * rk], ev[4 + 3 * rk]));
+      ms[3] += x;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  CK(cudaGetLastError());
+  return PLFBS_OK;
+}
+
+int plfbs_memory_bytes(plfbs_ctx* ctx, int64_t* bytes) {
+  if (!ctx || !bytes) return set_err(ctx, PLFBS_ERR_ARG, "null argument");
+  *bytes = ctx->bytes;
+  return PLFBS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,581 @@
+// sm_100a kernels of the LBFS explicit time step (FP64 path).
+//
+// One RK stage is three kernels, and a time step is the IBM kernel plus four
+// stages, all captured in one CUDA graph by capi.cpp:
+//
+//   gradient  (thread per cell)  ghost states inline + least-squares gradient
+//                                 [get_interior_gradients, update_unstructured_bcs]
+//   flux      (thread per face)  D3Q15 reconstruction + interface equilibrium
+//                                 + relaxed moment flux, written per face
+//                                 [calc_face_flux, get_bc_gradients]
+//   update    (thread per cell)  face->cell gather (no atomics) + body force +
+//                                 RK stage; last stage also reduces residuals
+//                                 and tests convergence on the device
+//                                 [add, time_integration, square/total<256>,
+//                                  l2_norm_rms_moukallad]
+//   ibm       (thread per node)  interpolation, advection, spring force and
+//                                 spreading with warp-aggregated atomics
+//
+// All of them are bandwidth kernels (no dense contraction: tensor cores do not
+// apply). Memory per cell is laid out for coalesced 32-byte accesses.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "plfbs_internal.hpp"
+
+namespace plfbs {
+namespace {
+
+struct __align__(32) d4 {
+  double x, y, z, w;
+};
+
+__device__ __forceinline__ d4 ld4(const void* base, long long i) {
+  const double2* p = reinterpret_cast<const double2*>(base) + 2 * i;
+  double2 a = __ldg(p), b = __ldg(p + 1);
+  return d4{a.x, a.y, b.x, b.y};
+}
+// Plain (coherent) load, for data the same kernel also writes.
+__device__ __forceinline__ d4 ld4rw(const void* base, long long i) {
+  const double2* p = reinterpret_cast<const double2*>(base) + 2 * i;
+  double2 a = p[0], b = p[1];
+  return d4{a.x, a.y, b.x, b.y};
+}
+__device__ __forceinline__ void st4(void* base, long long i, const d4& v) {
+  double2* p = reinterpret_cast<double2*>(base) + 2 * i;
+  p[0] = make_double2(v.x, v.y);
+  p[1] = make_double2(v.z, v.w);
+}
+
+__device__ __forceinline__ bool halted(const KernelArgs& a) {
+  return *(volatile const int*)&a.stats->halt != 0;
+}
+
+// Ghost state from its owner (update_unstructured_bcs, LBFS.cu:1228-1301).
+// bc1 holds the Dirichlet target: the raw value, or for the parabolic inlet
+// (vel type 9) the profile 16 u (H/2+y)(H/2-y)(H/2+z)(H/2-z)/H^4 in x.
+__device__ __forceinline__ d4 ghost_state(const d4& q, const d4& tgt, int types) {
+  const int rt = types & 0xff, vt = types >> 8;
+  d4 g;
+  g.w = (rt == 1) ? tgt.w - (q.w - tgt.w) : q.w;
+  if (vt == 2) {
+    g.x = q.x;
+    g.y = q.y;
+    g.z = q.z;
+  } else {
+    g.x = tgt.x - (q.x - tgt.x);
+    g.y = tgt.y - (q.y - tgt.y);
+    g.z = tgt.z - (q.z - tgt.z);
+  }
+  return g;
+}
+
+// ---------------------------------------------------------------------------
+// gradient: grad_i = sum_e G_e (q_e - q_i), G_e = LHS_i^-1 RHS_e precombined.
+// Gradient layout: 3 x d4 per cell = (rx, ry, rz, ux), (uy, uz, vx, vy),
+// (vz, wx, wy, wz).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_gradient(const KernelArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.C || halted(a)) return;
+  const d4 qi = ld4(a.state, i);
+  double g[12];
+#pragma unroll
+  for (int k = 0; k < 12; k++) g[k] = 0.0;
+  const double* wx = static_cast<const double*>(a.st_wx);
+  const double* wy = static_cast<const double*>(a.st_wy);
+  const double* wz = static_cast<const double*>(a.st_wz);
+  for (int k = 0; k < a.K; k++) {
+    const long long s = (long long)k * a.C + i;
+    const int j = __ldg(a.st_nbr + s);
+    if (j < 0) break;
+    d4 qj;
+    if (j < a.C) {
+      qj = ld4(a.state, j);
+    } else {
+      const int b = j - a.C;
+      const d4 tgt = ld4(a.bc1, b);
+      const int types = (int)__ldg(reinterpret_cast<const double*>(a.bc3) + 4LL * b + 3);
+      qj = ghost_state(qi, tgt, types);
+      st4(a.state, j, qj);  // ghost states are read back by get_state
+    }
+    const double w[3] = {__ldg(wx + s), __ldg(wy + s), __ldg(wz + s)};
+    const double d[4] = {qj.w - qi.w, qj.x - qi.x, qj.y - qi.y, qj.z - qi.z};
+#pragma unroll
+    for (int f = 0; f < 4; f++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) g[3 * f + c] = fma(w[c], d[f], g[3 * f + c]);
+  }
+  st4(a.grad, 3LL * i + 0, d4{g[0], g[1], g[2], g[3]});
+  st4(a.grad, 3LL * i + 1, d4{g[4], g[5], g[6], g[7]});
+  st4(a.grad, 3LL * i + 2, d4{g[8], g[9], g[10], g[11]});
+}
+
+// ---------------------------------------------------------------------------
+// flux
+// ---------------------------------------------------------------------------
+// Gradients as 12 doubles: rho, u, v, w, each (x, y, z).
+__device__ __forceinline__ void load_grad(const void* base, int c, double g[12]) {
+  const d4 a0 = ld4(base, 3LL * c), a1 = ld4(base, 3LL * c + 1), a2 = ld4(base, 3LL * c + 2);
+  g[0] = a0.x; g[1] = a0.y; g[2] = a0.z; g[3] = a0.w;
+  g[4] = a1.x; g[5] = a1.y; g[6] = a1.z; g[7] = a1.w;
+  g[8] = a2.x; g[9] = a2.y; g[10] = a2.z; g[11] = a2.w;
+}
+
+// Ghost gradient (get_bc_gradients, LBFS.cu:1306-1416): Dirichlet
+// 2 (bc - q_owner) / |d| * d_hat from the raw boundary value; Neumann the
+// owner's gradient times (1 - |n|) componentwise.
+__device__ __forceinline__ void ghost_grad(const d4& q, const double go[12], const d4& bv,
+                                           const d4& dd, const d4& nm, int types,
+                                           double g[12]) {
+  const int rt = types & 0xff, vt = types >> 8;
+  const double dir[3] = {dd.x, dd.y, dd.z}, m[3] = {nm.x, nm.y, nm.z};
+  const double dq[4] = {2 * (bv.w - q.w), 2 * (bv.x - q.x), 2 * (bv.y - q.y), 2 * (bv.z - q.z)};
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    const bool dirichlet = (f == 0) ? (rt == 1) : (vt != 2);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      g[3 * f + c] = dirichlet ? dq[f] / dd.w * dir[c] : go[3 * f + c] * m[c];
+  }
+}
+
+template <int EX, int EY, int EZ>
+__device__ __forceinline__ double edot(const double* g) {
+  // e . g for a lattice direction with components in {-1, 0, 1}
+  double s = 0.0;
+  if (EX) s = EX > 0 ? g[0] : -g[0];
+  if (EY) s = EY > 0 ? s + g[1] : s - g[1];
+  if (EZ) s = EZ > 0 ? s + g[2] : s - g[2];
+  return s;
+}
+
+// One opposite pair (k, k') of D3Q15 lattice nodes, e_k' = -e_k = -e, node k
+// at x_f - e dt_s (populate_lattice_macros, LBFS.cu:330-938). With s = e . n:
+// s > d1 takes node k from the owner side and k' from the neighbour side,
+// s < -d1 the reverse, otherwise both from the face average with averaged
+// gradients (the +-0.001 dt dead band, LBFS.cu:353-354). Their equilibria
+// (populate_feq, LBFS.cu:942-1038) are accumulated into the moments
+// rho_I, m = sum e f and P = sum e e^T f (xx, yy, zz, xy, xz, yz).
+template <int EX, int EY, int EZ>
+__device__ __forceinline__ void lattice_pair(const double si[4], const double sn[4],
+                                             const double sc[4], const double g1[12],
+                                             const double g2[12], const double n[3], double d1,
+                                             double dt, double pg, double wgt, double& rhoI,
+                                             double m[3], double P[6]) {
+  const double s = (EX ? (EX > 0 ? n[0] : -n[0]) : 0.0) + (EY ? (EY > 0 ? n[1] : -n[1]) : 0.0) +
+                   (EZ ? (EZ > 0 ? n[2] : -n[2]) : 0.0);
+  const int mode = s > d1 ? 1 : (s < -d1 ? 2 : 0);
+  double qa[4], qb[4];
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    const double e1 = edot<EX, EY, EZ>(g1 + 3 * f), e2 = edot<EX, EY, EZ>(g2 + 3 * f);
+    double ba, bb, ea, eb;
+    if (mode == 1) {
+      ba = si[f]; bb = sn[f]; ea = e1; eb = e2;
+    } else if (mode == 2) {
+      ba = sn[f]; bb = si[f]; ea = e2; eb = e1;
+    } else {
+      ba = sc[f]; bb = sc[f]; ea = (e1 + e2) * 0.5; eb = ea;
+    }
+    qa[f] = fma(-ea, dt, ba);
+    qb[f] = fma(eb, dt, bb);
+  }
+  // w rho (1 + 3 e.u + 4.5 (e.u)^2 / gamma - 1.5 u^2 / gamma)
+  const double eua = edot<EX, EY, EZ>(qa + 1), eub = -edot<EX, EY, EZ>(qb + 1);
+  const double u2a = (qa[1] * qa[1] + qa[2] * qa[2] + qa[3] * qa[3]) * pg;
+  const double u2b = (qb[1] * qb[1] + qb[2] * qb[2] + qb[3] * qb[3]) * pg;
+  const double fa = wgt * qa[0] * (1.0 + 3.0 * eua + 4.5 * eua * eua * pg - 1.5 * u2a);
+  const double fb = wgt * qb[0] * (1.0 + 3.0 * eub + 4.5 * eub * eub * pg - 1.5 * u2b);
+  const double sum = fa + fb, dif = fa - fb;
+  rhoI += sum;
+  if (EX) m[0] += EX > 0 ? dif : -dif;
+  if (EY) m[1] += EY > 0 ? dif : -dif;
+  if (EZ) m[2] += EZ > 0 ? dif : -dif;
+  if (EX) P[0] += sum;
+  if (EY) P[1] += sum;
+  if (EZ) P[2] += sum;
+  if (EX && EY) P[3] += (EX * EY > 0) ? sum : -sum;
+  if (EX && EZ) P[4] += (EX * EZ > 0) ? sum : -sum;
+  if (EY && EZ) P[5] += (EY * EZ > 0) ? sum : -sum;
+}
+
+// Flux of one face (calc_face_flux, LBFS.cu:1592-1710 and
+// calculate_flux_at_interface, LBFS.cu:1042-1223), in closed form:
+//   rho_I = sum_k feq_k(lattice), m = sum_k e_k feq_k(lattice), u_I = m / rho_I
+//   f_k = feq_k(rho_I, u_I) - tau (feq_k(rho_I, u_I) - feq_k(lattice)),
+//   tau = 3 nu / (dt_s gamma)
+// whose moments are, exactly (D3Q15 equilibrium moments are isotropic):
+//   sum e f = m
+//   sum e e^T f = (1 - tau) (rho_I / 3 I + m m^T / (rho_I gamma)) + tau P_lattice
+// The face flux is (momentum, mass) = ((sum e e^T f) n, (sum e f) . n) A.
+// A boundary face (neighbour > n_cells in the reference) takes both sides from
+// the boundary value and all gradients from the ghost (LBFS.cu:356-401).
+__global__ void __launch_bounds__(kBlock) k_flux(const KernelArgs a) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= a.F || halted(a)) return;
+  const d4 f0 = ld4(a.face0, f), f1 = ld4(a.face1, f), f2 = ld4(a.face2, f);
+  uint64_t ids;
+  memcpy(&ids, &f2.w, sizeof ids);
+  const int o = (int)(uint32_t)(ids & 0xffffffffu), nb = (int)(uint32_t)(ids >> 32);
+  const double n[3] = {f0.x, f0.y, f0.z};
+  const double area = f0.w, dt = f1.x;
+  const double t1[3] = {f1.y, f1.z, f1.w}, t2[3] = {f2.x, f2.y, f2.z};
+
+  const d4 qo = ld4(a.state, o);
+  double g1[12], g2[12], si[4], sn[4], sc[4];
+  load_grad(a.grad, o, g1);
+  const double qov[4] = {qo.w, qo.x, qo.y, qo.z};
+  bool interior = true;
+  d4 qn;
+  if (nb < a.C) {
+    qn = ld4(a.state, nb);
+    load_grad(a.grad, nb, g2);
+  } else {
+    const int b = nb - a.C;
+    const d4 bv = ld4(a.bc0, b), tgt = ld4(a.bc1, b), dd = ld4(a.bc2, b), nm = ld4(a.bc3, b);
+    const int types = (int)nm.w;
+    ghost_grad(qo, g1, bv, dd, nm, types, g2);
+    if (b == a.quirk_b) {
+      // The reference tests neighbour > n_cells (LBFS.cu:356), so its first
+      // ghost (index n_cells) goes through the interior branch with the ghost
+      // state and gradient as the neighbour's.
+      qn = ghost_state(qo, tgt, types);
+    } else {
+      interior = false;
+      const int rt = types & 0xff, vt = types >> 8;
+      const double bvv[4] = {bv.w, bv.x, bv.y, bv.z};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const bool dirichlet = (k == 0) ? (rt == 1) : (vt != 2);
+        sc[k] = dirichlet ? bvv[k]
+                          : qov[k] - (t1[0] * g2[3 * k] + t1[1] * g2[3 * k + 1] +
+                                      t1[2] * g2[3 * k + 2]);
+        si[k] = sc[k];
+        sn[k] = sc[k];
+      }
+#pragma unroll
+      for (int k = 0; k < 12; k++) g1[k] = g2[k];
+    }
+  }
+  if (interior) {
+    const double qnv[4] = {qn.w, qn.x, qn.y, qn.z};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      si[k] = qov[k] - (t1[0] * g1[3 * k] + t1[1] * g1[3 * k + 1] + t1[2] * g1[3 * k + 2]);
+      sn[k] = qnv[k] - (t2[0] * g2[3 * k] + t2[1] * g2[3 * k + 1] + t2[2] * g2[3 * k + 2]);
+      sc[k] = (si[k] + sn[k]) * 0.5;
+    }
+  }
+
+  const double pg = a.pg, d1 = 0.001 * dt;
+  const double w0 = 2.0 / 9.0, w1 = 1.0 / 9.0, w7 = 1.0 / 72.0;
+  // centre node (k = 0): e = 0
+  const double u2c = (sc[1] * sc[1] + sc[2] * sc[2] + sc[3] * sc[3]) * pg;
+  double rhoI = w0 * sc[0] * (1.0 - 1.5 * u2c);
+  double m[3] = {0.0, 0.0, 0.0};
+  double P[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  lattice_pair<1, 0, 0>(si, sn, sc, g1, g2, n, d1, dt, pg, w1, rhoI, m, P);
+  lattice_pair<0, 1, 0>(si, sn, sc, g1, g2, n, d1, dt, pg, w1, rhoI, m, P);
+  lattice_pair<0, 0, 1>(si, sn, sc, g1, g2, n, d1, dt, pg, w1, rhoI, m, P);
+  lattice_pair<1, 1, 1>(si, sn, sc, g1, g2, n, d1, dt, pg, w7, rhoI, m, P);
+  lattice_pair<1, 1, -1>(si, sn, sc, g1, g2, n, d1, dt, pg, w7, rhoI, m, P);
+  lattice_pair<1, -1, 1>(si, sn, sc, g1, g2, n, d1, dt, pg, w7, rhoI, m, P);
+  lattice_pair<-1, 1, 1>(si, sn, sc, g1, g2, n, d1, dt, pg, w7, rhoI, m, P);
+
+  const double tau = a.visc3 / dt * pg;
+  const double mn = m[0] * n[0] + m[1] * n[1] + m[2] * n[2];
+  const double Pn[3] = {P[0] * n[0] + P[3] * n[1] + P[4] * n[2],
+                        P[3] * n[0] + P[1] * n[1] + P[5] * n[2],
+                        P[4] * n[0] + P[5] * n[1] + P[2] * n[2]};
+  const double p3 = rhoI * (1.0 / 3.0);
+  const double mnr = mn / rhoI * pg;
+  d4 out;
+  out.x = ((1.0 - tau) * fma(m[0], mnr, p3 * n[0]) + tau * Pn[0]) * area;
+  out.y = ((1.0 - tau) * fma(m[1], mnr, p3 * n[1]) + tau * Pn[1]) * area;
+  out.z = ((1.0 - tau) * fma(m[2], mnr, p3 * n[2]) + tau * Pn[2]) * area;
+  out.w = mn * area;
+  st4(a.flux, f, out);
+}
+
+// ---------------------------------------------------------------------------
+// update: gather + body force + RK stage (time_integration, LBFS.cu:1457-1521)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int RK>
+__global__ void __launch_bounds__(kBlock) k_update(const KernelArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (halted(a)) return;  // uniform across the launch
+  constexpr double alpha = (RK == 0 || RK == 3) ? 1.0 : 0.5;
+  constexpr double beta = (RK == 0 || RK == 3) ? (1.0 / 6.0) : (1.0 / 3.0);
+  double sq[4] = {0.0, 0.0, 0.0, 0.0};
+  bool bad = false;
+  if (i < a.C) {
+    double r[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < a.K2; k++) {
+      const int e = __ldg(a.gather + (long long)k * a.C + i);
+      if (e < 0) break;
+      const d4 fl = ld4(a.flux, e >> 1);
+      if (e & 1) {
+        r[0] += fl.x; r[1] += fl.y; r[2] += fl.z; r[3] += fl.w;
+      } else {
+        r[0] -= fl.x; r[1] -= fl.y; r[2] -= fl.z; r[3] -= fl.w;
+      }
+    }
+    const double iv = __ldg(static_cast<const double*>(a.inv_volume) + i);
+    double R[4] = {r[0] * iv, r[1] * iv, r[2] * iv, r[3] * iv};  // u, v, w, rho
+    if (a.force_x) {
+      R[0] += a.force_x[i];
+      R[1] += a.force_y[i];
+      R[2] += a.force_z[i];
+      if (RK == 3) {  // the last reader of this step's force: reset for the IBM
+        a.force_x[i] = a.pressure_gradient;
+        a.force_y[i] = 0.0;
+        a.force_z[i] = 0.0;
+      }
+    } else {
+      R[0] += a.pressure_gradient;
+    }
+    if (a.res_debug) st4(a.res_debug, i, d4{R[0], R[1], R[2], R[3]});
+    const d4 t0 = ld4rw(a.t0, i);
+    d4 t1 = ld4rw(a.t1, i);
+    const double dt = a.dt;
+    double f1 = t0.w + R[3] * dt * alpha;
+    double f2 = t0.x + R[0] * dt * alpha;
+    double f3 = t0.y + R[1] * dt * alpha;
+    double f4 = t0.z + R[2] * dt * alpha;
+    t1.w = t1.w + dt * beta * R[3];
+    t1.x = t1.x + dt * beta * R[0];
+    t1.y = t1.y + dt * beta * R[1];
+    t1.z = t1.z + dt * beta * R[2];
+    d4 q;
+    if (RK == 3) {
+      q = d4{t1.x / t1.w, t1.y / t1.w, t1.z / t1.w, t1.w};
+      st4(a.t0, i, t1);  // the next step starts from t1 (Solver_gpu.cu:671)
+      sq[0] = R[3] * R[3];
+      sq[1] = R[0] * R[0];
+      sq[2] = R[1] * R[1];
+      sq[3] = R[2] * R[2];
+      bad = !(t1.w <= 1000.0);  // the CPU solver's divergence test, Solver.cpp:448-493
+    } else {
+      q = d4{f2 / f1, f3 / f1, f4 / f1, f1};
+    }
+    st4(a.t1, i, t1);
+    st4(a.state, i, q);
+  }
+  if (RK != 3) return;
+
+  // Residual reduction: warp shuffle, block, then the last block to finish
+  // sums the per-block partials in block order (deterministic), forms the
+  // rms norms and tests convergence.
+  __shared__ double red[kBlock / 32][4];
+  __shared__ int any_bad;
+  __shared__ bool last;
+  if (threadIdx.x == 0) any_bad = 0;
+  __syncthreads();
+  if (bad) atomicOr(&any_bad, 1);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const double v = warp_sum(sq[c]);
+    if (lane == 0) red[warp][c] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double v = 0.0;
+    for (int w = 0; w < kBlock / 32; w++) v += red[w][threadIdx.x];
+    a.partial[4LL * blockIdx.x + threadIdx.x] = v;
+  }
+  if (threadIdx.x == 0 && any_bad) atomicExch(&a.stats->diverged, 1);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int done = atomicAdd(&a.stats->block_counter, 1u);
+    last = (done == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // final pass: thread c < 4 sums component c over the blocks
+  __shared__ double tot[4];
+  if (threadIdx.x < 4) {
+    const volatile double* p = a.partial;
+    double v = 0.0;
+    for (int b = 0; b < (int)gridDim.x; b++) v += p[4LL * b + threadIdx.x];
+    tot[threadIdx.x] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    DevStats* st = a.stats;
+    const double nC = (double)a.C;
+    const double rho_rms = sqrt(tot[0] / nC) * a.inv_ref_rho;
+    const double u_rms = sqrt(tot[1] / nC) * a.inv_ref_mom;
+    const double v_rms = sqrt(tot[2] / nC) * a.inv_ref_mom;
+    const double w_rms = sqrt(tot[3] / nC) * a.inv_ref_mom;
+    const double me = fmax(fmax(w_rms, u_rms), v_rms);  // residuals::max_error
+    const long long t = st->steps;
+    double* h = st->history[t % kHistoryCap];
+    h[0] = (double)t;
+    h[1] = me;
+    h[2] = rho_rms;
+    h[3] = u_rms;
+    h[4] = v_rms;
+    h[5] = w_rms;
+    for (int c = 0; c < 6; c++) st->last[c] = h[c];
+    st->steps = t + 1;
+    st->block_counter = 0;
+    const bool nan = !(me == me) || !(rho_rms == rho_rms);
+    if (nan) st->diverged = 1;
+    if (me < a.tolerance) {
+      st->converged = 1;
+      st->converged_step = t;
+    }
+    if (st->converged || st->diverged) st->halt = 1;
+  }
+}
+
+// Seeds the RK accumulator from the state (Solver_gpu.cu:664): t0 = t1 = q.
+__global__ void k_seed(const KernelArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.C) return;
+  const d4 q = ld4(a.state, i);
+  st4(a.t0, i, q);
+  st4(a.t1, i, q);
+}
+
+// ---------------------------------------------------------------------------
+// IBM (immersed_boundary_method.cu:13-90, 161-190, 244-295, 299-375), one
+// thread per node, once per time step before the RK stages.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void stencil_origin(const KernelArgs& a, const double x[3],
+                                               double r[3], int lo[3]) {
+  r[0] = (x[0] - a.origin[0]) / a.ibm_dx;
+  r[1] = fabs((x[1] - a.origin[1]) / a.ibm_dx);
+  r[2] = fabs((x[2] - a.origin[2]) / a.ibm_dx);
+#pragma unroll
+  for (int c = 0; c < 3; c++) lo[c] = (int)round(r[c]) - 1;
+}
+
+__global__ void __launch_bounds__(128) k_ibm(const KernelArgs a) {
+  const int nd = blockIdx.x * blockDim.x + threadIdx.x;
+  if (halted(a)) return;
+  const bool active = nd < a.N;
+  const int xc = a.ibm_xc, yc = a.ibm_yc;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  double r[3];
+  int lo[3];
+  if (active) {
+    double x[3] = {a.node_x[3 * nd], a.node_x[3 * nd + 1], a.node_x[3 * nd + 2]};
+    stencil_origin(a, x, r, lo);
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int ii = lo[0]; ii <= lo[0] + 1; ii++)
+      for (int jj = lo[1]; jj <= lo[1] + 1; jj++)
+        for (int kk = lo[2]; kk <= lo[2] + 1; kk++) {
+          const long long cell = (long long)ii + (long long)jj * xc + (long long)kk * yc * xc;
+          if (cell < a.C && cell >= 0) {
+            const double wx = 1 - fabs(ii + 0.5 - r[0]);
+            const double wy = 1 - fabs(jj + 0.5 - r[1]);
+            const double wz = 1 - fabs(kk + 0.5 - r[2]);
+            const d4 q = ld4(a.state, a.ibm_map[cell]);
+            v[0] += q.x * wx * wy * wz * a.ibm_inv_dx3;
+            v[1] += q.y * wx * wy * wz * a.ibm_inv_dx3;
+            v[2] += q.z * wx * wy * wz * a.ibm_inv_dx3;
+          }
+        }
+    for (int c = 0; c < 3; c++) {
+      x[c] = a.node_x0[3 * nd + c] + v[c] * a.dt;
+      a.node_x[3 * nd + c] = x[c];
+      a.node_x0[3 * nd + c] = x[c];
+      a.node_vel[3 * nd + c] = v[c];
+    }
+    fx = (-a.ibm_area_k * (x[0] - a.node_ref[3 * nd]));
+    fy = (-a.ibm_area_k * (x[1] - a.node_ref[3 * nd + 1]));
+    fz = (-a.ibm_area_k * (x[2] - a.node_ref[3 * nd + 2]));
+    a.node_force[3 * nd] = fx;
+    a.node_force[3 * nd + 1] = fy;
+    a.node_force[3 * nd + 2] = fz;
+    stencil_origin(a, x, r, lo);
+  }
+  // Spreading: for each of the 8 stencil slots the lanes whose targets
+  // coincide are grouped with __match_any_sync and their contributions are
+  // summed in-warp, so one atomic per distinct cell per slot reaches memory.
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+#pragma unroll 1
+  for (int s = 0; s < 8; s++) {
+    const int ii = active ? lo[0] + (s & 1) : 0;
+    const int jj = active ? lo[1] + ((s >> 1) & 1) : 0;
+    const int kk = active ? lo[2] + (s >> 2) : 0;
+    long long cell = (long long)ii + (long long)jj * xc + (long long)kk * yc * xc;
+    const bool hit = active && cell < a.C && cell >= 0;
+    double vx = 0.0, vy = 0.0, vz = 0.0;
+    if (hit) {
+      const double wx = 1 - fabs(ii + 0.5 - r[0]);
+      const double wy = 1 - fabs(jj + 0.5 - r[1]);
+      const double wz = 1 - fabs(kk + 0.5 - r[2]);
+      vx = fx * wx * wy * wz * a.ibm_inv_dx3;
+      vy = fy * wx * wy * wz * a.ibm_inv_dx3;
+      vz = fz * wx * wy * wz * a.ibm_inv_dx3;
+    }
+    const long long key = hit ? cell : -1;
+    const unsigned peers = __match_any_sync(full, key);
+    const int leader = __ffs(peers) - 1;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    // group sum by shuffles: each lane adds its peers' values in lane order
+    for (int src = 0; src < 32; src++) {
+      const double ox = __shfl_sync(full, vx, src);
+      const double oy = __shfl_sync(full, vy, src);
+      const double oz = __shfl_sync(full, vz, src);
+      if ((peers >> src) & 1u) {
+        sx += ox;
+        sy += oy;
+        sz += oz;
+      }
+    }
+    if (hit && lane == leader) {
+      const int c = a.ibm_map[cell];
+      atomicAdd(a.force_x + c, sx);
+      atomicAdd(a.force_y + c, sy);
+      atomicAdd(a.force_z + c, sz);
+    }
+  }
+}
+
+inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
+
+}  // namespace
+
+void launch_gradient(const KernelArgs& a, int precision, cudaStream_t s) {
+  (void)precision;
+  k_gradient<<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
+}
+void launch_flux(const KernelArgs& a, int precision, cudaStream_t s) {
+  (void)precision;
+  k_flux<<<blocks_for(a.F, kBlock), kBlock, 0, s>>>(a);
+}
+void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t s) {
+  (void)precision;
+  const int nb = blocks_for(a.C, kBlock);
+  switch (rk) {
+    case 0: k_update<0><<<nb, kBlock, 0, s>>>(a); break;
+    case 1: k_update<1><<<nb, kBlock, 0, s>>>(a); break;
+    case 2: k_update<2><<<nb, kBlock, 0, s>>>(a); break;
+    default: k_update<3><<<nb, kBlock, 0, s>>>(a); break;
+  }
+}
+void launch_seed(const KernelArgs& a, int precision, cudaStream_t s) {
+  (void)precision;
+  k_seed<<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
+}
+void launch_ibm(const KernelArgs& a, int precision, cudaStream_t s) {
+  (void)precision;
+  if (a.N > 0) k_ibm<<<blocks_for(a.N, 128), 128, 0, s>>>(a);
+}
+
+}  // namespace plfbs

@@ -1,0 +1,285 @@
+"""ctypes binding of include/plfbs.h (libplfbs.so) and a small Python front end.
+
+This is the Python view of the same C ABI the reference-side C++ shim uses; it
+loads the in-tree library and raises if it is missing (no fallback path).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "_lib", "libplfbs.so")
+
+OK, ERR_ARG, ERR_MESH, ERR_BC, ERR_CUDA, ERR_DIVERGED, ERR_NO_DEVICE, ERR_STATE = (
+    0, -1, -2, -3, -4, -5, -6, -7)
+GRAD_LS, GRAD_HYBRID, GRAD_GREEN_GAUSS = 0, 1, 2
+FP64, FP32_DEVIATION = 0, 1
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+# every symbol include/plfbs.h declares
+EXPORTS = ("plfbs_create", "plfbs_set_state", "plfbs_run", "plfbs_get_state",
+           "plfbs_get_nodes", "plfbs_get_body_force", "plfbs_set_debug", "plfbs_run_stages",
+           "plfbs_get_gradients", "plfbs_get_face_flux", "plfbs_get_residual",
+           "plfbs_ls_weights", "plfbs_profile_steps", "plfbs_memory_bytes",
+           "plfbs_last_error", "plfbs_destroy", "plfbs_version")
+
+
+class MeshView(C.Structure):
+    _fields_ = [("n_cells", C.c_int32), ("n_faces", C.c_int32), ("n_internal", C.c_int32),
+                ("owner", _ip), ("neighbour", _ip), ("face_area", _dp), ("face_normal", _dp),
+                ("face_centroid", _dp), ("streaming_dt", _dp), ("cell_volume", _dp),
+                ("cell_centroid", _dp), ("stencil_offsets", _ip), ("stencil_cells", _ip),
+                ("stencil_faces", _ip)]
+
+
+class BCView(C.Structure):
+    _fields_ = [("rho_type", _ip), ("vel_type", _ip), ("value", _dp)]
+
+
+class IBMView(C.Structure):
+    _fields_ = [("n_nodes", C.c_int32), ("x_ref", _dp), ("x", _dp), ("stiffness", C.c_double),
+                ("radius", C.c_double), ("depth", C.c_double), ("object_nodes", C.c_int32)]
+
+
+class Config(C.Structure):
+    _fields_ = [("visc", C.c_double), ("gamma", C.c_double), ("time_marching_step", C.c_double),
+                ("domain_dt", C.c_double), ("max_velocity", C.c_double), ("ref_rho", C.c_double),
+                ("tolerance", C.c_double), ("pressure_gradient", C.c_double),
+                ("channel_height", C.c_double), ("origin", C.c_double * 3),
+                ("lengths", C.c_double * 3), ("gradient_mode", C.c_int32),
+                ("precision", C.c_int32), ("renumber", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("steps_done", C.c_int64), ("converged", C.c_int32), ("status", C.c_int32),
+                ("max_error", C.c_double), ("rho_rms", C.c_double), ("u_rms", C.c_double),
+                ("v_rms", C.c_double), ("w_rms", C.c_double), ("kernel_ms", C.c_double),
+                ("steps_run", C.c_int64)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libplfbs.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libplfbs.so is missing at %s: run `python -m plfbs.build`"
+                               % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        L.plfbs_last_error.restype = C.c_char_p
+        L.plfbs_version.restype = C.c_char_p
+        L.plfbs_create.argtypes = [C.POINTER(Config), C.POINTER(MeshView), C.POINTER(BCView),
+                                   C.POINTER(IBMView), C.c_int, C.POINTER(C.c_void_p)]
+        for name in ("plfbs_set_state", "plfbs_get_state"):
+            getattr(L, name).argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_int64]
+        L.plfbs_run.argtypes = [C.c_void_p, C.c_int64, C.POINTER(Stats), _dp]
+        L.plfbs_get_nodes.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_int32]
+        L.plfbs_get_body_force.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
+        L.plfbs_set_debug.argtypes = [C.c_void_p, C.c_int]
+        L.plfbs_run_stages.argtypes = [C.c_void_p, C.c_int64]
+        for name in ("plfbs_get_gradients", "plfbs_get_face_flux", "plfbs_get_residual"):
+            getattr(L, name).argtypes = [C.c_void_p, _dp, C.c_int32]
+        L.plfbs_ls_weights.argtypes = [C.POINTER(MeshView), C.c_int32, _dp, _dp]
+        L.plfbs_profile_steps.argtypes = [C.c_void_p, C.c_int64, _dp]
+        L.plfbs_memory_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        L.plfbs_last_error.argtypes = [C.c_void_p]
+        L.plfbs_destroy.argtypes = [C.c_void_p]
+        _lib = L
+    return _lib
+
+
+class PlfbsError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__("plfbs error %d: %s" % (code, message))
+        self.code = code
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip)
+
+
+def mesh_view(ma, keep):
+    """A MeshView over the arrays of a cases.MeshArrays (kept alive in ``keep``)."""
+    def k(a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a
+    v = MeshView()
+    v.n_cells, v.n_faces, v.n_internal = ma.n_cells, ma.n_faces, ma.n_internal
+    v.owner = _i(k(ma.owner, np.int32))
+    v.neighbour = _i(k(ma.neighbour, np.int32))
+    v.face_area = _d(k(ma.face_area, np.float64))
+    v.face_normal = _d(k(ma.face_normal, np.float64))
+    v.face_centroid = _d(k(ma.face_centroid, np.float64))
+    v.streaming_dt = _d(k(ma.streaming_dt, np.float64))
+    v.cell_volume = _d(k(ma.cell_volume, np.float64))
+    v.cell_centroid = _d(k(ma.cell_centroid, np.float64))
+    v.stencil_offsets = _i(k(ma.stencil_offsets, np.int32))
+    v.stencil_cells = _i(k(ma.stencil_cells, np.int32))
+    v.stencil_faces = _i(k(ma.stencil_faces, np.int32))
+    return v
+
+
+def ls_weights(ma, mode):
+    """Host-only least-squares weights: (lhs_inv [C,3,3], rhs [nnz,3])."""
+    keep = []
+    v = mesh_view(ma, keep)
+    nnz = int(ma.stencil_offsets[-1])
+    lhs = np.zeros((ma.n_cells, 3, 3))
+    rhs = np.zeros((nnz, 3))
+    rc = lib().plfbs_ls_weights(C.byref(v), int(mode), _d(lhs), _d(rhs))
+    if rc:
+        raise PlfbsError(rc, lib().plfbs_last_error(None).decode())
+    return lhs, rhs
+
+
+class Solver:
+    """One plfbs context on one GPU.
+
+    ``cfg`` keys: visc, gamma, dt (time_marching_step), domain_dt, max_velocity,
+    ref_rho, tolerance, pressure_gradient, channel_height, origin, lengths,
+    gradient_mode, precision, renumber. ``ibm`` (optional): node_ref [N,3],
+    node_x [N,3], stiffness, radius, depth, object_nodes.
+    """
+
+    def __init__(self, ma, rho_type, vel_type, bc_value, cfg, ibm=None, device=0):
+        self._keep = []
+        self.ma = ma
+        self.C, self.F, self.B = ma.n_cells, ma.n_faces, ma.n_bc
+        self.T = self.C + self.B
+        L = lib()
+        mv = mesh_view(ma, self._keep)
+        bv = BCView()
+        rt = np.ascontiguousarray(rho_type, np.int32)
+        vt = np.ascontiguousarray(vel_type, np.int32)
+        bval = np.ascontiguousarray(bc_value, np.float64).reshape(-1, 4)
+        self._keep += [rt, vt, bval]
+        bv.rho_type, bv.vel_type, bv.value = _i(rt), _i(vt), _d(bval)
+        cf = Config()
+        cf.visc = cfg["visc"]
+        cf.gamma = cfg.get("gamma", 1.0)
+        cf.time_marching_step = cfg["dt"]
+        cf.domain_dt = cfg.get("domain_dt", 0.5)
+        cf.max_velocity = cfg["max_velocity"]
+        cf.ref_rho = cfg.get("ref_rho", 1.0)
+        cf.tolerance = cfg.get("tolerance", 0.0)
+        cf.pressure_gradient = cfg.get("pressure_gradient", 0.0)
+        cf.channel_height = cfg.get("channel_height", 1.0)
+        for a in range(3):
+            cf.origin[a] = cfg.get("origin", (0.0, 0.0, 0.0))[a]
+            cf.lengths[a] = cfg.get("lengths", (1.0, 1.0, 1.0))[a]
+        cf.gradient_mode = cfg.get("gradient_mode", GRAD_LS)
+        cf.precision = cfg.get("precision", FP64)
+        cf.renumber = cfg.get("renumber", 0)
+        iv = IBMView()
+        self.N = 0
+        if ibm is not None and len(ibm.get("node_ref", [])) > 0:
+            nref = np.ascontiguousarray(ibm["node_ref"], np.float64).reshape(-1, 3)
+            nx = np.ascontiguousarray(ibm.get("node_x", nref), np.float64).reshape(-1, 3)
+            self._keep += [nref, nx]
+            self.N = nref.shape[0]
+            iv.n_nodes = self.N
+            iv.x_ref, iv.x = _d(nref), _d(nx)
+            iv.stiffness = ibm.get("stiffness", 0.0)
+            iv.radius = ibm.get("radius", 1.0)
+            iv.depth = ibm.get("depth", 1.0)
+            iv.object_nodes = int(ibm.get("object_nodes", self.N))
+        h = C.c_void_p()
+        rc = L.plfbs_create(C.byref(cf), C.byref(mv), C.byref(bv), C.byref(iv), int(device),
+                            C.byref(h))
+        if rc:
+            raise PlfbsError(rc, L.plfbs_last_error(None).decode())
+        self.h = h
+        self._keep.clear()
+
+    def _check(self, rc):
+        if rc:
+            raise PlfbsError(rc, lib().plfbs_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().plfbs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, state):
+        """state [C+B, 4] = (u, v, w, rho) in caller numbering."""
+        s = np.asarray(state, np.float64).reshape(self.T, 4)
+        cols = [np.ascontiguousarray(s[:, k]) for k in (3, 0, 1, 2)]
+        self._check(lib().plfbs_set_state(self.h, *[_d(c) for c in cols], self.T))
+
+    def get_state(self):
+        cols = [np.zeros(self.T) for _ in range(4)]
+        self._check(lib().plfbs_get_state(self.h, *[_d(c) for c in cols], self.T))
+        rho, u, v, w = cols
+        return np.stack([u, v, w, rho], axis=1)
+
+    def run(self, max_steps, history=True):
+        st = Stats()
+        hist = np.zeros((max(int(max_steps), 1), 6)) if history else None
+        rc = lib().plfbs_run(self.h, int(max_steps), C.byref(st),
+                             _d(hist) if history else C.cast(None, _dp))
+        out = {k: getattr(st, k) for k, _ in Stats._fields_}
+        if rc and rc != ERR_DIVERGED:
+            self._check(rc)
+        out["rc"] = rc
+        return out, (hist[: int(st.steps_run)] if history else None)
+
+    def run_stages(self, n):
+        self._check(lib().plfbs_run_stages(self.h, int(n)))
+
+    def set_debug(self, on=True):
+        self._check(lib().plfbs_set_debug(self.h, int(bool(on))))
+
+    def gradients(self):
+        g = np.zeros((self.C, 12))
+        self._check(lib().plfbs_get_gradients(self.h, _d(g), self.C))
+        return g
+
+    def face_flux(self):
+        g = np.zeros((self.F, 4))
+        self._check(lib().plfbs_get_face_flux(self.h, _d(g), self.F))
+        return g
+
+    def residual(self):
+        g = np.zeros((self.C, 4))
+        self._check(lib().plfbs_get_residual(self.h, _d(g), self.C))
+        return g
+
+    def nodes(self):
+        x, v, f = (np.zeros((self.N, 3)) for _ in range(3))
+        self._check(lib().plfbs_get_nodes(self.h, _d(x), _d(v), _d(f), self.N))
+        return x, v, f
+
+    def body_force(self, frontal_area):
+        cd, cl = C.c_double(), C.c_double()
+        self._check(lib().plfbs_get_body_force(self.h, float(frontal_area), C.byref(cd),
+                                               C.byref(cl)))
+        return cd.value, cl.value
+
+    def profile_steps(self, n):
+        ms = np.zeros(4)
+        self._check(lib().plfbs_profile_steps(self.h, int(n), _d(ms)))
+        return dict(zip(("ibm", "gradient", "flux", "update"), ms.tolist()))
+
+    def memory_bytes(self):
+        b = C.c_int64()
+        self._check(lib().plfbs_memory_bytes(self.h, C.byref(b)))
+        return b.value

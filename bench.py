@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Throughput of the LBFS explicit time step on B200 (one JSON line on rank 0).
+
+Workload: the sphere-in-channel case — a 128 x 64 x 64 uniform hex channel
+(524,288 cells, 1,593,344 faces) with an immersed sphere of diameter 16 cells
+at (32, 32, 32) carried by 3,217 Fibonacci-lattice nodes; inlet u = 0.05
+(Dirichlet velocity, Neumann density), outlet Neumann velocity with rho = 1,
+side walls Neumann in velocity and density (the GPU path has no slip type);
+Re = 100 on the diameter (nu = 0.008), RK dt 0.2, FP64. Synthetic, seeded
+inputs; uniform-flow start.
+
+A step is one full time step: the IBM update and 4 RK stages over all cells
+and faces. `value` is device throughput in Mcell-updates/s (cells x steps /
+time, summed over ranks, max time over ranks) with everything resident in
+HBM; the working set (~0.5 GB) exceeds the 126 MB L2, so no flush is needed
+between steps. `e2e` times the whole drop-in call through the C ABI from host
+buffers: create (mesh upload, least-squares weights, layout), set_state,
+run, the per-step residual history read-back, get_state and destroy.
+
+--impl reference times the reference's own CPU Solver (oracle/_ref, built
+from the reference sources) on the same mesh and boundary conditions.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "3d-plfbs-gpu_b200"))
+
+from plfbs import cases  # noqa: E402
+
+METRIC = "Mcell-updates/s"
+WORKLOAD = "sphere_channel_128x64x64_ibm3217_fp64"
+NX, NY, NZ = 128, 64, 64
+DIAM, CENTRE, NNODES = 16.0, (32.0, 32.0, 32.0), 3217
+U, RE, DT, STIFFNESS = 0.05, 100.0, 0.2, 0.5
+KERNELS_PER_STEP = 13  # ibm + 4 x (gradient, flux, update)
+
+# Algorithmic bytes per launch (FP64, perfect reuse): per face the geometry
+# (normal, area, streaming dt, owner/neighbour offsets: 72 B) and the flux
+# write (32 B); per cell the state (32 B), gradients (96 B), centroid and
+# volume (32 B) read once. gradient: state + 6 weights/indices + gradient
+# write; update: 6 face fluxes, indices, t0, t1 read+write, state write.
+def algorithmic_bytes(C, F, B):
+    return {"flux": 104 * F + 160 * C,
+            "gradient": 296 * C,
+            "update": 344 * C}
+
+
+def build_case():
+    pm = cases.uniform_box(NX, NY, NZ, patch_types=["inlet", "outlet", "side", "side", "side",
+                                                    "side"])
+    c = cases.Case(mesh_dir="", X=NX, Y=NY, Z=NZ, dt=DT, mach=U, reynolds=RE, ref_length=DIAM,
+                   tolerance=0.0, obj_radius=DIAM / 2, obj_depth=DIAM, obj_stiffness=STIFFNESS,
+                   obj_centre=CENTRE,
+                   bcs=[cases.BC("inlet", 1, 1, 0, 0, "dirichlet", "neumann"),
+                        cases.BC("outlet", 1, 0, 0, 0, "neumann", "dirichlet"),
+                        cases.BC("side", 1, 0, 0, 0, "neumann", "neumann")])
+    ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
+    nodes = cases.fibonacci_sphere(NNODES, DIAM / 2, CENTRE)
+    state0 = np.zeros((ma.total_cells, 4))
+    state0[:, 0] = U
+    state0[:, 3] = 1.0
+    return pm, c, ma, nodes, state0
+
+
+def solver_cfg(c):
+    return dict(visc=c.visc, gamma=1.0, dt=c.dt, domain_dt=0.5, max_velocity=c.mach,
+                ref_rho=1.0, tolerance=0.0, pressure_gradient=0.0, channel_height=c.Y,
+                origin=(0.0, 0.0, 0.0), lengths=(c.X, c.Y, c.Z), gradient_mode=0, renumber=0)
+
+
+def ibm_cfg(nodes):
+    return dict(node_ref=nodes, stiffness=STIFFNESS, radius=DIAM / 2, depth=DIAM,
+                object_nodes=len(nodes))
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, device):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.01)
+
+    def __enter__(self):
+        if self.nv:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self.nv:
+            self.t.join()
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic(kernel, workload):
+    """ncu DRAM bytes per launch of `kernel` on `workload`, committed under
+    profiles/traffic.json by the profiling recipe (null when absent)."""
+    try:
+        with open(os.path.join(REPO, "profiles", "traffic.json")) as f:
+            t = json.load(f)
+        return t.get(workload, {}).get(kernel)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's CPU Solver (serial) on the same case
+# ---------------------------------------------------------------------------
+
+REF_BIN = os.path.join(REPO, "oracle", "_ref", "plfbs_ref")
+
+
+def _run_ref_cpu(workdir, pm, c, nodes, steps):
+    import shutil
+    c.steps = steps
+    c.gpu_solver = 0
+    c.output_dir = os.path.join(workdir, "out") + "/"
+    if os.path.isdir(os.path.join(workdir, "out")):
+        shutil.rmtree(os.path.join(workdir, "out"))
+    node_file = os.path.join(workdir, "nodes.txt")
+    if not os.path.exists(node_file):
+        cases.write_spring_network(node_file, nodes)
+    c.obj_nodes_file = node_file
+    c.obj_num_nodes = len(nodes)
+    c.mesh_dir = os.path.join(workdir, "polyMesh")
+    xml = os.path.join(workdir, "case.xml")
+    cases.write_xml(xml, c)
+    t0 = time.perf_counter()
+    subprocess.run([REF_BIN, xml], cwd=workdir, check=True, stdout=subprocess.DEVNULL,
+                   stderr=subprocess.DEVNULL)
+    return time.perf_counter() - t0
+
+
+def reference_cpu_throughput(pm, c, nodes, sample_steps=1):
+    """Mcell-updates/s of the reference CPU Solver: wall time of a run of
+    `sample_steps` steps minus that of a 0-step run (mesh import and setup)."""
+    if not os.path.exists(REF_BIN):
+        return None, "oracle/_ref/plfbs_ref not built"
+    with tempfile.TemporaryDirectory(prefix="plfbs_refcpu_") as wd:
+        cases.write_polymesh(os.path.join(wd, "polyMesh"), pm)
+        t_setup = _run_ref_cpu(wd, pm, c, nodes, 0)
+        t_run = _run_ref_cpu(wd, pm, c, nodes, sample_steps)
+    per_step = max(t_run - t_setup, 1e-9) / sample_steps
+    return pm.n_cells / per_step / 1e6, (
+        "%d time step(s) of the reference CPU Solver on the same %dx%dx%d mesh and boundary "
+        "conditions (the CPU Solver has no IBM), setup subtracted via a 0-step run "
+        "(%.1f s setup, %.1f s per step), serial" % (sample_steps, NX, NY, NZ, t_setup,
+                                                    per_step))
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    pm, c, ma, nodes, _ = build_case()
+    value, sample = reference_cpu_throughput(pm, c, nodes, sample_steps=1)
+    cfg = {"workload": WORKLOAD, "cells": ma.n_cells, "faces": ma.n_faces,
+           "nodes": NNODES, "parallelism": "replicas"}
+    if value is None:
+        print(json.dumps({"impl": "reference", "unavailable": sample}))
+        return 0
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+            "n_gpus": world, "steps": 1, "warmup": 0, "requested_steps": args.steps,
+            "ms_per_step": ma.n_cells / value / 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": cfg,
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": 1, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=20)
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from plfbs import capi
+
+    pm, c, ma, nodes, state0 = build_case()
+    rt, vt, val = cases.bc_arrays(ma, c)
+    solver = capi.Solver(ma, rt, vt, val, solver_cfg(c), ibm=ibm_cfg(nodes), device=local_rank)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up
+    solver.set_state(state0)
+    st, _ = solver.run(args.warmup, history=False)
+    if st["rc"] != 0:
+        raise RuntimeError("warm-up diverged")
+    barrier()
+    with ClockSampler(local_rank) as clk:
+        st, hist = solver.run(args.steps, history=True)
+    barrier()
+    if st["rc"] != 0 or st["steps_run"] != args.steps:
+        raise RuntimeError("timed run stopped early: %r" % st)
+    ms = max_over_ranks(st["kernel_ms"])
+    value = world * ma.n_cells * args.steps / (ms / 1e3) / 1e6
+
+    # per-kernel device times (CUDA events between launches on the solver's stream)
+    prof = solver.profile_steps(args.profile_steps)
+    per_launch = {"ibm": prof["ibm"] / args.profile_steps,
+                  "gradient": prof["gradient"] / (4 * args.profile_steps),
+                  "flux": prof["flux"] / (4 * args.profile_steps),
+                  "update": prof["update"] / (4 * args.profile_steps)}
+    total = sum(prof.values())
+    alg = algorithmic_bytes(ma.n_cells, ma.n_faces, ma.n_bc)
+    peak, peak_kind = load_peaks()
+    kern = {}
+    for k in ("gradient", "flux", "update"):
+        gbs = alg[k] / (per_launch[k] / 1e3) / 1e9
+        kern[k] = {"ms_per_launch": per_launch[k], "share": prof[k] / total,
+                   "algorithmic_bytes": alg[k], "achieved_gbs": gbs, "frac": gbs / peak}
+    kern["ibm"] = {"ms_per_launch": per_launch["ibm"], "share": prof["ibm"] / total}
+    dom = max(("gradient", "flux", "update"), key=lambda k: prof[k])
+    roof = {"kernel": dom, "bound": "hbm", "achieved": kern[dom]["achieved_gbs"], "peak": peak,
+            "unit": "GB/s", "frac": kern[dom]["frac"], "peak_kind": peak_kind,
+            "traffic": load_traffic(dom, WORKLOAD)}
+
+    # end to end through the C ABI from host buffers
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        solver.close()
+        t0 = time.perf_counter()
+        s2 = capi.Solver(ma, rt, vt, val, solver_cfg(c), ibm=ibm_cfg(nodes), device=local_rank)
+        s2.set_state(state0)
+        st2, hist2 = s2.run(args.steps, history=True)
+        out = s2.get_state()
+        s2.close()
+        wall = max_over_ranks(time.perf_counter() - t0)
+        T = ma.total_cells
+        mesh_bytes = (ma.n_faces * (4 + 4 + 8 + 24 + 24 + 8) + T * (8 + 24) +
+                      (ma.n_cells + 1 + 2 * len(ma.stencil_cells)) * 4 + ma.n_bc * (4 + 4 + 32) +
+                      len(nodes) * 48)
+        h2d = mesh_bytes + T * 32
+        d2h = T * 32 + 48 * args.steps
+        e2e = {"value": world * ma.n_cells * args.steps / wall / 1e6, "unit": METRIC,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "wall_s": wall, "includes": "create+set_state+run+history+get_state+destroy"}
+        assert np.isfinite(out).all() and st2["steps_run"] == args.steps
+    else:
+        solver.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, sample = reference_cpu_throughput(pm, c, nodes, sample_steps=1)
+        if v is not None:
+            cpu = {"value": v, "unit": METRIC, "cores": 1, "kind": "reference", "sample": sample}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "cells": ma.n_cells, "faces": ma.n_faces,
+                           "nodes": NNODES, "re": RE, "dt": DT,
+                           "parallelism": "replicas" if world > 1 else "single",
+                           "l2": "working set > L2 (no flush)"},
+                "roofline": roof, "kernels": kern, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": KERNELS_PER_STEP * args.steps, "clocks": clk.summary(),
+                "final_max_error": float(hist[-1, 1]) if len(hist) else None}
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

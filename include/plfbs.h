@@ -1,0 +1,188 @@
+/*
+ * plfbs.h — C ABI of the B200 LBFS explicit time step.
+ *
+ * Drop-in for the GPU path of CHRG-Developer/3D-PLFBS-GPU:
+ *   gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh&, Solution&,
+ *       Boundary_Conditions&, external_forces&, global_variables&,
+ *       domain_geometry&, initial_conditions&, unstructured_bcs&, int mg,
+ *       Solution& residual, int fmg, post_processing&,
+ *       std::vector<lagrangian_object>&)          (src/Solver_gpu.h:28-31,
+ *                                                   src/Solver_gpu.cu:150-917)
+ * called from program.cpp:107-109. A thin C++ shim with that exact signature
+ * copies the mesh/BC/object getters into the plain views below and drives
+ * create -> set_state -> run -> get_state -> destroy.
+ *
+ * Conventions: all arrays are borrowed for the duration of the call only and
+ * use the caller's numbering (cells 0..C-1, then one ghost per boundary face,
+ * ghost index C + f - F_i for boundary face f, as unstructured_mesh assigns,
+ * unstructured_mesh.cpp:1346-1375). Per-cell state is four doubles (u, v, w,
+ * rho). Every function returns PLFBS_OK (0) or a negative status; it never
+ * exits the process and never traps the GPU; plfbs_last_error() explains the
+ * last failure. A context is single-threaded and bound to one device.
+ */
+#ifndef PLFBS_H
+#define PLFBS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  PLFBS_OK = 0,
+  PLFBS_ERR_ARG = -1,         /* null pointer, bad size */
+  PLFBS_ERR_MESH = -2,        /* inconsistent mesh arrays */
+  PLFBS_ERR_BC = -3,          /* boundary type the GPU path does not define */
+  PLFBS_ERR_CUDA = -4,        /* CUDA runtime error (message in last_error) */
+  PLFBS_ERR_DIVERGED = -5,    /* NaN residual or rho > 1000 (Solver.cpp:448-493) */
+  PLFBS_ERR_NO_DEVICE = -6,   /* no CUDA device / device not sm_100 */
+  PLFBS_ERR_STATE = -7        /* call out of order */
+};
+
+/* Gradient weighting, gradients.cpp:259-265 ("LS", "hybrid", anything else = GG). */
+enum { PLFBS_GRAD_LS = 0, PLFBS_GRAD_HYBRID = 1, PLFBS_GRAD_GREEN_GAUSS = 2 };
+
+/* Arithmetic of the time step. */
+enum {
+  PLFBS_FP64 = 0,            /* the reference's FP64 semantics */
+  PLFBS_FP32_DEVIATION = 1   /* FP32 state/flux, rho stored as rho - rho0,
+                                velocity scaled by the reference velocity;
+                                FP64 weights built then stored FP32, FP64
+                                reductions and node positions */
+};
+
+/* Pre-processed mesh: what unstructured_mesh exposes (unstructured_mesh.h:15-47)
+ * and what Solver_gpu.cu marshals (Solver_gpu.cu:629-651). B = n_faces - n_internal. */
+typedef struct {
+  int32_t n_cells;            /* C  = get_n_cells() */
+  int32_t n_faces;            /* F  = get_n_faces() */
+  int32_t n_internal;         /* F_i = get_n_neighbours(); faces [F_i, F) are boundary */
+  const int32_t* owner;       /* [F] get_mesh_owner */
+  const int32_t* neighbour;   /* [F] get_mesh_neighbour (boundary: C + f - F_i) */
+  const double* face_area;    /* [F] get_face_area */
+  const double* face_normal;  /* [3F] get_face_i/j/k, unit, owner -> neighbour */
+  const double* face_centroid;/* [3F] get_face_x/y/z */
+  const double* streaming_dt; /* [F] get_delta_t_face */
+  const double* cell_volume;  /* [C+B] get_cell_volume */
+  const double* cell_centroid;/* [3(C+B)] get_centroid_x/y/z */
+  const int32_t* stencil_offsets; /* [C+1] CSR over gradient_cells / gradient_faces */
+  const int32_t* stencil_cells;   /* [nnz] gradient_cells[i][*] */
+  const int32_t* stencil_faces;   /* [nnz] gradient_faces[i][*] */
+} plfbs_mesh_view;
+
+/* Boundary conditions per boundary face (Boundary_Conditions, marshalled as in
+ * Solver_gpu.cu:653-655). Supported on the GPU path: rho_type 1 (Dirichlet) or
+ * 2 (Neumann); vel_type 1 (Dirichlet), 2 (Neumann) or 9 (parabolic inlet). */
+typedef struct {
+  const int32_t* rho_type;    /* [B] */
+  const int32_t* vel_type;    /* [B] */
+  const double* value;        /* [4B] u, v, w, rho (get_u/v/w/rho) */
+} plfbs_bc_view;
+
+/* Lagrangian nodes of all objects (Solver_gpu.cu:1469-1499). Force area uses
+ * object 0's stiffness/radius/depth/num_nodes, as Solver_gpu.cu:708-709 does.
+ * n_nodes may be 0 (no immersed body). */
+typedef struct {
+  int32_t n_nodes;
+  const double* x_ref;        /* [3N] interleaved x, y, z reference positions */
+  const double* x;            /* [3N] interleaved current positions */
+  double stiffness, radius, depth;
+  int32_t object_nodes;       /* object_vec[0].num_nodes */
+} plfbs_ibm_view;
+
+typedef struct {
+  double visc;                /* globals.visc */
+  double gamma;               /* globals.pre_conditioned_gamma */
+  double time_marching_step;  /* globals.time_marching_step (the RK dt) */
+  double domain_dt;           /* domain.dt (streaming dt; IBM spacing = 2 domain.dt) */
+  double max_velocity;        /* globals.max_velocity */
+  double ref_rho;             /* globals.ref_rho */
+  double tolerance;           /* globals.tolerance */
+  double pressure_gradient;   /* init_conds.pressure_gradient (body force x) */
+  double channel_height;      /* domain.Y (parabolic inlet, LBFS.cu:1286) */
+  double origin[3];           /* domain.origin_x/y/z */
+  double lengths[3];          /* domain.X/Y/Z */
+  int32_t gradient_mode;      /* PLFBS_GRAD_* */
+  int32_t precision;          /* PLFBS_FP64 or PLFBS_FP32_DEVIATION */
+  int32_t renumber;           /* 1: reorder cells (RCM) and faces for locality */
+  int32_t reserved;
+} plfbs_config;
+
+typedef struct {
+  int64_t steps_done;         /* time steps completed by this context */
+  int32_t converged;          /* max_error < tolerance reached */
+  int32_t status;             /* PLFBS_OK or PLFBS_ERR_DIVERGED */
+  double max_error;           /* residuals::max_error() of the last step */
+  double rho_rms, u_rms, v_rms, w_rms; /* l2_norm_rms_moukallad of the last step */
+  double kernel_ms;           /* device time of the run() call (CUDA events) */
+  int64_t steps_run;          /* steps completed by this run() call */
+} plfbs_stats;
+
+typedef struct plfbs_ctx plfbs_ctx;
+
+/* Replaces the setup half of Solver_gpu.cu:150-662: validates the views,
+ * builds the least-squares weights (gradients.cpp:214-313), renumbers for
+ * locality, uploads everything to `device` and captures one time step in a
+ * CUDA graph. The initial state is all zeros until plfbs_set_state. */
+int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh,
+                 const plfbs_bc_view* bc, const plfbs_ibm_view* ibm, int device,
+                 plfbs_ctx** out);
+
+/* soln_to_double (Solver_gpu.cu:1646-1659) + the RK seed (Solver_gpu.cu:664):
+ * n_total = C + B values per array, caller numbering. Resets the step count. */
+int plfbs_set_state(plfbs_ctx* ctx, const double* rho, const double* u, const double* v,
+                    const double* w, int64_t n_total);
+
+/* The time loop of Solver_gpu.cu:667-898: up to max_steps steps, stopping after
+ * the first step whose max_error < tolerance (Solver_gpu.cu:870). Synchronous.
+ * history (optional, may be NULL) receives 6 doubles per completed step:
+ * step index, max_error, rho_rms, u_rms, v_rms, w_rms. */
+int plfbs_run(plfbs_ctx* ctx, int64_t max_steps, plfbs_stats* stats, double* history);
+
+/* soln.clone(temp_soln) (Solver_gpu.cu:846,872,904): C + B values per array. */
+int plfbs_get_state(plfbs_ctx* ctx, double* rho, double* u, double* v, double* w,
+                    int64_t n_total);
+
+/* Lagrangian node positions, velocities and forces, 3N each (interleaved xyz). */
+int plfbs_get_nodes(plfbs_ctx* ctx, double* x, double* vel, double* force, int32_t n_nodes);
+
+/* Immersed-body drag and lift: -sum(node force) projected on x and y,
+ * normalised by 0.5 rho_ref U^2 * frontal_area. No reference counterpart
+ * (the reference never reduces IBM forces); returns PLFBS_ERR_STATE without nodes. */
+int plfbs_get_body_force(plfbs_ctx* ctx, double frontal_area, double* cd, double* cl);
+
+/* Introspection for parity tests (caller numbering). plfbs_run_stages advances
+ * by RK stages (4 per time step; the IBM update runs before each step's first
+ * stage) with individual kernel launches instead of the step graph. The
+ * getters return the last stage's interior-cell gradients [12C] (rho, u, v, w,
+ * each x, y, z), face fluxes [4F] (x, y, z momentum, mass) and residuals [4C]
+ * (u, v, w, rho); residuals are only recorded after plfbs_set_debug(ctx, 1). */
+int plfbs_set_debug(plfbs_ctx* ctx, int enable);
+int plfbs_run_stages(plfbs_ctx* ctx, int64_t n_stages);
+int plfbs_get_gradients(plfbs_ctx* ctx, double* grad, int32_t n_cells);
+int plfbs_get_face_flux(plfbs_ctx* ctx, double* flux, int32_t n_faces);
+int plfbs_get_residual(plfbs_ctx* ctx, double* res, int32_t n_cells);
+
+/* Host-only: the least-squares weights as gradients::pre_fill_LHS_and_RHS_matrix
+ * computes them (gradients.cpp:214-313, determinant as written at :282-284):
+ * lhs_inv [9C] row-major, rhs [3 nnz] per stencil entry. No GPU needed. */
+int plfbs_ls_weights(const plfbs_mesh_view* mesh, int32_t gradient_mode, double* lhs_inv,
+                     double* rhs);
+
+/* Per-kernel device time: advances n_steps time steps launching each kernel
+ * between CUDA events and returns the summed milliseconds per kernel kind in
+ * ms[4] = {ibm, gradient, flux, update}. For profiling; the state advances. */
+int plfbs_profile_steps(plfbs_ctx* ctx, int64_t n_steps, double* ms);
+
+/* Device bytes held by the context. */
+int plfbs_memory_bytes(plfbs_ctx* ctx, int64_t* bytes);
+
+const char* plfbs_last_error(const plfbs_ctx* ctx);  /* ctx may be NULL: global error */
+void plfbs_destroy(plfbs_ctx* ctx);
+const char* plfbs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PLFBS_H */

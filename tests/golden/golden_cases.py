@@ -1,0 +1,105 @@
+"""Definitions of the small seeded cases behind the committed golden fixtures.
+
+Shared by make_golden.py (which runs the reference on them) and the tests
+(which rebuild the same inputs and compare against the fixtures). Each case
+exercises a different part of the reference's GPU path:
+
+  cavity    6x5x4 lid-driven cavity, Dirichlet walls + moving lid, LS weights
+  channel   10x6x6 channel: parabolic inlet (vel type 9), pressure outlet,
+            no-slip and Neumann walls, a body force, an IBM sphere of 30
+            Fibonacci nodes plus two nodes near x = 0 whose structured index
+            wraps across rows (the reference checks only the linear index)
+  graded    6x6x5 geometrically graded hexes, hybrid LS/Green-Gauss weights,
+            gamma = 1.3, streaming dt capped by fneq_min, offset origin
+  converge  the cavity with a loose tolerance: stops after its first step
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "3d-plfbs-gpu_b200"))
+
+from plfbs import cases  # noqa: E402
+
+NAMES = ("cavity", "channel", "graded", "converge")
+
+
+def _random_state(ma, seed, amp=0.02):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    T = ma.total_cells
+    x = ma.cell_centroid
+    s = np.zeros((T, 4))
+    s[:, 0] = amp * np.sin(0.7 * x[:, 0] + 0.3 * x[:, 2]) + 0.5 * amp * rng.standard_normal(T)
+    s[:, 1] = amp * np.cos(0.5 * x[:, 1]) + 0.5 * amp * rng.standard_normal(T)
+    s[:, 2] = 0.5 * amp * np.sin(x[:, 2] + x[:, 0]) + 0.5 * amp * rng.standard_normal(T)
+    s[:, 3] = 1.0 + 0.5 * amp * rng.standard_normal(T)
+    return s
+
+
+def build(name):
+    """Returns dict(pm, case, nodes, state0, ma) for a golden case."""
+    if name in ("cavity", "converge"):
+        pm = cases.uniform_box(6, 5, 4, patch_types=["wall", "wall", "wall", "lid", "wall", "wall"])
+        c = cases.Case(mesh_dir="", X=6, Y=5, Z=4, steps=3, dt=0.1, mach=0.1, reynolds=100,
+                       ref_length=6, obj_centre=(3.0, 2.5, 2.0),
+                       bcs=[cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann"),
+                            cases.BC("lid", 1, 1, 0, 0, "dirichlet", "neumann")])
+        if name == "converge":
+            c.tolerance = 1.0
+            c.steps = 5
+        nodes = np.array([[3.0, 2.5, 2.0]])
+        seed = 11
+    elif name == "channel":
+        pm = cases.uniform_box(10, 6, 6, patch_types=["inlet", "outlet", "wall", "wall",
+                                                      "side", "side"])
+        c = cases.Case(mesh_dir="", X=10, Y=6, Z=6, steps=3, dt=0.2, mach=0.05, reynolds=20,
+                       ref_length=3, pressure_gradient=1e-4,
+                       bcs=[cases.BC("inlet", 1, 1, 0, 0, "parabolic", "neumann"),
+                            cases.BC("outlet", 1, 0, 0, 0, "neumann", "dirichlet"),
+                            cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann"),
+                            cases.BC("side", 1, 0, 0, 0, "neumann", "neumann")])
+        sphere = cases.fibonacci_sphere(30, 1.5, (4.0, 3.0, 3.0))
+        edge = np.array([[0.2, 2.4, 3.3], [0.6, 4.5, 1.2]])
+        nodes = np.concatenate([sphere, edge])
+        c.obj_radius, c.obj_depth, c.obj_stiffness = 1.5, 3.0, 0.3
+        c.obj_centre = (4.0, 3.0, 3.0)
+        seed = 12
+    elif name == "graded":
+        g = lambda n, r: np.concatenate([[0.0], np.cumsum(r ** np.arange(n))])  # noqa: E731
+        xs, ys, zs = 0.5 + g(6, 1.15), -1.0 + g(6, 0.9), 2.0 + g(5, 1.25)
+        pm = cases.hex_box(xs, ys, zs, patch_types=["in", "out", "wall", "wall", "wall", "top"])
+        c = cases.Case(mesh_dir="", X=float(xs[-1] - xs[0]), Y=float(ys[-1] - ys[0]),
+                       Z=float(zs[-1] - zs[0]), origin=(0.5, -1.0, 2.0), steps=3, dt=0.05,
+                       mach=0.1, reynolds=100, ref_length=6, gamma=1.3,
+                       gradient_calc="hybrid", fneq_min=0.036,
+                       bcs=[cases.BC("in", 1.01, 0.5, 0.1, 0, "dirichlet", "neumann"),
+                            cases.BC("out", 0.99, 0, 0, 0, "neumann", "dirichlet"),
+                            cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann"),
+                            cases.BC("top", 1, 0.3, 0, 0.2, "dirichlet", "dirichlet")])
+        nodes = np.array([[2.0, 1.0, 3.0]])
+        c.obj_centre = (2.0, 1.0, 3.0)
+        seed = 13
+    else:
+        raise KeyError(name)
+    ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
+    state0 = _random_state(ma, seed)
+    return dict(pm=pm, case=c, nodes=nodes, state0=state0, ma=ma)
+
+
+def oracle_cfg(d):
+    """The scalar configuration the solver sees for a golden case."""
+    c = d["case"]
+    nodes = d["nodes"]
+    return dict(visc=c.visc, gamma=c.gamma, dt=c.dt, domain_dt=c.streaming_dt,
+                pressure_gradient=c.pressure_gradient, channel_height=c.Y,
+                max_velocity=c.mach, ref_rho=c.average_rho, tolerance=c.tolerance,
+                origin=c.origin, lengths=(c.X, c.Y, c.Z),
+                gradient_mode={"LS": 0, "hybrid": 1}.get(c.gradient_calc, 2),
+                node_ref=nodes, node_x=nodes, stiffness=c.obj_stiffness, radius=c.obj_radius,
+                depth=c.obj_depth, object_nodes=nodes.shape[0])

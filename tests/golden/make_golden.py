@@ -1,0 +1,53 @@
+"""Regenerate the golden fixtures tests/golden/<case>.npz from the reference.
+
+    make -C oracle/ref && python tests/golden/make_golden.py
+
+Runs oracle/_ref/plfbs_ref (the reference program, built from its own
+sources; its CUDA kernels execute serially on the host) on each case of
+golden_cases.py and keeps the dumps the tests compare against: the reference's
+pre-processed mesh arrays and least-squares weights, the ghost states,
+gradients, face fluxes, residuals and state after the first RK stage, the body
+force and Lagrangian nodes after the first IBM update, and the state, RK
+accumulator, residual history and nodes after the last step.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+import golden_cases  # noqa: E402
+import refrun  # noqa: E402
+
+KEEP = ("sizes", "owner", "neighbour", "stencil", "face_area", "streaming_dt", "face_normal",
+        "face_centroid", "cell_volume", "cell_centroid", "lhs_inv", "rhs_w", "bc_value",
+        "bc_rho_type", "bc_vel_type", "state_init", "params", "s0_force", "s0_nodes",
+        "s0_state_bc", "s0_grad", "s0_face_flux", "s0_residual", "s0_state_rk",
+        "final_state", "final_t1", "history", "steps_done", "final_nodes")
+
+
+def main():
+    tmp = tempfile.mkdtemp(prefix="plfbs_golden_")
+    try:
+        for name in golden_cases.NAMES:
+            d = golden_cases.build(name)
+            dumps = refrun.run_reference(os.path.join(tmp, name), d["pm"], d["case"],
+                                         nodes=d["nodes"], init_state=d["state0"])
+            out = {k: dumps[k] for k in KEEP}
+            path = os.path.join(HERE, name + ".npz")
+            np.savez_compressed(path, **out)
+            print("%-9s %7d bytes  steps_done=%d" % (name, os.path.getsize(path),
+                                                     int(out["steps_done"][0])))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()

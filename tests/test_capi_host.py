@@ -1,0 +1,100 @@
+"""The C-ABI library on CPU: it loads, exports every symbol include/plfbs.h
+declares, computes the least-squares weights on the host exactly as the
+reference does, and rejects bad input before touching a GPU."""
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import golden_cases
+from conftest import REPO, load_golden
+from plfbs import capi, cases
+
+
+def _declared():
+    src = open(os.path.join(REPO, "include", "plfbs.h")).read()
+    return sorted(set(re.findall(r"\b(plfbs_[a-z_]+)\s*\(", src)))
+
+
+def test_exports_every_declared_symbol(plfbs_lib):
+    names = _declared()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(plfbs_lib, n), n
+    assert set(names) == set(capi.EXPORTS)
+    assert plfbs_lib.plfbs_version().startswith(b"plfbs-b200")
+
+
+@pytest.mark.parametrize("name", golden_cases.NAMES)
+def test_host_ls_weights_bit_exact(plfbs_lib, name):
+    d = golden_cases.build(name)
+    g = load_golden(name)
+    mode = golden_cases.oracle_cfg(d)["gradient_mode"]
+    lhs, rhs = capi.ls_weights(d["ma"], mode)
+    np.testing.assert_array_equal(lhs, g["lhs_inv"])
+    np.testing.assert_array_equal(rhs.reshape(-1, 6, 3), g["rhs_w"])
+
+
+def _create(ma, rt, vt, val, **over):
+    cfg = dict(visc=0.006, dt=0.1, max_velocity=0.1, lengths=(6, 5, 4))
+    cfg.update(over)
+    return capi.Solver(ma, rt, vt, val, cfg)
+
+
+def _cavity():
+    d = golden_cases.build("cavity")
+    rt, vt, val = cases.bc_arrays(d["ma"], d["case"])
+    return d["ma"], rt, vt, val
+
+
+def test_rejects_undefined_boundary_types(plfbs_lib):
+    ma, rt, vt, val = _cavity()
+    vt = vt.copy()
+    vt[5] = 3  # periodic: CPU-only in the reference (LBFS.cu:1262-1294 has 1, 2, 9)
+    with pytest.raises(capi.PlfbsError) as e:
+        _create(ma, rt, vt, val)
+    assert e.value.code == capi.ERR_BC
+    rt = rt.copy()
+    rt[0] = 7
+    with pytest.raises(capi.PlfbsError) as e:
+        _create(ma, rt, vt * 0 + 1, val)
+    assert e.value.code == capi.ERR_BC
+
+
+def test_rejects_corrupt_mesh(plfbs_lib):
+    ma, rt, vt, val = _cavity()
+    import copy
+    bad = copy.deepcopy(ma)
+    bad.neighbour = bad.neighbour.copy()
+    bad.neighbour[3] = bad.n_cells + 7  # internal face pointing at a ghost
+    with pytest.raises(capi.PlfbsError) as e:
+        _create(bad, rt, vt, val)
+    assert e.value.code == capi.ERR_MESH
+    bad = copy.deepcopy(ma)
+    bad.stencil_cells = bad.stencil_cells.copy()
+    bad.stencil_cells[0] = bad.stencil_cells[7]  # not a face neighbour of cell 0
+    with pytest.raises(capi.PlfbsError) as e:
+        _create(bad, rt, vt, val)
+    assert e.value.code == capi.ERR_MESH
+    bad = copy.deepcopy(ma)
+    bad.cell_volume = bad.cell_volume.copy()
+    bad.cell_volume[2] = -1.0
+    with pytest.raises(capi.PlfbsError) as e:
+        _create(bad, rt, vt, val)
+    assert e.value.code == capi.ERR_MESH
+
+
+def test_rejects_bad_config(plfbs_lib):
+    ma, rt, vt, val = _cavity()
+    with pytest.raises(capi.PlfbsError) as e:
+        _create(ma, rt, vt, val, dt=0.0)
+    assert e.value.code == capi.ERR_ARG
+
+
+def test_null_context_calls_fail_cleanly(plfbs_lib):
+    assert plfbs_lib.plfbs_run_stages(None, 1) == capi.ERR_ARG
+    assert plfbs_lib.plfbs_set_debug(None, 1) == capi.ERR_ARG
+    plfbs_lib.plfbs_destroy(None)

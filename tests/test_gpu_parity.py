@@ -1,0 +1,181 @@
+"""CUDA path against the reference (golden fixtures) and the C oracle.
+
+Bar: the FP64 path matches the reference's FP64 kernels to <= 1e-10 relative
+L2 on every field (the reference itself is only defined up to the order of
+its FP64 atomic additions); per-kernel quantities of one stage are held to
+1e-12 relative max error. All calls go through the C ABI (libplfbs.so).
+"""
+
+import numpy as np
+import pytest
+
+import golden_cases
+import oracle
+from conftest import load_golden, rel_err, rel_l2
+from plfbs import capi, cases
+
+pytestmark = pytest.mark.gpu
+
+STAGE_TOL = 1e-12   # one RK stage, max relative error
+RUN_TOL = 1e-10     # whole runs, relative L2 per field
+
+
+def _solver(d, renumber=0, **over):
+    cfg = golden_cases.oracle_cfg(d)
+    cfg.update(over)
+    cfg["renumber"] = renumber
+    rt, vt, val = cases.bc_arrays(d["ma"], d["case"])
+    ibm = dict(node_ref=d["nodes"], node_x=d["nodes"], stiffness=cfg["stiffness"],
+               radius=cfg["radius"], depth=cfg["depth"], object_nodes=cfg["object_nodes"])
+    return capi.Solver(d["ma"], rt, vt, val, cfg, ibm=ibm)
+
+
+@pytest.mark.parametrize("renumber", [0, 1])
+@pytest.mark.parametrize("name", golden_cases.NAMES)
+def test_first_stage_matches_reference(plfbs_lib, name, renumber):
+    d = golden_cases.build(name)
+    g = load_golden(name)
+    C = d["ma"].n_cells
+    s = _solver(d, renumber)
+    s.set_debug(True)
+    s.set_state(d["state0"])
+    s.run_stages(1)
+    st = s.get_state()
+    np.testing.assert_array_equal(st[C:], g["s0_state_bc"][C:])  # ghost states
+    assert rel_err(s.gradients(), g["s0_grad"][:C]) < STAGE_TOL
+    assert rel_err(s.face_flux(), g["s0_face_flux"]) < STAGE_TOL
+    assert rel_err(s.residual(), g["s0_residual"]) < STAGE_TOL
+    assert rel_err(st[:C], g["s0_state_rk"][:C]) < STAGE_TOL
+    x, v, f = s.nodes()
+    assert rel_err(x, g["s0_nodes"][:, 0:3]) < STAGE_TOL
+    assert rel_err(v, g["s0_nodes"][:, 3:6]) < STAGE_TOL
+    assert rel_err(f, g["s0_nodes"][:, 6:9]) < STAGE_TOL
+    s.close()
+
+
+@pytest.mark.parametrize("name", golden_cases.NAMES)
+def test_graph_run_matches_reference(plfbs_lib, name):
+    """The captured step graph, run to the case's end or to convergence."""
+    d = golden_cases.build(name)
+    g = load_golden(name)
+    s = _solver(d, renumber=1)
+    s.set_state(d["state0"])
+    stats, hist = s.run(d["case"].steps)
+    assert stats["rc"] == 0
+    assert stats["steps_done"] == int(g["steps_done"][0])
+    assert bool(stats["converged"]) == (name == "converge")
+    st = s.get_state()
+    for k in range(4):
+        assert rel_l2(st[:, k], g["final_state"][:, k]) < RUN_TOL, k
+    assert rel_err(hist, g["history"]) < 1e-10
+    x, _, _ = s.nodes()
+    assert rel_err(x, g["final_nodes"][:, 0:3]) < 1e-12
+    # a further run after convergence does nothing
+    if name == "converge":
+        stats2, hist2 = s.run(3)
+        assert stats2["steps_run"] == 0 and stats2["steps_done"] == 1
+    s.close()
+
+
+def test_stage_path_equals_graph_path(plfbs_lib):
+    """Without IBM atomics both paths are deterministic and bitwise equal."""
+    d = golden_cases.build("graded")
+    a = _solver(d, renumber=1)
+    b = _solver(d, renumber=1)
+    a.set_state(d["state0"])
+    b.set_state(d["state0"])
+    a.run(2)
+    b.run_stages(8)
+    np.testing.assert_array_equal(a.get_state(), b.get_state())
+
+
+def _cavity32(n=32):
+    pm = cases.uniform_box(n, n, n, patch_types=["wall", "wall", "wall", "lid", "wall", "wall"])
+    c = cases.Case(mesh_dir="", X=n, Y=n, Z=n, steps=10, dt=0.18, mach=0.1, reynolds=100,
+                   ref_length=n, bcs=[cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann"),
+                                      cases.BC("lid", 1, 1, 0, 0, "dirichlet", "neumann")])
+    ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
+    return ma, c
+
+
+def test_cavity_32cubed_against_oracle(plfbs_lib):
+    """The 32^3 lid-driven cavity (FP64, Re 100, lid 0.1), 10 steps from rest,
+    renumbered, against the C oracle: relative L2 <= 1e-10 per field."""
+    ma, c = _cavity32()
+    rt, vt, val = cases.bc_arrays(ma, c)
+    T = ma.total_cells
+    s0 = np.zeros((T, 4))
+    s0[:, 3] = 1.0
+    cfg = dict(visc=c.visc, gamma=1.0, dt=c.dt, domain_dt=0.5, pressure_gradient=0.0,
+               channel_height=c.Y, max_velocity=c.mach, ref_rho=1.0, tolerance=0.0,
+               origin=(0, 0, 0), lengths=(c.X, c.Y, c.Z), gradient_mode=0)
+    o = oracle.OracleRun(ma, rt, vt, val, cfg, s0)
+    o.run_steps(10)
+    s = capi.Solver(ma, rt, vt, val, dict(cfg, renumber=1))
+    s.set_state(s0)
+    stats, hist = s.run(10)
+    st = s.get_state()
+    for k in range(4):
+        assert rel_l2(st[:, k], o.state[:, k]) < RUN_TOL, k
+    assert rel_err(hist, o.history) < 1e-10
+
+
+def _channel(nx=128, ny=64, nz=64, d=16.0, nodes=3217):
+    pm = cases.uniform_box(nx, ny, nz, patch_types=["inlet", "outlet", "side", "side",
+                                                    "side", "side"])
+    c = cases.Case(mesh_dir="", X=nx, Y=ny, Z=nz, dt=0.2, mach=0.05, reynolds=100, ref_length=d,
+                   bcs=[cases.BC("inlet", 1, 1, 0, 0, "dirichlet", "neumann"),
+                        cases.BC("outlet", 1, 0, 0, 0, "neumann", "dirichlet"),
+                        cases.BC("side", 1, 0, 0, 0, "neumann", "neumann")])
+    ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
+    pts = cases.fibonacci_sphere(nodes, d / 2, (32.0, 32.0, 32.0))
+    return ma, c, pts
+
+
+def test_conservation_full_size_sphere_channel(plfbs_lib):
+    """128x64x64 channel + 3217-node IBM sphere (the headline case): after one
+    stage, sum_i V_i R_i + sum_boundary F = sum_i V_i f_i exactly up to
+    rounding (interior face fluxes telescope), for mass and momentum."""
+    ma, c, pts = _channel()
+    rt, vt, val = cases.bc_arrays(ma, c)
+    T = ma.total_cells
+    rng = np.random.Generator(np.random.PCG64(5))
+    s0 = np.zeros((T, 4))
+    s0[:, 0] = 0.05 + 0.005 * rng.standard_normal(T)
+    s0[:, 1:3] = 0.005 * rng.standard_normal((T, 2))
+    s0[:, 3] = 1.0 + 0.001 * rng.standard_normal(T)
+    cfg = dict(visc=c.visc, dt=c.dt, max_velocity=c.mach, channel_height=c.Y,
+               lengths=(c.X, c.Y, c.Z), renumber=1)
+    s = capi.Solver(ma, rt, vt, val, cfg, ibm=dict(node_ref=pts, stiffness=0.5, radius=8.0,
+                                                     depth=16.0, object_nodes=len(pts)))
+    s.set_debug(True)
+    s.set_state(s0)
+    s.run_stages(1)
+    R = s.residual()
+    F = s.face_flux()
+    _, _, nf = s.nodes()
+    V = ma.cell_volume[: ma.n_cells]
+    bsum = F[ma.n_internal:].sum(axis=0)
+    vr = (V[:, None] * R).sum(axis=0)
+    scale = np.abs(F).sum(axis=0)
+    # mass: no body force
+    assert abs(vr[3] + bsum[3]) < 1e-12 * scale[3]
+    # momentum: the spread force integrates to the node forces (weights sum to 1 per node)
+    for k in range(3):
+        assert abs(vr[k] + bsum[k] - nf[:, k].sum()) < 1e-11 * scale[k], k
+
+
+def test_divergence_is_reported(plfbs_lib):
+    d = golden_cases.build("cavity")
+    s = _solver(d)
+    st = d["state0"].copy()
+    st[7, 3] = np.nan
+    s.set_state(st)
+    stats, _ = s.run(5)
+    assert stats["rc"] == capi.ERR_DIVERGED
+    assert stats["steps_done"] == 1
+    stats2, _ = s.run(5)  # halted: nothing more runs
+    assert stats2["steps_run"] == 0
+    s.set_state(d["state0"])  # a new state clears the halt
+    stats3, _ = s.run(2)
+    assert stats3["rc"] == 0 and stats3["steps_done"] == 2
