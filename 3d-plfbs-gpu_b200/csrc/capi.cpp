@@ -531,7 +531,9 @@ int plfbs_profile_steps(plfbs_ctx* ctx, int64_t n_steps, double* ms) {
   if (!ctx->have_state || ctx->stages_done != 0)
     return set_err(ctx, PLFBS_ERR_STATE, "profile needs a state at a step boundary");
   for (int k = 0; k < 4; k++) ms[k] = 0.0;
-  cudaEvent_t ev[13];
+  // ev[0] before the IBM kernel, ev[1] after it, ev[2 + 3 rk + j] after kernel j
+  // (gradient, flux, update) of stage rk: 14 events in all
+  cudaEvent_t ev[14];
   for (auto& e : ev) CK(cudaEventCreate(&e));
   const KernelArgs& a = ctx->args;
   const int prec = ctx->cfg.precision;
@@ -547,7 +549,7 @@ int plfbs_profile_steps(plfbs_ctx* ctx, int64_t n_steps, double* ms) {
       plfbs::launch_update(a, prec, rk, ctx->stream);
       CK(cudaEventRecord(ev[4 + 3 * rk], ctx->stream));
     }
-    CK(cudaEventSynchronize(ev[12]));
+    CK(cudaEventSynchronize(ev[13]));
     float x = 0.f;
     CK(cudaEventElapsedTime(&x, ev[0], ev[1]));
     ms[0] += x;

@@ -1,0 +1,294 @@
+// Drop-in body of the reference's GPU solver entry point.
+//
+// Compile this file in the reference's source tree in place of Solver_gpu.cu
+// (plus LBFS.cu, immersed_boundary_method.cu and common_kernels.cu, which it
+// makes unnecessary) and link against libplfbs.so. It keeps the class and the
+// signature that program.cpp calls (Solver_gpu.h:28-31, program.cpp:107-109):
+//
+//   void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh&, Solution&,
+//       Boundary_Conditions&, external_forces&, global_variables&,
+//       domain_geometry&, initial_conditions&, unstructured_bcs&, int mg,
+//       Solution& residual, int fmg, post_processing&,
+//       std::vector<lagrangian_object>&)
+//
+// and reproduces the host side of Solver_gpu.cu:150-917: the marshalling of
+// mesh, boundary conditions and Lagrangian objects (here into the plain views
+// of include/plfbs.h), the time loop with its output every output_step steps
+// (error.txt, console line, Tecplot calls, Solution::output below a decade
+// threshold), the convergence exit with the host post-processing, and
+// soln.clone of the final state. All arithmetic of the time step runs in
+// libplfbs (FP64). Unlike the reference it never calls exit(): a failed
+// library call prints plfbs_last_error() and returns with soln unchanged
+// since the last output. In addition it writes the final state losslessly to
+// <output_file>/state.bin (4 x (n_cells + n_bc) doubles: rho, u, v, w).
+#include <cmath>
+#include <cstdio>
+#include <fstream>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "Solver_gpu.h"
+#include "plfbs.h"
+#include "residuals.h"
+#include "tecplot_output.h"
+
+gpu_solver::gpu_solver() {}
+gpu_solver::~gpu_solver() {}
+
+namespace {
+
+struct Owned {
+  std::vector<int32_t> owner, neighbour, st_off, st_cells, st_faces, rho_type, vel_type;
+  std::vector<double> area, normal, fcen, sdt, vol, ccen, bcval, xref, x;
+};
+
+int gradient_mode(const std::string& s) {
+  // gradients.cpp:259-265
+  if (s == "hybrid") return PLFBS_GRAD_HYBRID;
+  if (s == "LS") return PLFBS_GRAD_LS;
+  return PLFBS_GRAD_GREEN_GAUSS;
+}
+
+void report(plfbs_ctx* ctx, const char* what, int rc) {
+  std::cout << "plfbs: " << what << " failed (" << rc << "): " << plfbs_last_error(ctx)
+            << std::endl;
+}
+
+}  // namespace
+
+void gpu_solver::General_Purpose_Solver_mk_i(
+    unstructured_mesh& Mesh, Solution& soln, Boundary_Conditions& bcs, external_forces& source,
+    global_variables& globals, domain_geometry& domain, initial_conditions& init_conds,
+    unstructured_bcs& quad_bcs_orig, int mg, Solution& residual, int fmg, post_processing& pp,
+    std::vector<lagrangian_object>& object_vec) {
+  (void)source;
+  (void)quad_bcs_orig;
+  const int C = Mesh.get_n_cells(), F = Mesh.get_n_faces(), Fi = Mesh.get_n_neighbours();
+  const int B = Mesh.get_num_bc(), T = Mesh.get_total_cells();
+  Owned o;
+  // --- mesh (Solver_gpu.cu:629-651, with the stencil as CSR) -------------------
+  o.owner.resize(F);
+  o.neighbour.resize(F);
+  o.area.resize(F);
+  o.sdt.resize(F);
+  o.normal.resize(3 * (size_t)F);
+  o.fcen.resize(3 * (size_t)F);
+  for (int f = 0; f < F; f++) {
+    o.owner[f] = Mesh.get_mesh_owner(f);
+    o.neighbour[f] = Mesh.get_mesh_neighbour(f);
+    o.area[f] = Mesh.get_face_area(f);
+    o.sdt[f] = Mesh.get_delta_t_face(f);
+    o.normal[3 * f] = Mesh.get_face_i(f);
+    o.normal[3 * f + 1] = Mesh.get_face_j(f);
+    o.normal[3 * f + 2] = Mesh.get_face_k(f);
+    o.fcen[3 * f] = Mesh.get_face_x(f);
+    o.fcen[3 * f + 1] = Mesh.get_face_y(f);
+    o.fcen[3 * f + 2] = Mesh.get_face_z(f);
+  }
+  o.vol.resize(T);
+  o.ccen.resize(3 * (size_t)T);
+  for (int i = 0; i < T; i++) {
+    o.vol[i] = Mesh.get_cell_volume(i);
+    o.ccen[3 * i] = Mesh.get_centroid_x(i);
+    o.ccen[3 * i + 1] = Mesh.get_centroid_y(i);
+    o.ccen[3 * i + 2] = Mesh.get_centroid_z(i);
+  }
+  o.st_off.assign(1, 0);
+  for (int i = 0; i < C; i++) {
+    for (size_t j = 0; j < Mesh.gradient_cells[i].size(); j++) {
+      o.st_cells.push_back(Mesh.gradient_cells[i][j]);
+      o.st_faces.push_back(Mesh.gradient_faces[i][j]);
+    }
+    o.st_off.push_back((int32_t)o.st_cells.size());
+  }
+  plfbs_mesh_view mv = {C, F, Fi, o.owner.data(), o.neighbour.data(), o.area.data(),
+                        o.normal.data(), o.fcen.data(), o.sdt.data(), o.vol.data(),
+                        o.ccen.data(), o.st_off.data(), o.st_cells.data(), o.st_faces.data()};
+  // --- boundary conditions (Solver_gpu.cu:653-655) -----------------------------
+  o.rho_type.resize(B);
+  o.vel_type.resize(B);
+  o.bcval.resize(4 * (size_t)B);
+  for (int b = 0; b < B; b++) {
+    o.rho_type[b] = bcs.get_rho_type(b);
+    o.vel_type[b] = bcs.get_vel_type(b);
+    o.bcval[4 * b] = bcs.get_u(b);
+    o.bcval[4 * b + 1] = bcs.get_v(b);
+    o.bcval[4 * b + 2] = bcs.get_w(b);
+    o.bcval[4 * b + 3] = bcs.get_rho(b);
+  }
+  plfbs_bc_view bv = {o.rho_type.data(), o.vel_type.data(), o.bcval.data()};
+  // --- Lagrangian objects (Solver_gpu.cu:1469-1499) ---------------------------
+  int N = 0;
+  for (auto& obj : object_vec) N += obj.num_nodes;
+  o.xref.resize(3 * (size_t)N);
+  o.x.resize(3 * (size_t)N);
+  {
+    int n = 0;
+    for (auto& obj : object_vec)
+      for (int j = 0; j < obj.num_nodes; j++, n++) {
+        o.xref[3 * n] = obj.node_x_ref[j];
+        o.xref[3 * n + 1] = obj.node_y_ref[j];
+        o.xref[3 * n + 2] = obj.node_z_ref[j];
+        o.x[3 * n] = obj.node_x[j];
+        o.x[3 * n + 1] = obj.node_y[j];
+        o.x[3 * n + 2] = obj.node_z[j];
+      }
+  }
+  plfbs_ibm_view iv = {N, o.xref.data(), o.x.data(), 0.0, 0.0, 0.0, 0};
+  if (!object_vec.empty()) {
+    iv.stiffness = object_vec[0].stiffness;
+    iv.radius = object_vec[0].radius;
+    iv.depth = object_vec[0].depth;
+    iv.object_nodes = object_vec[0].num_nodes;
+  }
+  plfbs_config cfg = {};
+  cfg.visc = globals.visc;
+  cfg.gamma = globals.pre_conditioned_gamma;
+  cfg.time_marching_step = globals.time_marching_step;
+  cfg.domain_dt = domain.dt;
+  cfg.max_velocity = globals.max_velocity;
+  cfg.ref_rho = globals.ref_rho;
+  cfg.tolerance = globals.tolerance;
+  cfg.pressure_gradient = init_conds.pressure_gradient;
+  cfg.channel_height = domain.Y;
+  cfg.origin[0] = domain.origin_x;
+  cfg.origin[1] = domain.origin_y;
+  cfg.origin[2] = domain.origin_z;
+  cfg.lengths[0] = domain.X;
+  cfg.lengths[1] = domain.Y;
+  cfg.lengths[2] = domain.Z;
+  cfg.gradient_mode = gradient_mode(globals.gradient_calc_type);
+  cfg.precision = PLFBS_FP64;
+  cfg.renumber = 1;
+
+  plfbs_ctx* ctx = nullptr;
+  int rc = plfbs_create(&cfg, &mv, &bv, &iv, 0, &ctx);
+  if (rc) {
+    report(nullptr, "plfbs_create", rc);
+    return;
+  }
+  std::vector<double> rho(T), u(T), v(T), w(T);
+  for (int i = 0; i < T; i++) {  // soln_to_double, Solver_gpu.cu:1646-1659
+    rho[i] = soln.get_rho(i);
+    u[i] = soln.get_u(i);
+    v[i] = soln.get_v(i);
+    w[i] = soln.get_w(i);
+  }
+  auto pull = [&]() {  // soln.clone(temp_soln)
+    if (plfbs_get_state(ctx, rho.data(), u.data(), v.data(), w.data(), T) == PLFBS_OK)
+      for (int i = 0; i < T; i++) soln.update(rho[i], u[i], v[i], w[i], i);
+  };
+  rc = plfbs_set_state(ctx, rho.data(), u.data(), v.data(), w.data(), T);
+  if (rc) {
+    report(ctx, "plfbs_set_state", rc);
+    plfbs_destroy(ctx);
+    return;
+  }
+
+  std::ofstream error_output((globals.output_file + "/error.txt").c_str(), std::ios::out);
+  tecplot_output<double> tecplot;
+  Solution residual_worker(T);
+  gradients grads(T);
+  grads.pre_fill_LHS_and_RHS_matrix(bcs, Mesh, domain, soln, globals);  // for post-processing
+  Solution wall_shear_stress(Mesh.get_n_wall_cells());
+  std::vector<double> delta_t_local(C, globals.time_marching_step), local_fneq(T, 0.0);
+  std::vector<double> nx(3 * (size_t)N), nvel(3 * (size_t)N), nforce(3 * (size_t)N);
+  auto node_arrays = [&](std::vector<double>& a, int c) {
+    std::vector<double> r(N);
+    for (int n = 0; n < N; n++) r[n] = a[3 * n + c];
+    return r;
+  };
+  auto output_objects = [&](double t) {
+    if (N == 0 || object_vec.empty()) return;
+    plfbs_get_nodes(ctx, nx.data(), nvel.data(), nforce.data(), N);
+    auto vx = node_arrays(nvel, 0), vy = node_arrays(nvel, 1), vz = node_arrays(nvel, 2);
+    auto px = node_arrays(nx, 0), py = node_arrays(nx, 1), pz = node_arrays(nx, 2);
+    auto fx = node_arrays(nforce, 0), fy = node_arrays(nforce, 1), fz = node_arrays(nforce, 2);
+    tecplot.tecplot_output_lagrangian_object_gpu(
+        vx.data(), vy.data(), vz.data(), px.data(), py.data(), pz.data(), fx.data(), fy.data(),
+        fz.data(), globals, domain, t, object_vec[0].name, object_vec[0].num_nodes,
+        object_vec[0].depth_nodes, object_vec[0].radial_nodes);
+  };
+
+  const long long timesteps = (long long)std::ceil(globals.simulation_length);
+  const double delta_t = globals.time_marching_step;
+  const int out_step = globals.output_step > 0 ? globals.output_step : 1;
+  double output_residual_threshold = 0;
+  std::vector<double> hist;
+  long long t = 0;
+  bool converged = false;
+  while (t < timesteps) {
+    // run up to and including the next output step (t % output_step == 1)
+    long long next = t;
+    while (next < timesteps - 1 && !(mg == 0 && next % out_step == 1)) next++;
+    const long long n = next - t + 1;
+    hist.assign(6 * (size_t)n, 0.0);
+    plfbs_stats st;
+    rc = plfbs_run(ctx, n, &st, hist.data());
+    if (rc && rc != PLFBS_ERR_DIVERGED) {
+      report(ctx, "plfbs_run", rc);
+      break;
+    }
+    const long long ran = st.steps_run;
+    const long long last = t + ran - 1;
+    const double max_error = st.max_error;
+    if (mg == 0 && last % out_step == 1 && ran > 0) {  // Solver_gpu.cu:844-868
+      pull();
+      error_output << last << ", " << max_error << ", " << st.rho_rms << ", " << st.u_rms << ", "
+                   << st.v_rms << ", " << st.w_rms << " , FMG cycle: " << fmg << std::endl;
+      std::cout << "time t=" << last * delta_t << " error e =" << max_error
+                << " delta_t:" << delta_t << std::endl;
+      if (max_error < std::pow(10, output_residual_threshold)) {
+        tecplot.tecplot_output_unstructured_soln(globals, Mesh, soln, bcs, last, pp,
+                                                 residual_worker, delta_t_local.data(),
+                                                 local_fneq.data());
+        output_objects(last);
+        output_residual_threshold = output_residual_threshold - 1;
+        soln.output(globals.output_file, globals, domain);
+      }
+    }
+    t += ran;
+    if (rc == PLFBS_ERR_DIVERGED) {
+      report(ctx, "time step", rc);
+      break;
+    }
+    if (st.converged) {  // Solver_gpu.cu:870-895
+      converged = true;
+      break;
+    }
+    if (ran < n) break;
+  }
+  pull();
+  error_output.close();
+  if (converged) {
+    if (mg == 0) {
+      std::cout << "convergence" << std::endl;
+      std::cout << "time t=" << (t - 1) * delta_t << std::endl;
+      soln.update_unstructured_bcs(bcs, Mesh, domain, (int)(t - 1));
+      grads.Get_LS_Gradients(bcs, Mesh, domain, soln, globals);
+      pp.cylinder_post_processing(Mesh, globals, grads, bcs, soln, domain, wall_shear_stress);
+      tecplot.tecplot_output_unstructured_soln(globals, Mesh, soln, bcs, t - 1, pp,
+                                               residual_worker, delta_t_local.data(),
+                                               local_fneq.data());
+      output_objects((double)timesteps);
+    }
+  } else {
+    std::cout << "out of time" << std::endl;
+    pp.cylinder_post_processing(Mesh, globals, grads, bcs, soln, domain, wall_shear_stress);
+    tecplot.tecplot_output_unstructured_soln(globals, Mesh, soln, bcs, timesteps, pp,
+                                             residual_worker, delta_t_local.data(),
+                                             local_fneq.data());
+    output_objects((double)timesteps);
+  }
+  // lossless checkpoint of the final state (the text output keeps 6 digits)
+  if (FILE* f = std::fopen((globals.output_file + "/state.bin").c_str(), "wb")) {
+    std::fwrite(rho.data(), sizeof(double), T, f);
+    std::fwrite(u.data(), sizeof(double), T, f);
+    std::fwrite(v.data(), sizeof(double), T, f);
+    std::fwrite(w.data(), sizeof(double), T, f);
+    std::fclose(f);
+  }
+  (void)residual;
+  plfbs_destroy(ctx);
+}

@@ -24,6 +24,7 @@ from the reference sources) on the same mesh and boundary conditions.
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import os
 import statistics
@@ -225,7 +226,12 @@ def run_reference_arm(args, rank, world):
 # our arm
 # ---------------------------------------------------------------------------
 
+def log(msg):
+    print("[bench] %s" % msg, file=sys.stderr, flush=True)
+
+
 def main():
+    faulthandler.enable()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
@@ -255,6 +261,7 @@ def main():
 
     pm, c, ma, nodes, state0 = build_case()
     rt, vt, val = cases.bc_arrays(ma, c)
+    log("case built: %d cells, %d faces" % (ma.n_cells, ma.n_faces))
     solver = capi.Solver(ma, rt, vt, val, solver_cfg(c), ibm=ibm_cfg(nodes), device=local_rank)
 
     def barrier():
@@ -269,6 +276,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    log("solver created")
     # warm-up
     solver.set_state(state0)
     st, _ = solver.run(args.warmup, history=False)
@@ -283,8 +291,10 @@ def main():
     ms = max_over_ranks(st["kernel_ms"])
     value = world * ma.n_cells * args.steps / (ms / 1e3) / 1e6
 
+    log("timed run: %.3f ms for %d steps" % (ms, args.steps))
     # per-kernel device times (CUDA events between launches on the solver's stream)
     prof = solver.profile_steps(args.profile_steps)
+    log("profile: %r" % prof)
     per_launch = {"ibm": prof["ibm"] / args.profile_steps,
                   "gradient": prof["gradient"] / (4 * args.profile_steps),
                   "flux": prof["flux"] / (4 * args.profile_steps),
@@ -328,6 +338,7 @@ def main():
     else:
         solver.close()
 
+    log("e2e: %r" % e2e)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, sample = reference_cpu_throughput(pm, c, nodes, sample_steps=1)
