@@ -76,16 +76,18 @@ __device__ __forceinline__ d4 ghost_state(const d4& q, const d4& tgt, int types)
 // Gradient layout: 3 x d4 per cell = (rx, ry, rz, ux), (uy, uz, vx, vy),
 // (vz, wx, wy, wz).
 // ---------------------------------------------------------------------------
+// One thread per cell walking its stencil slots. (Loading all slots up front
+// needs ~100 registers and measured slower than this 62-register loop.)
 __global__ void __launch_bounds__(kBlock) k_gradient(const KernelArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.C || halted(a)) return;
   const d4 qi = ld4(a.state, i);
-  double g[12];
-#pragma unroll
-  for (int k = 0; k < 12; k++) g[k] = 0.0;
   const double* wx = static_cast<const double*>(a.st_wx);
   const double* wy = static_cast<const double*>(a.st_wy);
   const double* wz = static_cast<const double*>(a.st_wz);
+  double g[12];
+#pragma unroll
+  for (int k = 0; k < 12; k++) g[k] = 0.0;
   for (int k = 0; k < a.K; k++) {
     const long long s = (long long)k * a.C + i;
     const int j = __ldg(a.st_nbr + s);
@@ -98,7 +100,7 @@ __global__ void __launch_bounds__(kBlock) k_gradient(const KernelArgs a) {
       const d4 tgt = ld4(a.bc1, b);
       const int types = (int)__ldg(reinterpret_cast<const double*>(a.bc3) + 4LL * b + 3);
       qj = ghost_state(qi, tgt, types);
-      st4(a.state, j, qj);  // ghost states are read back by get_state
+      st4(a.state, j, qj);
     }
     const double w[3] = {__ldg(wx + s), __ldg(wy + s), __ldg(wz + s)};
     const double d[4] = {qj.w - qi.w, qj.x - qi.x, qj.y - qi.y, qj.z - qi.z};
@@ -212,7 +214,7 @@ __device__ __forceinline__ void lattice_pair(const double si[4], const double sn
 // The face flux is (momentum, mass) = ((sum e e^T f) n, (sum e f) . n) A.
 // A boundary face (neighbour > n_cells in the reference) takes both sides from
 // the boundary value and all gradients from the ghost (LBFS.cu:356-401).
-__global__ void __launch_bounds__(kBlock) k_flux(const KernelArgs a) {
+__global__ void __launch_bounds__(kFluxBlock, 4) k_flux(const KernelArgs a) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= a.F || halted(a)) return;
   const d4 f0 = ld4(a.face0, f), f1 = ld4(a.face1, f), f2 = ld4(a.face2, f);
@@ -308,7 +310,8 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-template <int RK>
+// K2MAX: face slots the launch is specialised for (0 = any count, looped).
+template <int RK, int K2MAX>
 __global__ void __launch_bounds__(kBlock) k_update(const KernelArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (halted(a)) return;  // uniform across the launch
@@ -318,14 +321,33 @@ __global__ void __launch_bounds__(kBlock) k_update(const KernelArgs a) {
   bool bad = false;
   if (i < a.C) {
     double r[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int k = 0; k < a.K2; k++) {
-      const int e = __ldg(a.gather + (long long)k * a.C + i);
-      if (e < 0) break;
-      const d4 fl = ld4(a.flux, e >> 1);
-      if (e & 1) {
-        r[0] += fl.x; r[1] += fl.y; r[2] += fl.z; r[3] += fl.w;
-      } else {
-        r[0] -= fl.x; r[1] -= fl.y; r[2] -= fl.z; r[3] -= fl.w;
+    if (K2MAX > 0) {
+      int e[K2MAX > 0 ? K2MAX : 1];
+#pragma unroll
+      for (int k = 0; k < K2MAX; k++) e[k] = (k < a.K2) ? __ldg(a.gather + (long long)k * a.C + i) : -1;
+      d4 fl[K2MAX > 0 ? K2MAX : 1];
+#pragma unroll
+      for (int k = 0; k < K2MAX; k++)
+        if (e[k] >= 0) fl[k] = ld4(a.flux, e[k] >> 1);
+#pragma unroll
+      for (int k = 0; k < K2MAX; k++) {
+        if (e[k] < 0) continue;
+        const double sg = (e[k] & 1) ? 1.0 : -1.0;
+        r[0] = fma(sg, fl[k].x, r[0]);
+        r[1] = fma(sg, fl[k].y, r[1]);
+        r[2] = fma(sg, fl[k].z, r[2]);
+        r[3] = fma(sg, fl[k].w, r[3]);
+      }
+    } else {
+      for (int k = 0; k < a.K2; k++) {
+        const int e = __ldg(a.gather + (long long)k * a.C + i);
+        if (e < 0) break;
+        const d4 fl = ld4(a.flux, e >> 1);
+        const double sg = (e & 1) ? 1.0 : -1.0;
+        r[0] = fma(sg, fl.x, r[0]);
+        r[1] = fma(sg, fl.y, r[1]);
+        r[2] = fma(sg, fl.z, r[2]);
+        r[3] = fma(sg, fl.w, r[3]);
       }
     }
     const double iv = __ldg(static_cast<const double*>(a.inv_volume) + i);
@@ -402,15 +424,28 @@ __global__ void __launch_bounds__(kBlock) k_update(const KernelArgs a) {
   __syncthreads();
   if (!last) return;
   __threadfence();
-  // final pass: thread c < 4 sums component c over the blocks
+  // final pass: every thread sums a fixed strided subset of the block
+  // partials, then the same warp/block tree as above (deterministic order)
   __shared__ double tot[4];
-  if (threadIdx.x < 4) {
-    const volatile double* p = a.partial;
-    double v = 0.0;
-    for (int b = 0; b < (int)gridDim.x; b++) v += p[4LL * b + threadIdx.x];
-    tot[threadIdx.x] = v;
+  {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+      for (int c = 0; c < 4; c++) v[c] += __ldcg(a.partial + 4LL * b + c);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const double w = warp_sum(v[c]);
+      if (lane == 0) red[warp][c] = w;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      double t = 0.0;
+      for (int w = 0; w < kBlock / 32; w++) t += red[w][threadIdx.x];
+      tot[threadIdx.x] = t;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   if (threadIdx.x == 0) {
     DevStats* st = a.stats;
     const double nC = (double)a.C;
@@ -557,16 +592,27 @@ void launch_gradient(const KernelArgs& a, int precision, cudaStream_t s) {
 }
 void launch_flux(const KernelArgs& a, int precision, cudaStream_t s) {
   (void)precision;
-  k_flux<<<blocks_for(a.F, kBlock), kBlock, 0, s>>>(a);
+  k_flux<<<blocks_for(a.F, kFluxBlock), kFluxBlock, 0, s>>>(a);
+}
+template <int RK>
+static void launch_update_rk(const KernelArgs& a, int nb, cudaStream_t s) {
+  if (a.K2 <= 4)
+    k_update<RK, 4><<<nb, kBlock, 0, s>>>(a);
+  else if (a.K2 <= 6)
+    k_update<RK, 6><<<nb, kBlock, 0, s>>>(a);
+  else if (a.K2 <= 8)
+    k_update<RK, 8><<<nb, kBlock, 0, s>>>(a);
+  else
+    k_update<RK, 0><<<nb, kBlock, 0, s>>>(a);
 }
 void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t s) {
   (void)precision;
   const int nb = blocks_for(a.C, kBlock);
   switch (rk) {
-    case 0: k_update<0><<<nb, kBlock, 0, s>>>(a); break;
-    case 1: k_update<1><<<nb, kBlock, 0, s>>>(a); break;
-    case 2: k_update<2><<<nb, kBlock, 0, s>>>(a); break;
-    default: k_update<3><<<nb, kBlock, 0, s>>>(a); break;
+    case 0: launch_update_rk<0>(a, nb, s); break;
+    case 1: launch_update_rk<1>(a, nb, s); break;
+    case 2: launch_update_rk<2>(a, nb, s); break;
+    default: launch_update_rk<3>(a, nb, s); break;
   }
 }
 void launch_seed(const KernelArgs& a, int precision, cudaStream_t s) {

@@ -73,7 +73,8 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
 // ---------------------------------------------------------------------------
 
 constexpr int kHistoryCap = 4096;   // per-step residual records kept on the device
-constexpr int kBlock = 256;         // threads per block of the cell/face kernels
+constexpr int kBlock = 256;         // threads per block of the cell kernels
+constexpr int kFluxBlock = 128;     // threads per block of the face-flux kernel (128 registers, 4 blocks/SM)
 
 // Run status shared by all kernels of a step, in device memory.
 struct DevStats {
