@@ -17,7 +17,7 @@
  * Everything else follows the reference formula by formula, including its
  * quirks: the strict ghost test neighbour > n_cells (LBFS.cu:356), the
  * determinant typo (gradients.cpp:282-284), RK alpha = {1, .5, .5, 1}
- * (LBFS.cu:1468), the +-0.001 dt dead band (LBFS.cu:353-354) and the Neumann
+ * (LBFS.cu:1467), the +-0.001 dt dead band (LBFS.cu:353-354) and the Neumann
  * ghost gradient g (1 - |n|) (LBFS.cu:1366-1368).
  *
  * State layout: 4 doubles per cell (u, v, w, rho), cells then ghosts.
