@@ -136,6 +136,8 @@ int check_ctx(plfbs_ctx* ctx) {
 
 }  // namespace
 
+void plfbs::set_global_error(const std::string& m) { g_err = m; }
+
 extern "C" {
 
 const char* plfbs_version(void) { return kVersion; }

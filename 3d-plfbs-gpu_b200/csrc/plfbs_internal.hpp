@@ -64,6 +64,9 @@ struct Layout {
 int ls_weights(const plfbs_mesh_view& m, int mode, double* lhs_inv, double* rhs,
                std::string& err);
 
+// The error string plfbs_last_error(NULL) returns (capi.cpp).
+void set_global_error(const std::string& m);
+
 // Validate the views and build the device layout.
 int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bc,
                  Layout& L, std::string& err);

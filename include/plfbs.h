@@ -178,6 +178,27 @@ int plfbs_profile_steps(plfbs_ctx* ctx, int64_t n_steps, double* ms);
 /* Device bytes held by the context. */
 int plfbs_memory_bytes(plfbs_ctx* ctx, int64_t* bytes);
 
+/* Residual norms with no device allocation. No counterpart in the reference.
+ * For callers that cannot let a library call cudaMalloc while they run: an
+ * application under a fixed device-memory budget that reserves everything at
+ * start-up (an allocation mid-run may fail, and cudaMalloc may synchronise the
+ * device), or a host framework whose caching allocator must own all device
+ * memory. From residuals the caller keeps in device memory ([4 n_cells]:
+ * u, v, w, rho per cell, as plfbs_get_residual lays them out) it writes
+ * out[5] = {max_error, rho_rms, u_rms, v_rms, w_rms} (device memory) with the
+ * normalisation of plfbs_run's last RK stage (residuals.cpp:95-147),
+ * asynchronously on `stream` (a cudaStream_t, NULL for the default stream).
+ * Its only scratch is a file-scope __device__ array of 65,792 bytes (2048
+ * block partials + a counter) that every GPU loading this library holds until
+ * exit, so n_cells is limited to 8,388,608; larger inputs are rejected with
+ * PLFBS_ERR_ARG. The first call on each device looks up that array's device
+ * address with cudaGetSymbolAddress; make that first call before any stream
+ * capture. All calls share the array: calls that overlap on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller.
+ * Errors are reported through plfbs_last_error(NULL). */
+int plfbs_residual_norms_noalloc(const double* residual, int64_t n_cells, double ref_rho,
+                                 double max_velocity, double* out, void* stream);
+
 const char* plfbs_last_error(const plfbs_ctx* ctx);  /* ctx may be NULL: global error */
 void plfbs_destroy(plfbs_ctx* ctx);
 const char* plfbs_version(void);
