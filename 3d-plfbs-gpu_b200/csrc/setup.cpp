@@ -92,8 +92,9 @@ int ls_weights(const plfbs_mesh_view& m, int mode, double* lhs_inv, double* rhs,
       max_disp = std::max(std::sqrt(dx * dx + dy * dy + dz * dz), max_disp);
     }
     const double aspect = 2 * std::fabs(max_disp) * max_area / m.cell_volume[i];
-    const double beta = mode == PLFBS_GRAD_HYBRID ? std::min(1.0, 2 / aspect)
-                        : mode == PLFBS_GRAD_LS  ? 1.0
+    const int base = mode & 0xff;
+    const double beta = base == PLFBS_GRAD_HYBRID ? std::min(1.0, 2 / aspect)
+                        : base == PLFBS_GRAD_LS  ? 1.0
                                                  : 0.0;
     L[0] = L[0] + 2 * (1 - beta) * m.cell_volume[i];
     L[4] = L[4] + 2 * (1 - beta) * m.cell_volume[i];
@@ -122,7 +123,9 @@ int ls_weights(const plfbs_mesh_view& m, int mode, double* lhs_inv, double* rhs,
     }
     const double a = L[0], b = L[1], c = L[2], dd = L[3], e = L[4], f = L[5], g = L[6],
                  h = L[7], k = L[8];
-    const double det = a * (e * k - f * h) + b * (dd * k - f - g) + c * (dd * h - e * g);
+    const double det = (mode & PLFBS_GRAD_EXACT_INVERSE)
+                           ? a * (e * k - f * h) - b * (dd * k - f * g) + c * (dd * h - e * g)
+                           : a * (e * k - f * h) + b * (dd * k - f - g) + c * (dd * h - e * g);
     double* o = lhs_inv + 9 * (size_t)i;
     o[0] = 1 / det * (e * k - f * h);
     o[1] = 1 / det * (c * h - b * k);

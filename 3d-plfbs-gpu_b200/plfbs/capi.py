@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(PKG, "_lib", "libplfbs.so")
 
 OK, ERR_ARG, ERR_MESH, ERR_BC, ERR_CUDA, ERR_DIVERGED, ERR_NO_DEVICE, ERR_STATE = (
     0, -1, -2, -3, -4, -5, -6, -7)
-GRAD_LS, GRAD_HYBRID, GRAD_GREEN_GAUSS = 0, 1, 2
+GRAD_LS, GRAD_HYBRID, GRAD_GREEN_GAUSS, GRAD_EXACT_INVERSE = 0, 1, 2, 0x100
 FP64, FP32_DEVIATION = 0, 1
 
 _dp = C.POINTER(C.c_double)

@@ -40,8 +40,19 @@ enum {
   PLFBS_ERR_STATE = -7        /* call out of order */
 };
 
-/* Gradient weighting, gradients.cpp:259-265 ("LS", "hybrid", anything else = GG). */
-enum { PLFBS_GRAD_LS = 0, PLFBS_GRAD_HYBRID = 1, PLFBS_GRAD_GREEN_GAUSS = 2 };
+/* Gradient weighting, gradients.cpp:259-265 ("LS", "hybrid", anything else = GG).
+ * OR-ing PLFBS_GRAD_EXACT_INVERSE inverts the LS matrix with the true
+ * determinant instead of the one gradients.cpp:282-284 computes (which drops a
+ * product and a sign in its second term). The two agree when the matrix has no
+ * xy/yx coupling (axis-aligned hexes); on skewed or tetrahedral cells the
+ * as-written determinant can flip the sign of the inverse and the scheme
+ * diverges. Default (flag clear): the reference's arithmetic. */
+enum {
+  PLFBS_GRAD_LS = 0,
+  PLFBS_GRAD_HYBRID = 1,
+  PLFBS_GRAD_GREEN_GAUSS = 2,
+  PLFBS_GRAD_EXACT_INVERSE = 0x100
+};
 
 /* Arithmetic of the time step. */
 enum {
@@ -103,7 +114,7 @@ typedef struct {
   double channel_height;      /* domain.Y (parabolic inlet, LBFS.cu:1286) */
   double origin[3];           /* domain.origin_x/y/z */
   double lengths[3];          /* domain.X/Y/Z */
-  int32_t gradient_mode;      /* PLFBS_GRAD_* */
+  int32_t gradient_mode;      /* PLFBS_GRAD_*, optionally | PLFBS_GRAD_EXACT_INVERSE */
   int32_t precision;          /* PLFBS_FP64 or PLFBS_FP32_DEVIATION */
   int32_t renumber;           /* 1: reorder cells (RCM) and faces for locality */
   int32_t reserved;

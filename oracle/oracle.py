@@ -106,7 +106,7 @@ class OracleRun:
         self._keep = []
         self.ma = ma
         C_, F, B = ma.n_cells, ma.n_faces, ma.n_bc
-        self.lhs, self.rhs = ls_weights(ma, int(cfg.get("gradient_mode", 0)))
+        self.lhs, self.rhs = ls_weights(ma, int(cfg.get("gradient_mode", 0)))  # | 0x100: exact
         p = _Problem()
         p.n_cells, p.n_faces, p.n_internal = C_, F, ma.n_internal
 

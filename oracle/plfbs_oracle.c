@@ -74,7 +74,8 @@ static double wgt(int k) { return k == 0 ? W0 : (k < 7 ? W1 : W7); }
 /* -------------------------------------------------------------------------
  * Least-squares weights, gradients.cpp:214-313 (beta_0 by mode, LHS/RHS
  * contributions :149-210, inverse by cofactors with the reference's
- * determinant typo :282-284). mode: 0 = LS, 1 = hybrid, 2 = Green-Gauss.
+ * determinant typo :282-284). mode: 0 = LS, 1 = hybrid, 2 = Green-Gauss;
+ * | 0x100 uses the true determinant instead (an extension for skewed cells).
  * ------------------------------------------------------------------------- */
 int oracle_ls_weights(int n_cells, const int *off, const int *st_cells, const int *st_faces,
                       const int *owner, const double *face_area, const double *face_normal,
@@ -94,9 +95,9 @@ int oracle_ls_weights(int n_cells, const int *off, const int *st_cells, const in
     }
     double aspect = 2 * fabs(max_disp) * max_area / cell_volume[i];
     double beta;
-    if (mode == 1)
+    if ((mode & 0xff) == 1)
       beta = (2 / aspect) < 1.0 ? (2 / aspect) : 1.0;
-    else if (mode == 0)
+    else if ((mode & 0xff) == 0)
       beta = 1.0;
     else
       beta = 0.0;
@@ -138,9 +139,13 @@ int oracle_ls_weights(int n_cells, const int *off, const int *st_cells, const in
       }
     }
     /* the reference's determinant, typo included: (yz - zx) where the
-       cofactor expansion has -(yx zz - yz zx) */
-    double det = L[0] * (L[4] * L[8] - L[5] * L[7]) + L[1] * (L[3] * L[8] - L[5] - L[6]) +
-                 L[2] * (L[3] * L[7] - L[4] * L[6]);
+       cofactor expansion has -(yx zz - yz zx); mode bit 0x100 asks for the
+       true determinant */
+    double det = (mode & 0x100)
+                     ? L[0] * (L[4] * L[8] - L[5] * L[7]) - L[1] * (L[3] * L[8] - L[5] * L[6]) +
+                           L[2] * (L[3] * L[7] - L[4] * L[6])
+                     : L[0] * (L[4] * L[8] - L[5] * L[7]) + L[1] * (L[3] * L[8] - L[5] - L[6]) +
+                           L[2] * (L[3] * L[7] - L[4] * L[6]);
     double a = L[0], b = L[1], c = L[2], d = L[3], e_ = L[4], f_ = L[5], g = L[6], h = L[7],
            k = L[8];
     double *o = lhs_inv + 9 * i;

@@ -34,8 +34,11 @@ def write_restart(out_dir, state):
             f.write("".join("%d ,%.17g\n" % (i, v) for i, v in enumerate(state[:, k])))
 
 
-def run_reference(workdir, pm, case, nodes=None, init_state=None, dump=True, timeout=600):
-    """Write ``pm``/``case`` under ``workdir``, run the reference, return dumps."""
+def run_reference(workdir, pm, case, nodes=None, init_state=None, dump=True, timeout=600,
+                  binary=None):
+    """Write ``pm``/``case`` under ``workdir``, run the reference program (or
+    ``binary``, another build of it), return the .npy dumps it wrote."""
+    binary = binary or REF_BIN
     workdir = os.path.abspath(workdir)
     os.makedirs(workdir, exist_ok=True)
     mesh_dir = os.path.join(workdir, "polyMesh")
@@ -54,7 +57,7 @@ def run_reference(workdir, pm, case, nodes=None, init_state=None, dump=True, tim
         steps, restart = case.steps, case.restart
         case.steps, case.restart = 0, False
         cases.write_xml(xml, case)
-        subprocess.run([REF_BIN, xml], cwd=workdir, env=env, check=True,
+        subprocess.run([binary, xml], cwd=workdir, env=env, check=True,
                        stdout=subprocess.DEVNULL, timeout=timeout)
         outs = [d for d in glob.glob(os.path.join(workdir, "out", "*")) if os.path.isdir(d)]
         assert len(outs) == 1, outs
@@ -65,7 +68,7 @@ def run_reference(workdir, pm, case, nodes=None, init_state=None, dump=True, tim
     os.makedirs(dump_dir, exist_ok=True)
     if dump:
         env["PLFBS_REF_DUMP"] = dump_dir
-    subprocess.run([REF_BIN, xml], cwd=workdir, env=env, check=True,
+    subprocess.run([binary, xml], cwd=workdir, env=env, check=True,
                    stdout=subprocess.DEVNULL, timeout=timeout)
     return {os.path.splitext(os.path.basename(p))[0]: np.load(p)
             for p in glob.glob(os.path.join(dump_dir, "*.npy"))}

@@ -98,3 +98,54 @@ def test_null_context_calls_fail_cleanly(plfbs_lib):
     assert plfbs_lib.plfbs_run_stages(None, 1) == capi.ERR_ARG
     assert plfbs_lib.plfbs_set_debug(None, 1) == capi.ERR_ARG
     plfbs_lib.plfbs_destroy(None)
+
+
+def _tets(n=4, seed=3):
+    pm = cases.jittered_tet_box(n, jitter=0.2, seed=seed,
+                                patch_types=["wall", "wall", "wall", "lid", "wall", "wall"])
+    c = cases.Case(mesh_dir="", X=n, Y=n, Z=n, dt=0.02, mach=0.1, reynolds=100, ref_length=n,
+                   bcs=[cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann"),
+                        cases.BC("lid", 1, 1, 0, 0, "dirichlet", "neumann")])
+    return cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min), c
+
+
+def test_tet_mesh_is_valid():
+    """Jittered hexes split into 6 tets: conforming, positive, closed cells."""
+    ma, c = _tets()
+    V = ma.cell_volume[: ma.n_cells]
+    assert V.min() > 0 and abs(V.sum() - 64.0) < 1e-9
+    assert set(np.diff(ma.stencil_offsets)) == {4}
+    nA = ma.face_normal * ma.face_area[:, None]
+    acc = np.zeros((ma.n_cells, 3))
+    np.add.at(acc, ma.owner, nA)
+    np.add.at(acc, ma.neighbour[: ma.n_internal], -nA[: ma.n_internal])
+    assert np.abs(acc).max() < 1e-12
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_exact_inverse_option(plfbs_lib, mode):
+    """PLFBS_GRAD_EXACT_INVERSE: the true inverse of the LS matrix; without it
+    the reference's determinant (which flips sign on some tets)."""
+    import oracle
+
+    ma, _ = _tets()
+    lhs_x, rhs_x = capi.ls_weights(ma, mode | capi.GRAD_EXACT_INVERSE)
+    lo, ro = oracle.ls_weights(ma, mode | 0x100)
+    np.testing.assert_array_equal(lhs_x, lo)
+    np.testing.assert_array_equal(rhs_x, ro)
+    lhs_r, _ = capi.ls_weights(ma, mode)
+    lr, _ = oracle.ls_weights(ma, mode)
+    np.testing.assert_array_equal(lhs_r, lr)
+    # the exact inverse inverts the LHS rebuilt from the same formula
+    C = ma.n_cells
+    for i in range(0, C, 37):
+        L = np.zeros((3, 3))
+        e0, e1 = ma.stencil_offsets[i], ma.stencil_offsets[i + 1]
+        for e in range(e0, e1):
+            f, i1 = ma.stencil_faces[e], ma.stencil_cells[e]
+            d = ma.cell_centroid[i1] - ma.cell_centroid[i]
+            ln = (ma.face_centroid[f] - ma.cell_centroid[i]) @ ma.face_normal[f]
+            w = (2 * ln / (d @ ma.face_normal[f])) ** 2 * ma.face_area[f] / np.sqrt(d @ d)
+            L += w * np.outer(d, d)
+        if mode == 0:
+            np.testing.assert_allclose(lhs_x[i] @ L, np.eye(3), atol=1e-12)

@@ -1,0 +1,39 @@
+"""The drop-in: the reference program itself, with its GPU solver replaced by
+the shim (3d-plfbs-gpu_b200/shim) over libplfbs, against the golden dumps of
+the reference's own kernels. Needs oracle/_ref/plfbs_ref_b200 (built from the
+reference sources by `make -C oracle/ref integration`); skipped without it."""
+
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import golden_cases
+import refrun
+from conftest import REPO, load_golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+BIN = os.path.join(REPO, "oracle", "_ref", "plfbs_ref_b200")
+
+
+@pytest.mark.parametrize("name", ["cavity", "channel", "converge"])
+def test_reference_program_with_plfbs(tmp_path, name):
+    if not os.path.exists(BIN):
+        pytest.skip("oracle/_ref/plfbs_ref_b200 not built (needs the reference sources)")
+    d = golden_cases.build(name)
+    g = load_golden(name)
+    refrun.run_reference(str(tmp_path), d["pm"], d["case"], nodes=d["nodes"],
+                         init_state=d["state0"], dump=False, binary=BIN)
+    paths = glob.glob(os.path.join(str(tmp_path), "out", "*", "state.bin"))
+    assert len(paths) == 1, paths
+    T = d["ma"].total_cells
+    raw = np.fromfile(paths[0], dtype=np.float64).reshape(4, T)  # rho, u, v, w
+    state = np.stack([raw[1], raw[2], raw[3], raw[0]], axis=1)
+    for k in range(4):
+        assert rel_l2(state[:, k], g["final_state"][:, k]) < 1e-10, k
+    # the reference's 6-significant-digit text output agrees too
+    u_txt = glob.glob(os.path.join(str(tmp_path), "out", "*", "u.txt"))[0]
+    u = np.loadtxt(u_txt, delimiter=",")[:, 1]
+    np.testing.assert_allclose(u, g["final_state"][:, 0], rtol=1e-5, atol=1e-9)

@@ -179,3 +179,37 @@ def test_divergence_is_reported(plfbs_lib):
     s.set_state(d["state0"])  # a new state clears the halt
     stats3, _ = s.run(2)
     assert stats3["rc"] == 0 and stats3["steps_done"] == 2
+
+
+def _tet_case(n=5, seed=3):
+    pm = cases.jittered_tet_box(n, jitter=0.2, seed=seed,
+                                patch_types=["wall", "wall", "wall", "lid", "wall", "wall"])
+    c = cases.Case(mesh_dir="", X=n, Y=n, Z=n, dt=0.02, mach=0.1, reynolds=100, ref_length=n,
+                   bcs=[cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann"),
+                        cases.BC("lid", 1, 1, 0, 0, "dirichlet", "neumann")])
+    ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    s0 = np.zeros((ma.total_cells, 4))
+    s0[:, :3] = 0.01 * rng.standard_normal((ma.total_cells, 3))
+    s0[:, 3] = 1.0 + 0.002 * rng.standard_normal(ma.total_cells)
+    return ma, c, s0
+
+
+@pytest.mark.parametrize("mode,steps", [(0x100, 8), (0x101, 8), (0, 2)])
+def test_tet_mesh_against_oracle(plfbs_lib, mode, steps):
+    """Jittered tets (4-face cells, the general stencil the reference GPU path
+    lacks): LS or hybrid weights with the exact inverse for 8 steps, and the
+    reference's determinant for 2 steps (it diverges later on tets)."""
+    ma, c, s0 = _tet_case()
+    rt, vt, val = cases.bc_arrays(ma, c)
+    cfg = dict(visc=c.visc, gamma=1.0, dt=c.dt, domain_dt=0.5, pressure_gradient=0.0,
+               channel_height=c.Y, max_velocity=c.mach, ref_rho=1.0, tolerance=0.0,
+               origin=(0, 0, 0), lengths=(c.X, c.Y, c.Z), gradient_mode=mode)
+    o = oracle.OracleRun(ma, rt, vt, val, cfg, s0)
+    o.run_steps(steps)
+    s = capi.Solver(ma, rt, vt, val, dict(cfg, renumber=1))
+    s.set_state(s0)
+    s.run(steps)
+    st = s.get_state()
+    for k in range(4):
+        assert rel_l2(st[:, k], o.state[:, k]) < RUN_TOL, k
