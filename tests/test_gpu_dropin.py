@@ -33,7 +33,10 @@ def test_reference_program_with_plfbs(tmp_path, name):
     state = np.stack([raw[1], raw[2], raw[3], raw[0]], axis=1)
     for k in range(4):
         assert rel_l2(state[:, k], g["final_state"][:, k]) < 1e-10, k
-    # the reference's 6-significant-digit text output agrees too
+    # the reference's 6-significant-digit text output agrees too on interior
+    # cells (after a converged exit the host re-applies its CPU boundary update
+    # to the ghosts before writing, Solver_gpu.cu:882, as the reference does)
+    C = d["ma"].n_cells
     u_txt = glob.glob(os.path.join(str(tmp_path), "out", "*", "u.txt"))[0]
     u = np.loadtxt(u_txt, delimiter=",")[:, 1]
-    np.testing.assert_allclose(u, g["final_state"][:, 0], rtol=1e-5, atol=1e-9)
+    np.testing.assert_allclose(u[:C], g["final_state"][:C, 0], rtol=1e-5, atol=1e-9)
