@@ -195,11 +195,10 @@ def _tet_case(n=5, seed=3):
     return ma, c, s0
 
 
-@pytest.mark.parametrize("mode,steps", [(0x100, 8), (0x101, 8), (0, 2)])
+@pytest.mark.parametrize("mode,steps", [(0x100, 8), (0x101, 8)])
 def test_tet_mesh_against_oracle(plfbs_lib, mode, steps):
     """Jittered tets (4-face cells, the general stencil the reference GPU path
-    lacks): LS or hybrid weights with the exact inverse for 8 steps, and the
-    reference's determinant for 2 steps (it diverges later on tets)."""
+    lacks), LS or hybrid weights with the exact inverse, 8 steps."""
     ma, c, s0 = _tet_case()
     rt, vt, val = cases.bc_arrays(ma, c)
     cfg = dict(visc=c.visc, gamma=1.0, dt=c.dt, domain_dt=0.5, pressure_gradient=0.0,
@@ -213,3 +212,25 @@ def test_tet_mesh_against_oracle(plfbs_lib, mode, steps):
     st = s.get_state()
     for k in range(4):
         assert rel_l2(st[:, k], o.state[:, k]) < RUN_TOL, k
+
+
+def test_tet_mesh_reference_determinant_one_stage(plfbs_lib):
+    """With the reference's determinant some tets get a sign-flipped LS inverse
+    and the scheme blows up within a few steps, amplifying rounding without
+    bound; so this path is compared stage-wise: one RK stage, every quantity."""
+    ma, c, s0 = _tet_case()
+    rt, vt, val = cases.bc_arrays(ma, c)
+    cfg = dict(visc=c.visc, gamma=1.0, dt=c.dt, domain_dt=0.5, pressure_gradient=0.0,
+               channel_height=c.Y, max_velocity=c.mach, ref_rho=1.0, tolerance=0.0,
+               origin=(0, 0, 0), lengths=(c.X, c.Y, c.Z), gradient_mode=0)
+    o = oracle.OracleRun(ma, rt, vt, val, cfg, s0)
+    o.run_stages(1)
+    s = capi.Solver(ma, rt, vt, val, dict(cfg, renumber=1))
+    s.set_debug(True)
+    s.set_state(s0)
+    s.run_stages(1)
+    C = ma.n_cells
+    assert rel_err(s.gradients(), o.grad[:C]) < STAGE_TOL
+    assert rel_err(s.face_flux(), o.face_flux) < STAGE_TOL
+    assert rel_err(s.residual(), o.residual) < STAGE_TOL
+    assert rel_err(s.get_state(), o.state) < STAGE_TOL
