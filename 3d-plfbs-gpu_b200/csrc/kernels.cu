@@ -168,21 +168,29 @@ __device__ __forceinline__ void lattice_pair(const double si[4], const double sn
                                              double m[3], double P[6]) {
   const double s = (EX ? (EX > 0 ? n[0] : -n[0]) : 0.0) + (EY ? (EY > 0 ? n[1] : -n[1]) : 0.0) +
                    (EZ ? (EZ > 0 ? n[2] : -n[2]) : 0.0);
-  const int mode = s > d1 ? 1 : (s < -d1 ? 2 : 0);
+  // Faces are sorted by their branch signature, so these branches are
+  // uniform across almost every warp; each computes only its own values.
   double qa[4], qb[4];
+  if (s > d1) {
 #pragma unroll
-  for (int f = 0; f < 4; f++) {
-    const double e1 = edot<EX, EY, EZ>(g1 + 3 * f), e2 = edot<EX, EY, EZ>(g2 + 3 * f);
-    double ba, bb, ea, eb;
-    if (mode == 1) {
-      ba = si[f]; bb = sn[f]; ea = e1; eb = e2;
-    } else if (mode == 2) {
-      ba = sn[f]; bb = si[f]; ea = e2; eb = e1;
-    } else {
-      ba = sc[f]; bb = sc[f]; ea = (e1 + e2) * 0.5; eb = ea;
+    for (int f = 0; f < 4; f++) {
+      qa[f] = fma(-edot<EX, EY, EZ>(g1 + 3 * f), dt, si[f]);
+      qb[f] = fma(edot<EX, EY, EZ>(g2 + 3 * f), dt, sn[f]);
     }
-    qa[f] = fma(-ea, dt, ba);
-    qb[f] = fma(eb, dt, bb);
+  } else if (s < -d1) {
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+      qa[f] = fma(-edot<EX, EY, EZ>(g2 + 3 * f), dt, sn[f]);
+      qb[f] = fma(edot<EX, EY, EZ>(g1 + 3 * f), dt, si[f]);
+    }
+  } else {
+    const double hdt = 0.5 * dt;  // e . (g1 + g2) / 2 dt
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+      const double e = edot<EX, EY, EZ>(g1 + 3 * f) + edot<EX, EY, EZ>(g2 + 3 * f);
+      qa[f] = fma(-e, hdt, sc[f]);
+      qb[f] = fma(e, hdt, sc[f]);
+    }
   }
   // w rho (1 + 3 e.u + 4.5 (e.u)^2 / gamma - 1.5 u^2 / gamma)
   const double eua = edot<EX, EY, EZ>(qa + 1), eub = -edot<EX, EY, EZ>(qb + 1);

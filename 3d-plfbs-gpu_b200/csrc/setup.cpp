@@ -66,6 +66,22 @@ std::vector<int32_t> rcm_order(int C, int Fi, const int32_t* owner, const int32_
   return order;  // order[new] = old
 }
 
+// For each of the 7 opposite lattice pairs of D3Q15 (first members e = x, y,
+// z, (1,1,1), (1,1,-1), (1,-1,1), (-1,1,1)) the branch the flux kernel takes:
+// 1 if e.n > 0.001 dt, 2 if e.n < -0.001 dt, 0 in the dead band
+// (LBFS.cu:353-354); packed base 3.
+int upwind_signature(const double* n, double dt) {
+  static const int E[7][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 1},
+                              {1, 1, -1}, {1, -1, 1}, {-1, 1, 1}};
+  const double d1 = 0.001 * dt;
+  int sig = 0, p3 = 1;
+  for (int p = 0; p < 7; p++, p3 *= 3) {
+    const double s = E[p][0] * n[0] + E[p][1] * n[1] + E[p][2] * n[2];
+    sig += p3 * (s > d1 ? 1 : (s < -d1 ? 2 : 0));
+  }
+  return sig;
+}
+
 }  // namespace
 
 // gradients::pre_fill_LHS_and_RHS_matrix (gradients.cpp:214-313) with
@@ -260,11 +276,17 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
   for (int i = 0; i < C; i++) L.cell_new_of_old[L.cell_old_of_new[i]] = i;
   auto newc = [&](int old) { return L.cell_new_of_old[old]; };
 
-  // internal faces by (new owner, new neighbour); boundary faces by new owner
+  // Internal faces by (upwind signature, new owner, new neighbour): faces
+  // with the same signature take the same branches in the flux kernel, and
+  // on structured meshes each signature class is a stream of owner/neighbour
+  // pairs at a fixed offset. Boundary faces by new owner.
   std::vector<int32_t> fint(Fi), fbnd(B);
   std::iota(fint.begin(), fint.end(), 0);
   std::iota(fbnd.begin(), fbnd.end(), Fi);
+  std::vector<int32_t> sig(Fi);
+  for (int f = 0; f < Fi; f++) sig[f] = upwind_signature(m.face_normal + 3 * (size_t)f, m.streaming_dt[f]);
   std::stable_sort(fint.begin(), fint.end(), [&](int a, int b) {
+    if (sig[a] != sig[b]) return sig[a] < sig[b];
     const int oa = newc(m.owner[a]), ob = newc(m.owner[b]);
     if (oa != ob) return oa < ob;
     return newc(m.neighbour[a]) < newc(m.neighbour[b]);
