@@ -164,8 +164,8 @@ template <int EX, int EY, int EZ>
 __device__ __forceinline__ void lattice_pair(const double si[4], const double sn[4],
                                              const double sc[4], const double g1[12],
                                              const double g2[12], const double n[3], double d1,
-                                             double dt, double pg, double wgt, double& rhoI,
-                                             double m[3], double P[6]) {
+                                             double dt, double c45, double c15, double wgt,
+                                             double& rhoI, double m[3], double P[6]) {
   const double s = (EX ? (EX > 0 ? n[0] : -n[0]) : 0.0) + (EY ? (EY > 0 ? n[1] : -n[1]) : 0.0) +
                    (EZ ? (EZ > 0 ? n[2] : -n[2]) : 0.0);
   // Faces are sorted by their branch signature, so these branches are
@@ -192,12 +192,15 @@ __device__ __forceinline__ void lattice_pair(const double si[4], const double sn
       qb[f] = fma(e, hdt, sc[f]);
     }
   }
-  // w rho (1 + 3 e.u + 4.5 (e.u)^2 / gamma - 1.5 u^2 / gamma)
+  // w rho (1 + 3 e.u + 4.5 (e.u)^2 / gamma - 1.5 u^2 / gamma), with
+  // c45 = 4.5 / gamma and c15 = 1.5 / gamma folded in
   const double eua = edot<EX, EY, EZ>(qa + 1), eub = -edot<EX, EY, EZ>(qb + 1);
-  const double u2a = (qa[1] * qa[1] + qa[2] * qa[2] + qa[3] * qa[3]) * pg;
-  const double u2b = (qb[1] * qb[1] + qb[2] * qb[2] + qb[3] * qb[3]) * pg;
-  const double fa = wgt * qa[0] * (1.0 + 3.0 * eua + 4.5 * eua * eua * pg - 1.5 * u2a);
-  const double fb = wgt * qb[0] * (1.0 + 3.0 * eub + 4.5 * eub * eub * pg - 1.5 * u2b);
+  const double u2a = fma(qa[3], qa[3], fma(qa[2], qa[2], qa[1] * qa[1]));
+  const double u2b = fma(qb[3], qb[3], fma(qb[2], qb[2], qb[1] * qb[1]));
+  const double fa =
+      wgt * qa[0] * fma(-c15, u2a, fma(c45 * eua, eua, fma(3.0, eua, 1.0)));
+  const double fb =
+      wgt * qb[0] * fma(-c15, u2b, fma(c45 * eub, eub, fma(3.0, eub, 1.0)));
   const double sum = fa + fb, dif = fa - fb;
   rhoI += sum;
   if (EX) m[0] += EX > 0 ? dif : -dif;
@@ -279,20 +282,20 @@ __global__ void __launch_bounds__(kFluxBlock, 4) k_flux(const KernelArgs a) {
     }
   }
 
-  const double pg = a.pg, d1 = 0.001 * dt;
+  const double pg = a.pg, d1 = 0.001 * dt, c45 = 4.5 * pg, c15 = 1.5 * pg;
   const double w0 = 2.0 / 9.0, w1 = 1.0 / 9.0, w7 = 1.0 / 72.0;
   // centre node (k = 0): e = 0
-  const double u2c = (sc[1] * sc[1] + sc[2] * sc[2] + sc[3] * sc[3]) * pg;
-  double rhoI = w0 * sc[0] * (1.0 - 1.5 * u2c);
+  const double u2c = fma(sc[3], sc[3], fma(sc[2], sc[2], sc[1] * sc[1]));
+  double rhoI = w0 * sc[0] * fma(-c15, u2c, 1.0);
   double m[3] = {0.0, 0.0, 0.0};
   double P[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  lattice_pair<1, 0, 0>(si, sn, sc, g1, g2, n, d1, dt, pg, w1, rhoI, m, P);
-  lattice_pair<0, 1, 0>(si, sn, sc, g1, g2, n, d1, dt, pg, w1, rhoI, m, P);
-  lattice_pair<0, 0, 1>(si, sn, sc, g1, g2, n, d1, dt, pg, w1, rhoI, m, P);
-  lattice_pair<1, 1, 1>(si, sn, sc, g1, g2, n, d1, dt, pg, w7, rhoI, m, P);
-  lattice_pair<1, 1, -1>(si, sn, sc, g1, g2, n, d1, dt, pg, w7, rhoI, m, P);
-  lattice_pair<1, -1, 1>(si, sn, sc, g1, g2, n, d1, dt, pg, w7, rhoI, m, P);
-  lattice_pair<-1, 1, 1>(si, sn, sc, g1, g2, n, d1, dt, pg, w7, rhoI, m, P);
+  lattice_pair<1, 0, 0>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w1, rhoI, m, P);
+  lattice_pair<0, 1, 0>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w1, rhoI, m, P);
+  lattice_pair<0, 0, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w1, rhoI, m, P);
+  lattice_pair<1, 1, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P);
+  lattice_pair<1, 1, -1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P);
+  lattice_pair<1, -1, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P);
+  lattice_pair<-1, 1, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P);
 
   const double tau = a.visc3 / dt * pg;
   const double mn = m[0] * n[0] + m[1] * n[1] + m[2] * n[2];

@@ -276,18 +276,22 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
   for (int i = 0; i < C; i++) L.cell_new_of_old[L.cell_old_of_new[i]] = i;
   auto newc = [&](int old) { return L.cell_new_of_old[old]; };
 
-  // Internal faces by (upwind signature, new owner, new neighbour): faces
-  // with the same signature take the same branches in the flux kernel, and
-  // on structured meshes each signature class is a stream of owner/neighbour
-  // pairs at a fixed offset. Boundary faces by new owner.
+  // Internal faces by (owner window, upwind signature, new owner, new
+  // neighbour): within each window of kFaceWindow owners, faces with the same
+  // signature take the same branches in the flux kernel (and on structured
+  // meshes form a stream of owner/neighbour pairs at a fixed offset), while
+  // the window keeps the cells they read resident in L2 across the classes.
+  // Boundary faces by new owner.
   std::vector<int32_t> fint(Fi), fbnd(B);
   std::iota(fint.begin(), fint.end(), 0);
   std::iota(fbnd.begin(), fbnd.end(), Fi);
   std::vector<int32_t> sig(Fi);
   for (int f = 0; f < Fi; f++) sig[f] = upwind_signature(m.face_normal + 3 * (size_t)f, m.streaming_dt[f]);
+  constexpr int kFaceWindow = 4096;
   std::stable_sort(fint.begin(), fint.end(), [&](int a, int b) {
-    if (sig[a] != sig[b]) return sig[a] < sig[b];
     const int oa = newc(m.owner[a]), ob = newc(m.owner[b]);
+    if (oa / kFaceWindow != ob / kFaceWindow) return oa / kFaceWindow < ob / kFaceWindow;
+    if (sig[a] != sig[b]) return sig[a] < sig[b];
     if (oa != ob) return oa < ob;
     return newc(m.neighbour[a]) < newc(m.neighbour[b]);
   });
