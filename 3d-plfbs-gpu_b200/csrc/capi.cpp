@@ -108,8 +108,17 @@ int capture_step(plfbs_ctx* ctx) {
 }
 
 int reset_force(plfbs_ctx* ctx) {
-  if (!ctx->args.force_x) return PLFBS_OK;
   const int C = ctx->L.C;
+  if (ctx->args.fforce_x) {
+    std::vector<float> base(C, (float)(ctx->cfg.pressure_gradient / ctx->cfg.max_velocity));
+    CK(cudaMemcpyAsync(ctx->args.fforce_x, base.data(), C * sizeof(float), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaMemsetAsync(ctx->args.fforce_y, 0, C * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(ctx->args.fforce_z, 0, C * sizeof(float), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PLFBS_OK;
+  }
+  if (!ctx->args.force_x) return PLFBS_OK;
   std::vector<double> base(C, ctx->cfg.pressure_gradient);
   CK(cudaMemcpyAsync(ctx->args.force_x, base.data(), C * sizeof(double), cudaMemcpyHostToDevice,
                      ctx->stream));
@@ -123,6 +132,32 @@ int read_stats(plfbs_ctx* ctx) {
   CK(cudaMemcpyAsync(ctx->stats_host, ctx->args.stats, offsetof(DevStats, history),
                      cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  return PLFBS_OK;
+}
+
+// Downloads n four-component records (state-like: u, v, w, rho layout) as FP64.
+// The FP32 form stores (u/U, v/U, w/U, rho - rho0): with `increments` the
+// records are differences (residuals, fluxes) and only the scaling applies.
+int download4(plfbs_ctx* ctx, const void* src, size_t n, std::vector<double>& out,
+              bool increments) {
+  out.resize(4 * n);
+  if (ctx->cfg.precision == PLFBS_FP32_DEVIATION) {
+    std::vector<float> f(4 * n);
+    CK(cudaMemcpyAsync(f.data(), src, f.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double U = ctx->cfg.max_velocity, r0 = increments ? 0.0 : ctx->cfg.ref_rho;
+    for (size_t i = 0; i < n; i++) {
+      out[4 * i] = U * f[4 * i];
+      out[4 * i + 1] = U * f[4 * i + 1];
+      out[4 * i + 2] = U * f[4 * i + 2];
+      out[4 * i + 3] = r0 + f[4 * i + 3];
+    }
+  } else {
+    CK(cudaMemcpyAsync(out.data(), src, out.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
   return PLFBS_OK;
 }
 
@@ -161,8 +196,6 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   *out = nullptr;
   if (cfg->precision != PLFBS_FP64 && cfg->precision != PLFBS_FP32_DEVIATION)
     return set_err(nullptr, PLFBS_ERR_ARG, "unknown precision mode");
-  if (cfg->precision == PLFBS_FP32_DEVIATION)
-    return set_err(nullptr, PLFBS_ERR_ARG, "the FP32 deviation form is not built in this library");
   if (!(cfg->time_marching_step > 0) || !(cfg->gamma > 0) || !(cfg->ref_rho > 0) ||
       !(cfg->max_velocity > 0) || !std::isfinite(cfg->visc))
     return set_err(nullptr, PLFBS_ERR_ARG,
@@ -178,6 +211,11 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     return set_err(nullptr, rc, err);
   }
   const Layout& L = ctx->L;
+  const bool fp32 = cfg->precision == PLFBS_FP32_DEVIATION;
+  if (fp32 && L.K2 > 16) {
+    delete ctx;
+    return set_err(nullptr, PLFBS_ERR_MESH, "the FP32 form handles cells with at most 16 faces");
+  }
   const int N = (ibm && ibm->n_nodes > 0) ? ibm->n_nodes : 0;
   if (N > 0) {
     if (!ibm->x || !ibm->x_ref || ibm->object_nodes <= 0 || !(cfg->domain_dt > 0) ||
@@ -229,47 +267,86 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   a.pressure_gradient = cfg->pressure_gradient;
   a.tolerance = cfg->tolerance;
   a.inv_ref_rho = 1.0 / cfg->ref_rho;
-  a.inv_ref_mom = 1.0 / (cfg->ref_rho * cfg->max_velocity);
+  // the FP32 form keeps momentum residuals divided by U
+  a.inv_ref_mom = fp32 ? 1.0 / cfg->ref_rho : 1.0 / (cfg->ref_rho * cfg->max_velocity);
   a.rho0 = cfg->ref_rho;
   a.uref = cfg->max_velocity;
+  a.rho0f = (float)cfg->ref_rho;
+  a.inv_uref_f = (float)(1.0 / cfg->max_velocity);
   for (int c = 0; c < 3; c++) a.origin[c] = cfg->origin[c];
 
+  // element sizes: FP64 double4 = 32 B, FP32 float4 = 16 B
+  const size_t e4 = fp32 ? 16 : 32;
   void* p = nullptr;
-  if ((rc = dev_alloc(ctx, &p, (size_t)T * 32))) return fail(rc);
+  if ((rc = dev_alloc(ctx, &p, (size_t)T * e4))) return fail(rc);
   a.state = p;
-  if ((rc = dev_alloc(ctx, &p, (size_t)L.C * 32))) return fail(rc);
+  if ((rc = dev_alloc(ctx, &p, (size_t)L.C * e4))) return fail(rc);
   a.t0 = p;
-  if ((rc = dev_alloc(ctx, &p, (size_t)L.C * 32))) return fail(rc);
+  if ((rc = dev_alloc(ctx, &p, (size_t)L.C * e4))) return fail(rc);
   a.t1 = p;
-  if ((rc = dev_alloc(ctx, &p, (size_t)L.C * 96))) return fail(rc);
+  if ((rc = dev_alloc(ctx, &p, (size_t)L.C * 3 * e4))) return fail(rc);
   a.grad = p;
-  if ((rc = dev_alloc(ctx, &p, (size_t)L.F * 32))) return fail(rc);
+  if ((rc = dev_alloc(ctx, &p, (size_t)L.F * e4))) return fail(rc);
   a.flux = p;
-  if ((rc = dev_upload(ctx, &p, L.face0))) return fail(rc);
-  a.face0 = p;
-  if ((rc = dev_upload(ctx, &p, L.face1))) return fail(rc);
-  a.face1 = p;
-  if ((rc = dev_upload(ctx, &p, L.face2))) return fail(rc);
-  a.face2 = p;
-  if ((rc = dev_upload(ctx, &p, L.bc0))) return fail(rc);
-  a.bc0 = p;
-  if ((rc = dev_upload(ctx, &p, L.bc1))) return fail(rc);
-  a.bc1 = p;
-  if ((rc = dev_upload(ctx, &p, L.bc2))) return fail(rc);
-  a.bc2 = p;
-  if ((rc = dev_upload(ctx, &p, L.bc3))) return fail(rc);
-  a.bc3 = p;
+  plfbs::Layout32 L32;
+  if (fp32) {
+    plfbs::build_layout32(L, cfg->ref_rho, cfg->max_velocity, L32);
+    if ((rc = dev_upload(ctx, &p, L32.face0))) return fail(rc);
+    a.face0 = p;
+    if ((rc = dev_upload(ctx, &p, L32.face1))) return fail(rc);
+    a.face1 = p;
+    if ((rc = dev_upload(ctx, &p, L32.face2))) return fail(rc);
+    a.face2 = p;
+    if ((rc = dev_upload(ctx, &p, L32.face_ids))) return fail(rc);
+    a.face_ids = static_cast<const int32_t*>(p);
+    if ((rc = dev_upload(ctx, &p, L32.bc0))) return fail(rc);
+    a.bc0 = p;
+    if ((rc = dev_upload(ctx, &p, L32.bc1))) return fail(rc);
+    a.bc1 = p;
+    if ((rc = dev_upload(ctx, &p, L32.bc2))) return fail(rc);
+    a.bc2 = p;
+    if ((rc = dev_upload(ctx, &p, L32.bc3))) return fail(rc);
+    a.bc3 = p;
+  } else {
+    if ((rc = dev_upload(ctx, &p, L.face0))) return fail(rc);
+    a.face0 = p;
+    if ((rc = dev_upload(ctx, &p, L.face1))) return fail(rc);
+    a.face1 = p;
+    if ((rc = dev_upload(ctx, &p, L.face2))) return fail(rc);
+    a.face2 = p;
+    if ((rc = dev_upload(ctx, &p, L.bc0))) return fail(rc);
+    a.bc0 = p;
+    if ((rc = dev_upload(ctx, &p, L.bc1))) return fail(rc);
+    a.bc1 = p;
+    if ((rc = dev_upload(ctx, &p, L.bc2))) return fail(rc);
+    a.bc2 = p;
+    if ((rc = dev_upload(ctx, &p, L.bc3))) return fail(rc);
+    a.bc3 = p;
+  }
   if ((rc = dev_upload(ctx, &p, L.st_nbr))) return fail(rc);
   a.st_nbr = static_cast<const int32_t*>(p);
-  if ((rc = dev_upload(ctx, &p, L.st_wx))) return fail(rc);
-  a.st_wx = p;
-  if ((rc = dev_upload(ctx, &p, L.st_wy))) return fail(rc);
-  a.st_wy = p;
-  if ((rc = dev_upload(ctx, &p, L.st_wz))) return fail(rc);
-  a.st_wz = p;
+  if (fp32) {
+    if ((rc = dev_upload(ctx, &p, L32.st_wx))) return fail(rc);
+    a.st_wx = p;
+    if ((rc = dev_upload(ctx, &p, L32.st_wy))) return fail(rc);
+    a.st_wy = p;
+    if ((rc = dev_upload(ctx, &p, L32.st_wz))) return fail(rc);
+    a.st_wz = p;
+  } else {
+    if ((rc = dev_upload(ctx, &p, L.st_wx))) return fail(rc);
+    a.st_wx = p;
+    if ((rc = dev_upload(ctx, &p, L.st_wy))) return fail(rc);
+    a.st_wy = p;
+    if ((rc = dev_upload(ctx, &p, L.st_wz))) return fail(rc);
+    a.st_wz = p;
+  }
   if ((rc = dev_upload(ctx, &p, L.gather))) return fail(rc);
   a.gather = static_cast<const int32_t*>(p);
-  if ((rc = dev_upload(ctx, &p, L.inv_volume))) return fail(rc);
+  if (fp32) {
+    if ((rc = dev_upload(ctx, &p, L32.inv_volume))) return fail(rc);
+  } else {
+    if ((rc = dev_upload(ctx, &p, L.inv_volume))) return fail(rc);
+  }
   a.inv_volume = p;
   if ((rc = dev_alloc(ctx, &p, (size_t)a.nblk_update * 4 * sizeof(double)))) return fail(rc);
   a.partial = static_cast<double*>(p);
@@ -277,6 +354,7 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   a.stats = static_cast<DevStats*>(p);
   a.res_debug = nullptr;
   a.force_x = a.force_y = a.force_z = nullptr;
+  a.fforce_x = a.fforce_y = a.fforce_z = nullptr;
   if (N > 0) {
     const double dx = cfg->domain_dt * 2;  // Solver_gpu.cu:517
     a.ibm_dx = dx;
@@ -284,9 +362,16 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     a.ibm_xc = (int)(cfg->lengths[0] / dx);
     a.ibm_yc = (int)(cfg->lengths[1] / dx);
     a.ibm_area_k = ibm->stiffness * (2 * std::acos(-1.0) * ibm->radius / ibm->object_nodes * ibm->depth);
-    for (double** f : {&a.force_x, &a.force_y, &a.force_z}) {
-      if ((rc = dev_alloc(ctx, &p, (size_t)L.C * sizeof(double)))) return fail(rc);
-      *f = static_cast<double*>(p);
+    if (fp32) {
+      for (float** f : {&a.fforce_x, &a.fforce_y, &a.fforce_z}) {
+        if ((rc = dev_alloc(ctx, &p, (size_t)L.C * sizeof(float)))) return fail(rc);
+        *f = static_cast<float*>(p);
+      }
+    } else {
+      for (double** f : {&a.force_x, &a.force_y, &a.force_z}) {
+        if ((rc = dev_alloc(ctx, &p, (size_t)L.C * sizeof(double)))) return fail(rc);
+        *f = static_cast<double*>(p);
+      }
     }
     std::vector<double> x(ibm->x, ibm->x + 3 * (size_t)N), xr(ibm->x_ref, ibm->x_ref + 3 * (size_t)N);
     if ((rc = dev_upload(ctx, &p, x))) return fail(rc);
@@ -329,16 +414,33 @@ int plfbs_set_state(plfbs_ctx* ctx, const double* rho, const double* u, const do
   const int64_t T = (int64_t)L.C + L.B;
   if (!rho || !u || !v || !w || n_total != T)
     return set_err(ctx, PLFBS_ERR_ARG, "set_state needs 4 arrays of n_cells + n_boundary values");
-  std::vector<double> q(4 * (size_t)T);
-  for (int64_t o = 0; o < T; o++) {
-    const int64_t n = o < L.C ? L.cell_new_of_old[o] : L.C + L.bc_new_of_old[o - L.C];
-    q[4 * n] = u[o];
-    q[4 * n + 1] = v[o];
-    q[4 * n + 2] = w[o];
-    q[4 * n + 3] = rho[o];
+  if (ctx->cfg.precision == PLFBS_FP32_DEVIATION) {
+    // deviation units: velocity / U, rho - rho0
+    const double U = ctx->cfg.max_velocity, r0 = ctx->cfg.ref_rho;
+    std::vector<float> q(4 * (size_t)T);
+    for (int64_t o = 0; o < T; o++) {
+      const int64_t n = o < L.C ? L.cell_new_of_old[o] : L.C + L.bc_new_of_old[o - L.C];
+      q[4 * n] = (float)(u[o] / U);
+      q[4 * n + 1] = (float)(v[o] / U);
+      q[4 * n + 2] = (float)(w[o] / U);
+      q[4 * n + 3] = (float)(rho[o] - r0);
+    }
+    CK(cudaMemcpyAsync(ctx->args.state, q.data(), q.size() * sizeof(float),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  } else {
+    std::vector<double> q(4 * (size_t)T);
+    for (int64_t o = 0; o < T; o++) {
+      const int64_t n = o < L.C ? L.cell_new_of_old[o] : L.C + L.bc_new_of_old[o - L.C];
+      q[4 * n] = u[o];
+      q[4 * n + 1] = v[o];
+      q[4 * n + 2] = w[o];
+      q[4 * n + 3] = rho[o];
+    }
+    CK(cudaMemcpyAsync(ctx->args.state, q.data(), q.size() * sizeof(double),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
   }
-  CK(cudaMemcpyAsync(ctx->args.state, q.data(), q.size() * sizeof(double), cudaMemcpyHostToDevice,
-                     ctx->stream));
   CK(cudaMemsetAsync(ctx->args.stats, 0, sizeof(DevStats), ctx->stream));
   plfbs::launch_seed(ctx->args, ctx->cfg.precision, ctx->stream);
   CK(cudaGetLastError());
@@ -412,10 +514,8 @@ int plfbs_get_state(plfbs_ctx* ctx, double* rho, double* u, double* v, double* w
   const int64_t T = (int64_t)L.C + L.B;
   if (!rho || !u || !v || !w || n_total != T)
     return set_err(ctx, PLFBS_ERR_ARG, "get_state needs 4 arrays of n_cells + n_boundary values");
-  std::vector<double> q(4 * (size_t)T);
-  CK(cudaMemcpyAsync(q.data(), ctx->args.state, q.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                     ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<double> q;
+  TRY(download4(ctx, ctx->args.state, (size_t)T, q, false));
   for (int64_t o = 0; o < T; o++) {
     const int64_t n = o < L.C ? L.cell_new_of_old[o] : L.C + L.bc_new_of_old[o - L.C];
     u[o] = q[4 * n];
@@ -462,7 +562,7 @@ int plfbs_set_debug(plfbs_ctx* ctx, int enable) {
   if ((enable != 0) == ctx->debug) return PLFBS_OK;
   if (enable) {
     void* p = nullptr;
-    TRY(dev_alloc(ctx, &p, (size_t)ctx->L.C * 32));
+    TRY(dev_alloc(ctx, &p, (size_t)ctx->L.C * (ctx->cfg.precision == PLFBS_FP32_DEVIATION ? 16 : 32)));
     ctx->args.res_debug = p;
   } else {
     ctx->args.res_debug = nullptr;
@@ -492,9 +592,18 @@ int plfbs_get_gradients(plfbs_ctx* ctx, double* grad, int32_t n_cells) {
   const Layout& L = ctx->L;
   if (!grad || n_cells != L.C) return set_err(ctx, PLFBS_ERR_ARG, "gradients: need 12 n_cells");
   std::vector<double> g(12 * (size_t)L.C);
-  CK(cudaMemcpyAsync(g.data(), ctx->args.grad, g.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                     ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->cfg.precision == PLFBS_FP32_DEVIATION) {
+    std::vector<float> f(g.size());
+    CK(cudaMemcpyAsync(f.data(), ctx->args.grad, f.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double U = ctx->cfg.max_velocity;  // velocity gradients are stored / U
+    for (size_t i = 0; i < g.size(); i++) g[i] = (i % 12 < 3 ? 1.0 : U) * f[i];
+  } else {
+    CK(cudaMemcpyAsync(g.data(), ctx->args.grad, g.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
   for (int o = 0; o < L.C; o++)
     std::memcpy(grad + 12 * (size_t)o, &g[12 * (size_t)L.cell_new_of_old[o]], 12 * sizeof(double));
   return PLFBS_OK;
@@ -504,10 +613,14 @@ int plfbs_get_face_flux(plfbs_ctx* ctx, double* flux, int32_t n_faces) {
   TRY(check_ctx(ctx));
   const Layout& L = ctx->L;
   if (!flux || n_faces != L.F) return set_err(ctx, PLFBS_ERR_ARG, "face flux: need 4 n_faces");
-  std::vector<double> g(4 * (size_t)L.F);
-  CK(cudaMemcpyAsync(g.data(), ctx->args.flux, g.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                     ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<double> g;
+  TRY(download4(ctx, ctx->args.flux, (size_t)L.F, g, true));
+  if (ctx->cfg.precision == PLFBS_FP32_DEVIATION) {
+    // add back the constant rho0/3 n A the deviation form leaves out
+    const double p3 = ctx->cfg.ref_rho / 3.0;
+    for (int k = 0; k < L.F; k++)
+      for (int c = 0; c < 3; c++) g[4 * (size_t)k + c] += p3 * L.face0[4 * (size_t)k + c] * L.face0[4 * (size_t)k + 3];
+  }
   for (int f = 0; f < L.F; f++)
     std::memcpy(flux + 4 * (size_t)f, &g[4 * (size_t)L.face_new_of_old[f]], 4 * sizeof(double));
   return PLFBS_OK;
@@ -518,10 +631,8 @@ int plfbs_get_residual(plfbs_ctx* ctx, double* res, int32_t n_cells) {
   const Layout& L = ctx->L;
   if (!ctx->args.res_debug) return set_err(ctx, PLFBS_ERR_STATE, "enable plfbs_set_debug first");
   if (!res || n_cells != L.C) return set_err(ctx, PLFBS_ERR_ARG, "residual: need 4 n_cells");
-  std::vector<double> g(4 * (size_t)L.C);
-  CK(cudaMemcpyAsync(g.data(), ctx->args.res_debug, g.size() * sizeof(double),
-                     cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<double> g;
+  TRY(download4(ctx, ctx->args.res_debug, (size_t)L.C, g, true));
   for (int o = 0; o < L.C; o++)
     std::memcpy(res + 4 * (size_t)o, &g[4 * (size_t)L.cell_new_of_old[o]], 4 * sizeof(double));
   return PLFBS_OK;

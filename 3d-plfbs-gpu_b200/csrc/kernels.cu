@@ -598,11 +598,11 @@ inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 }  // namespace
 
 void launch_gradient(const KernelArgs& a, int precision, cudaStream_t s) {
-  (void)precision;
+  if (precision == PLFBS_FP32_DEVIATION) return launch_gradient32(a, s);
   k_gradient<<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
 }
 void launch_flux(const KernelArgs& a, int precision, cudaStream_t s) {
-  (void)precision;
+  if (precision == PLFBS_FP32_DEVIATION) return launch_flux32(a, s);
   k_flux<<<blocks_for(a.F, kFluxBlock), kFluxBlock, 0, s>>>(a);
 }
 template <int RK>
@@ -617,7 +617,7 @@ static void launch_update_rk(const KernelArgs& a, int nb, cudaStream_t s) {
     k_update<RK, 0><<<nb, kBlock, 0, s>>>(a);
 }
 void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t s) {
-  (void)precision;
+  if (precision == PLFBS_FP32_DEVIATION) return launch_update32(a, rk, s);
   const int nb = blocks_for(a.C, kBlock);
   switch (rk) {
     case 0: launch_update_rk<0>(a, nb, s); break;
@@ -627,11 +627,11 @@ void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t s) {
   }
 }
 void launch_seed(const KernelArgs& a, int precision, cudaStream_t s) {
-  (void)precision;
+  if (precision == PLFBS_FP32_DEVIATION) return launch_seed32(a, s);
   k_seed<<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
 }
 void launch_ibm(const KernelArgs& a, int precision, cudaStream_t s) {
-  (void)precision;
+  if (precision == PLFBS_FP32_DEVIATION) return launch_ibm32(a, s);
   if (a.N > 0) k_ibm<<<blocks_for(a.N, 128), 128, 0, s>>>(a);
 }
 

@@ -59,6 +59,19 @@ struct Layout {
   std::vector<double> centroid;                // [3(C+B)]
 };
 
+// FP32 copies of the layout for the deviation form (PLFBS_FP32_DEVIATION):
+// geometry and weights rounded once from the FP64 records (weights are built
+// in FP64 first), boundary values expressed as deviations (rho - rho0,
+// velocity / U), face ids moved to their own int2 array.
+struct Layout32 {
+  std::vector<float> face0, face1, face2;        // [4F] (n, A), (dt_s, t1), (t2, 0)
+  std::vector<int32_t> face_ids;                 // [2F] new owner, new neighbour
+  std::vector<float> bc0, bc1, bc2, bc3;         // [4B]
+  std::vector<float> st_wx, st_wy, st_wz;        // [K*C]
+  std::vector<float> inv_volume;                 // [C]
+};
+void build_layout32(const Layout& L, double rho0, double uref, Layout32& L32);
+
 // Least-squares weights exactly as gradients::pre_fill_LHS_and_RHS_matrix
 // (gradients.cpp:214-313): lhs_inv [9C], rhs [3 nnz], caller numbering.
 int ls_weights(const plfbs_mesh_view& m, int mode, double* lhs_inv, double* rhs,
@@ -124,14 +137,24 @@ struct KernelArgs {
   const int32_t* ibm_map;  // caller cell index -> new cell index
   double* partial;      // [nblk_update * 4] per-block squared-residual sums
   DevStats* stats;
-  void* res_debug;      // double4 [C] or null
+  void* res_debug;      // double4 [C] (FP32 form: float4) or null
+  // FP32 deviation form only
+  const int32_t* face_ids;                     // int2 [F]
+  float* fforce_x; float* fforce_y; float* fforce_z;  // [C] body force / U, or null
+  float rho0f, inv_uref_f;
 };
 
-// Launchers (kernels.cu). All enqueue on `stream`, never synchronise.
+// Launchers (kernels.cu; the FP32 deviation form in kernels_fp32.cu). All
+// enqueue on `stream`, never synchronise.
 void launch_ibm(const KernelArgs& a, int precision, cudaStream_t stream);
 void launch_gradient(const KernelArgs& a, int precision, cudaStream_t stream);
 void launch_flux(const KernelArgs& a, int precision, cudaStream_t stream);
 void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t stream);
 void launch_seed(const KernelArgs& a, int precision, cudaStream_t stream);
+void launch_ibm32(const KernelArgs& a, cudaStream_t stream);
+void launch_gradient32(const KernelArgs& a, cudaStream_t stream);
+void launch_flux32(const KernelArgs& a, cudaStream_t stream);
+void launch_update32(const KernelArgs& a, int rk, cudaStream_t stream);
+void launch_seed32(const KernelArgs& a, cudaStream_t stream);
 
 }  // namespace plfbs

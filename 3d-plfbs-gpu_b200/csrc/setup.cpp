@@ -436,3 +436,44 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
 }
 
 }  // namespace plfbs
+
+namespace plfbs {
+
+void build_layout32(const Layout& L, double rho0, double uref, Layout32& o) {
+  const size_t F = L.F, B = L.B;
+  auto cast = [](const std::vector<double>& v) {
+    std::vector<float> r(v.size());
+    for (size_t i = 0; i < v.size(); i++) r[i] = (float)v[i];
+    return r;
+  };
+  o.face0 = cast(L.face0);
+  o.face1 = cast(L.face1);
+  o.face2.assign(4 * F, 0.0f);
+  o.face_ids.resize(2 * F);
+  for (size_t k = 0; k < F; k++) {
+    for (int c = 0; c < 3; c++) o.face2[4 * k + c] = (float)L.face2[4 * k + c];
+    uint64_t ids;
+    std::memcpy(&ids, &L.face2[4 * k + 3], sizeof ids);
+    o.face_ids[2 * k] = (int32_t)(uint32_t)(ids & 0xffffffffu);
+    o.face_ids[2 * k + 1] = (int32_t)(uint32_t)(ids >> 32);
+  }
+  // boundary values as deviations: velocity / U, rho - rho0
+  auto dev = [&](const std::vector<double>& v) {
+    std::vector<float> r(v.size());
+    for (size_t b = 0; b < B; b++) {
+      for (int c = 0; c < 3; c++) r[4 * b + c] = (float)(v[4 * b + c] / uref);
+      r[4 * b + 3] = (float)(v[4 * b + 3] - rho0);
+    }
+    return r;
+  };
+  o.bc0 = dev(L.bc0);
+  o.bc1 = dev(L.bc1);
+  o.bc2 = cast(L.bc2);
+  o.bc3 = cast(L.bc3);  // the type code (< 2^24) is exact in float
+  o.st_wx = cast(L.st_wx);
+  o.st_wy = cast(L.st_wy);
+  o.st_wz = cast(L.st_wz);
+  o.inv_volume = cast(L.inv_volume);
+}
+
+}  // namespace plfbs

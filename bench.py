@@ -53,7 +53,9 @@ KERNELS_PER_STEP = 13  # ibm + 4 x (gradient, flux, update)
 # write (32 B); per cell the state (32 B), gradients (96 B), centroid and
 # volume (32 B) read once. gradient: state + 6 weights/indices + gradient
 # write; update: 6 face fluxes, indices, t0, t1 read+write, state write.
-def algorithmic_bytes(C, F, B):
+def algorithmic_bytes(C, F, B, fp32=False):
+    if fp32:  # the same traffic with 4-byte values (indices stay 4 bytes)
+        return {"flux": 56 * F + 80 * C, "gradient": 160 * C, "update": 196 * C}
     return {"flux": 104 * F + 160 * C,
             "gradient": 296 * C,
             "update": 344 * C}
@@ -76,10 +78,11 @@ def build_case():
     return pm, c, ma, nodes, state0
 
 
-def solver_cfg(c):
+def solver_cfg(c, precision=0):
     return dict(visc=c.visc, gamma=1.0, dt=c.dt, domain_dt=0.5, max_velocity=c.mach,
                 ref_rho=1.0, tolerance=0.0, pressure_gradient=0.0, channel_height=c.Y,
-                origin=(0.0, 0.0, 0.0), lengths=(c.X, c.Y, c.Z), gradient_mode=0, renumber=0)
+                origin=(0.0, 0.0, 0.0), lengths=(c.X, c.Y, c.Z), gradient_mode=0, renumber=0,
+                precision=precision)
 
 
 def ibm_cfg(nodes):
@@ -240,6 +243,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=20)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="fp32: the FP32 deviation form (the headline line is fp64)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -262,7 +267,9 @@ def main():
     pm, c, ma, nodes, state0 = build_case()
     rt, vt, val = cases.bc_arrays(ma, c)
     log("case built: %d cells, %d faces" % (ma.n_cells, ma.n_faces))
-    solver = capi.Solver(ma, rt, vt, val, solver_cfg(c), ibm=ibm_cfg(nodes), device=local_rank)
+    prec = capi.FP32_DEVIATION if args.precision == "fp32" else capi.FP64
+    solver = capi.Solver(ma, rt, vt, val, solver_cfg(c, prec), ibm=ibm_cfg(nodes),
+                         device=local_rank)
 
     def barrier():
         if dist:
@@ -300,7 +307,7 @@ def main():
                   "flux": prof["flux"] / (4 * args.profile_steps),
                   "update": prof["update"] / (4 * args.profile_steps)}
     total = sum(prof.values())
-    alg = algorithmic_bytes(ma.n_cells, ma.n_faces, ma.n_bc)
+    alg = algorithmic_bytes(ma.n_cells, ma.n_faces, ma.n_bc, fp32=args.precision == "fp32")
     peak, peak_kind = load_peaks()
     kern = {}
     for k in ("gradient", "flux", "update"):
@@ -319,7 +326,8 @@ def main():
         barrier()
         solver.close()
         t0 = time.perf_counter()
-        s2 = capi.Solver(ma, rt, vt, val, solver_cfg(c), ibm=ibm_cfg(nodes), device=local_rank)
+        s2 = capi.Solver(ma, rt, vt, val, solver_cfg(c, prec), ibm=ibm_cfg(nodes),
+                         device=local_rank)
         s2.set_state(state0)
         st2, hist2 = s2.run(args.steps, history=True)
         out = s2.get_state()
@@ -349,8 +357,9 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "cells": ma.n_cells, "faces": ma.n_faces,
+                "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD if args.precision == "fp64"
+                           else WORKLOAD.replace("fp64", "fp32dev"), "cells": ma.n_cells, "faces": ma.n_faces,
                            "nodes": NNODES, "re": RE, "dt": DT,
                            "parallelism": "replicas" if world > 1 else "single",
                            "l2": "working set > L2 (no flush)"},
