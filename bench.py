@@ -202,6 +202,86 @@ def reference_cpu_throughput(pm, c, nodes, sample_steps=1):
                                                     per_step))
 
 
+def reduce_max(x, dist=None, device="cuda"):
+    """Max of a float over the ranks of a process group (identity without one)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, cells, steps, max_ms):
+    """Whole-job Mcell-updates/s of `world` independent replicas, each updating
+    `cells` cells for `steps` steps, timed by the slowest rank."""
+    return world * cells * steps / (max_ms / 1e3) / 1e6
+
+
+# ---------------------------------------------------------------------------
+# time to a residual: FP64 vs the FP32 deviation form from the same cold start
+# ---------------------------------------------------------------------------
+
+TTR_WORKLOAD = "sphere_channel_64x32x32_D8_re100"
+
+
+def build_ttr_case(nx=64, ny=32, nz=32, D=8.0, re=100.0):
+    """The learned-warm-start geometry (64 x 32 x 32 channel, sphere D = 8 at
+    (16, 16, 16), Fibonacci nodes at the node density of the headline case)."""
+    pm = cases.uniform_box(nx, ny, nz, patch_types=["inlet", "outlet", "side", "side", "side",
+                                                    "side"])
+    c = cases.Case(mesh_dir="", X=nx, Y=ny, Z=nz, dt=DT, mach=U, reynolds=re, ref_length=D,
+                   tolerance=0.0,
+                   bcs=[cases.BC("inlet", 1, 1, 0, 0, "dirichlet", "neumann"),
+                        cases.BC("outlet", 1, 0, 0, 0, "neumann", "dirichlet"),
+                        cases.BC("side", 1, 0, 0, 0, "neumann", "neumann")])
+    ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
+    n_nodes = int(round(4 * np.pi * (D / 2) ** 2 / (4 * np.pi * (DIAM / 2) ** 2 / NNODES)))
+    nodes = cases.fibonacci_sphere(n_nodes, D / 2, (2 * D, ny / 2, nz / 2))
+    state0 = np.zeros((ma.total_cells, 4))
+    state0[:, 0] = U
+    state0[:, 3] = 1.0
+    ibm = dict(node_ref=nodes, stiffness=STIFFNESS, radius=D / 2, depth=D,
+               object_nodes=len(nodes))
+    return c, ma, state0, ibm, np.pi * D * D / 4
+
+
+def time_to_residual(args):
+    from plfbs import capi
+
+    c, ma, state0, ibm, area = build_ttr_case()
+    rt, vt, val = cases.bc_arrays(ma, c)
+    out, states = {}, {}
+    for name, prec in (("fp64", capi.FP64), ("fp32", capi.FP32_DEVIATION)):
+        cfg = solver_cfg(c, prec)
+        cfg["tolerance"] = args.time_to_residual
+        s = capi.Solver(ma, rt, vt, val, cfg, ibm=ibm)
+        s.set_state(state0)
+        t0 = time.perf_counter()
+        st, hist = s.run(args.max_steps, history=False)
+        wall = time.perf_counter() - t0
+        cd, cl = s.body_force(area)
+        states[name] = s.get_state()
+        s.close()
+        out[name] = {"converged": bool(st["converged"]), "steps": st["steps_done"],
+                     "device_s": st["kernel_ms"] / 1e3, "wall_s": wall,
+                     "final_max_error": st["max_error"], "cd": cd, "cl": cl}
+    a, b = states["fp64"], states["fp32"]
+    err = {k: float(np.linalg.norm(b[:, i] - a[:, i]) / np.linalg.norm(a[:, i]))
+           for i, k in enumerate(("u", "v", "w"))}
+    err["rho-rho0"] = float(np.linalg.norm(b[:, 3] - a[:, 3]) / np.linalg.norm(a[:, 3] - 1.0))
+    line = {"metric": "time-to-residual", "tolerance": args.time_to_residual,
+            "unit": "s", "higher_is_better": False, "data": "synthetic",
+            "config": {"workload": TTR_WORKLOAD, "cells": ma.n_cells, "faces": ma.n_faces,
+                       "nodes": len(ibm["node_ref"]), "start": "uniform flow (cold)"},
+            "fp64": out["fp64"], "fp32": out["fp32"],
+            "speedup_fp32_over_fp64": out["fp64"]["wall_s"] / out["fp32"]["wall_s"],
+            "fp32_vs_fp64_rel_l2": err,
+            "cd_rel_diff": abs(out["fp32"]["cd"] - out["fp64"]["cd"]) / abs(out["fp64"]["cd"])}
+    print(json.dumps(line))
+    return 0
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -245,6 +325,10 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=20)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
                     help="fp32: the FP32 deviation form (the headline line is fp64)")
+    ap.add_argument("--time-to-residual", type=float, default=None,
+                    help="instead of throughput: steps and time to max_error < this value, "
+                         "FP64 vs FP32 from a cold start")
+    ap.add_argument("--max-steps", type=int, default=100000)
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -252,6 +336,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
+    if args.time_to_residual is not None:
+        return time_to_residual(args) if rank == 0 else 0
 
     dist = None
     if world > 1:
@@ -276,12 +362,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, "cuda")
 
     log("solver created")
     # warm-up
@@ -296,7 +377,7 @@ def main():
     if st["rc"] != 0 or st["steps_run"] != args.steps:
         raise RuntimeError("timed run stopped early: %r" % st)
     ms = max_over_ranks(st["kernel_ms"])
-    value = world * ma.n_cells * args.steps / (ms / 1e3) / 1e6
+    value = replica_throughput(world, ma.n_cells, args.steps, ms)
 
     log("timed run: %.3f ms for %d steps" % (ms, args.steps))
     # per-kernel device times (CUDA events between launches on the solver's stream)
@@ -339,7 +420,8 @@ def main():
                       len(nodes) * 48)
         h2d = mesh_bytes + T * 32
         d2h = T * 32 + 48 * args.steps
-        e2e = {"value": world * ma.n_cells * args.steps / wall / 1e6, "unit": METRIC,
+        e2e = {"value": replica_throughput(world, ma.n_cells, args.steps, wall * 1e3),
+               "unit": METRIC,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "wall_s": wall, "includes": "create+set_state+run+history+get_state+destroy"}
         assert np.isfinite(out).all() and st2["steps_run"] == args.steps
