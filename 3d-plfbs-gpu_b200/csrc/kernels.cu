@@ -424,9 +424,9 @@ __global__ void __launch_bounds__(kBlock) k_update(const KernelArgs a) {
     double v = 0.0;
     for (int w = 0; w < kBlock / 32; w++) v += red[w][threadIdx.x];
     a.partial[4LL * blockIdx.x + threadIdx.x] = v;
+    __threadfence();  // only the writers of the partials need to publish them
   }
   if (threadIdx.x == 0 && any_bad) atomicExch(&a.stats->diverged, 1);
-  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned int done = atomicAdd(&a.stats->block_counter, 1u);

@@ -73,8 +73,8 @@ k_residual_norms_scratch(const double* __restrict__ res, long long n, double inv
     double v = 0.0;
     for (int w = 0; w < kNaThreads / 32; w++) v += red[w][threadIdx.x];
     scratch[4LL * blockIdx.x + threadIdx.x] = v;
+    __threadfence();  // only the writers of the partials need to publish them
   }
-  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) last = (atomicAdd(counter, 1ull) == gridDim.x - 1);
   __syncthreads();
