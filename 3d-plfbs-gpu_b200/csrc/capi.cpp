@@ -485,8 +485,10 @@ int plfbs_run(plfbs_ctx* ctx, int64_t max_steps, plfbs_stats* stats, double* his
       }
       CK(cudaStreamSynchronize(ctx->stream));
     }
-    done = now - start;
     halt = ctx->stats_host->halt != 0;
+    if (now - start == done && !halt)  // a batch that advanced nothing: never wait again
+      return set_err(ctx, PLFBS_ERR_STATE, "the step graph made no progress");
+    done = now - start;
   }
   CK(cudaGetLastError());
   if (stats) {

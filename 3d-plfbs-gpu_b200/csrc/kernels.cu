@@ -48,8 +48,13 @@ __device__ __forceinline__ void st4(void* base, long long i, const d4& v) {
   p[1] = make_double2(v.z, v.w);
 }
 
+// Whether the context has converged or diverged. One thread per block reads
+// the flag; every thread of the block must call this (it synchronises).
 __device__ __forceinline__ bool halted(const KernelArgs& a) {
-  return *(volatile const int*)&a.stats->halt != 0;
+  __shared__ int h;
+  if (threadIdx.x == 0) h = *(volatile const int*)&a.stats->halt;
+  __syncthreads();
+  return h != 0;
 }
 
 // Ghost state from its owner (update_unstructured_bcs, LBFS.cu:1228-1301).
@@ -80,7 +85,8 @@ __device__ __forceinline__ d4 ghost_state(const d4& q, const d4& tgt, int types)
 // needs ~100 registers and measured slower than this 62-register loop.)
 __global__ void __launch_bounds__(kBlock) k_gradient(const KernelArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.C || halted(a)) return;
+  if (halted(a)) return;
+  if (i >= a.C) return;
   const d4 qi = ld4(a.state, i);
   const double* wx = static_cast<const double*>(a.st_wx);
   const double* wy = static_cast<const double*>(a.st_wy);
@@ -227,7 +233,8 @@ __device__ __forceinline__ void lattice_pair(const double si[4], const double sn
 // the boundary value and all gradients from the ghost (LBFS.cu:356-401).
 __global__ void __launch_bounds__(kFluxBlock, 4) k_flux(const KernelArgs a) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= a.F || halted(a)) return;
+  if (halted(a)) return;
+  if (f >= a.F) return;
   const d4 f0 = ld4(a.face0, f), f1 = ld4(a.face1, f), f2 = ld4(a.face2, f);
   uint64_t ids;
   memcpy(&ids, &f2.w, sizeof ids);
@@ -331,6 +338,10 @@ __global__ void __launch_bounds__(kBlock) k_update(const KernelArgs a) {
   double sq[4] = {0.0, 0.0, 0.0, 0.0};
   bool bad = false;
   if (i < a.C) {
+    // The RK accumulators are loaded first, with the gather, so no store of
+    // the stage can come between them and the flux loads.
+    const d4 t0 = ld4rw(a.t0, i);
+    d4 t1 = ld4rw(a.t1, i);
     double r[4] = {0.0, 0.0, 0.0, 0.0};
     if (K2MAX > 0) {
       int e[K2MAX > 0 ? K2MAX : 1];
@@ -367,17 +378,10 @@ __global__ void __launch_bounds__(kBlock) k_update(const KernelArgs a) {
       R[0] += a.force_x[i];
       R[1] += a.force_y[i];
       R[2] += a.force_z[i];
-      if (RK == 3) {  // the last reader of this step's force: reset for the IBM
-        a.force_x[i] = a.pressure_gradient;
-        a.force_y[i] = 0.0;
-        a.force_z[i] = 0.0;
-      }
     } else {
       R[0] += a.pressure_gradient;
     }
     if (a.res_debug) st4(a.res_debug, i, d4{R[0], R[1], R[2], R[3]});
-    const d4 t0 = ld4rw(a.t0, i);
-    d4 t1 = ld4rw(a.t1, i);
     const double dt = a.dt;
     double f1 = t0.w + R[3] * dt * alpha;
     double f2 = t0.x + R[0] * dt * alpha;
@@ -401,15 +405,21 @@ __global__ void __launch_bounds__(kBlock) k_update(const KernelArgs a) {
     }
     st4(a.t1, i, t1);
     st4(a.state, i, q);
+    // The last reader of this step's force resets it for the IBM. The stores
+    // come after every load of the stage: placed before the t0/t1 loads they
+    // would hold those loads back (the pointers may alias).
+    if (RK == 3 && a.force_x) {
+      a.force_x[i] = a.pressure_gradient;
+      a.force_y[i] = 0.0;
+      a.force_z[i] = 0.0;
+    }
   }
   if (RK != 3) return;
 
-  // Residual reduction: warp shuffle, block, then the last block to finish
-  // sums the per-block partials in block order (deterministic), forms the
-  // rms norms and tests convergence.
+  // Per-block squared-residual sums (warp shuffle, then the block's warps in
+  // order); k_finish reduces them.
   __shared__ double red[kBlock / 32][4];
   __shared__ int any_bad;
-  __shared__ bool last;
   if (threadIdx.x == 0) any_bad = 0;
   __syncthreads();
   if (bad) atomicOr(&any_bad, 1);
@@ -424,40 +434,40 @@ __global__ void __launch_bounds__(kBlock) k_update(const KernelArgs a) {
     double v = 0.0;
     for (int w = 0; w < kBlock / 32; w++) v += red[w][threadIdx.x];
     a.partial[4LL * blockIdx.x + threadIdx.x] = v;
-    __threadfence();  // only the writers of the partials need to publish them
   }
-  if (threadIdx.x == 0 && any_bad) atomicExch(&a.stats->diverged, 1);
+  if (threadIdx.x == 0 && any_bad) a.stats->diverged = 1;
+}
+
+// One block after the last stage: sums the per-block partials in a fixed
+// order, forms the rms norms of l2_norm_rms_moukallad (residuals.cpp:95-113)
+// and max_error (:139-147), records the step and tests convergence
+// (Solver_gpu.cu:870); a converged or diverged context halts.
+__global__ void __launch_bounds__(kFinishBlock) k_finish(const KernelArgs a) {
+  if (halted(a)) return;
+  __shared__ double red[kFinishBlock / 32][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+  for (int b = threadIdx.x; b < a.nblk_update; b += kFinishBlock) {
+    const double2 p0 = __ldg(reinterpret_cast<const double2*>(a.partial + 4LL * b));
+    const double2 p1 = __ldg(reinterpret_cast<const double2*>(a.partial + 4LL * b) + 1);
+    v[0] += p0.x;
+    v[1] += p0.y;
+    v[2] += p1.x;
+    v[3] += p1.y;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const double w = warp_sum(v[c]);
+    if (lane == 0) red[warp][c] = w;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned int done = atomicAdd(&a.stats->block_counter, 1u);
-    last = (done == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  // final pass: every thread sums a fixed strided subset of the block
-  // partials, then the same warp/block tree as above (deterministic order)
-  __shared__ double tot[4];
-  {
-    double v[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-#pragma unroll
-      for (int c = 0; c < 4; c++) v[c] += __ldcg(a.partial + 4LL * b + c);
-    }
-#pragma unroll
+    double tot[4];
     for (int c = 0; c < 4; c++) {
-      const double w = warp_sum(v[c]);
-      if (lane == 0) red[warp][c] = w;
+      tot[c] = 0.0;
+      for (int w = 0; w < kFinishBlock / 32; w++) tot[c] += red[w][c];
     }
-    __syncthreads();
-    if (threadIdx.x < 4) {
-      double t = 0.0;
-      for (int w = 0; w < kBlock / 32; w++) t += red[w][threadIdx.x];
-      tot[threadIdx.x] = t;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
     DevStats* st = a.stats;
     const double nC = (double)a.C;
     const double rho_rms = sqrt(tot[0] / nC) * a.inv_ref_rho;
@@ -475,9 +485,7 @@ __global__ void __launch_bounds__(kBlock) k_update(const KernelArgs a) {
     h[5] = w_rms;
     for (int c = 0; c < 6; c++) st->last[c] = h[c];
     st->steps = t + 1;
-    st->block_counter = 0;
-    const bool nan = !(me == me) || !(rho_rms == rho_rms);
-    if (nan) st->diverged = 1;
+    if (!(me == me) || !(rho_rms == rho_rms)) st->diverged = 1;
     if (me < a.tolerance) {
       st->converged = 1;
       st->converged_step = t;
@@ -623,7 +631,10 @@ void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t s) {
     case 0: launch_update_rk<0>(a, nb, s); break;
     case 1: launch_update_rk<1>(a, nb, s); break;
     case 2: launch_update_rk<2>(a, nb, s); break;
-    default: launch_update_rk<3>(a, nb, s); break;
+    default:
+      launch_update_rk<3>(a, nb, s);
+      k_finish<<<1, kFinishBlock, 0, s>>>(a);
+      break;
   }
 }
 void launch_seed(const KernelArgs& a, int precision, cudaStream_t s) {

@@ -40,8 +40,13 @@ __device__ __forceinline__ void stf(void* base, long long i, const f4& v) {
   reinterpret_cast<float4*>(base)[i] = make_float4(v.x, v.y, v.z, v.w);
 }
 
+// Whether the context has converged or diverged. One thread per block reads
+// the flag; every thread of the block must call this (it synchronises).
 __device__ __forceinline__ bool halted(const KernelArgs& a) {
-  return *(volatile const int*)&a.stats->halt != 0;
+  __shared__ int h;
+  if (threadIdx.x == 0) h = *(volatile const int*)&a.stats->halt;
+  __syncthreads();
+  return h != 0;
 }
 
 // Ghost state in deviation units (the same affine rules as the FP64 path).
@@ -64,7 +69,8 @@ __device__ __forceinline__ f4 ghost_state32(const f4& q, const f4& tgt, int type
 // Gradient layout: 3 x float4 per cell: (rx ry rz ux)(uy uz vx vy)(vz wx wy wz).
 __global__ void __launch_bounds__(kBlock) k_gradient32(const KernelArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.C || halted(a)) return;
+  if (halted(a)) return;
+  if (i >= a.C) return;
   const f4 qi = ldf(a.state, i);
   const float* wx = static_cast<const float*>(a.st_wx);
   const float* wy = static_cast<const float*>(a.st_wy);
@@ -191,7 +197,8 @@ __device__ __forceinline__ void lattice_pair32(const float si[4], const float sn
 // boundary handling as k_flux in kernels.cu.
 __global__ void __launch_bounds__(kFluxBlock, 4) k_flux32(const KernelArgs a) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= a.F || halted(a)) return;
+  if (halted(a)) return;
+  if (f >= a.F) return;
   const f4 f0 = ldf(a.face0, f), f1 = ldf(a.face1, f), f2 = ldf(a.face2, f);
   const int2 ids = __ldg(reinterpret_cast<const int2*>(a.face_ids) + f);
   const int o = ids.x, nb = ids.y;
@@ -297,6 +304,10 @@ __global__ void __launch_bounds__(kBlock) k_update32(const KernelArgs a) {
   double sq[4] = {0.0, 0.0, 0.0, 0.0};
   bool bad = false;
   if (i < a.C) {
+    // The RK accumulators are loaded first, with the gather, so no store of
+    // the stage can come between them and the flux loads.
+    const f4 t0 = ldf_rw(a.t0, i);
+    f4 t1 = ldf_rw(a.t1, i);
     float r[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     int e[K2MAX];
 #pragma unroll
@@ -321,17 +332,10 @@ __global__ void __launch_bounds__(kBlock) k_update32(const KernelArgs a) {
       R[0] += a.fforce_x[i];
       R[1] += a.fforce_y[i];
       R[2] += a.fforce_z[i];
-      if (RK == 3) {
-        a.fforce_x[i] = pgU;
-        a.fforce_y[i] = 0.0f;
-        a.fforce_z[i] = 0.0f;
-      }
     } else {
       R[0] += pgU;
     }
     if (a.res_debug) stf(a.res_debug, i, f4{R[0], R[1], R[2], R[3]});
-    const f4 t0 = ldf_rw(a.t0, i);
-    f4 t1 = ldf_rw(a.t1, i);
     const float dt = (float)a.dt;
     const float f1 = t0.w + R[3] * dt * alpha;
     const float f2 = t0.x + R[0] * dt * alpha;
@@ -357,12 +361,18 @@ __global__ void __launch_bounds__(kBlock) k_update32(const KernelArgs a) {
     }
     stf(a.t1, i, t1);
     stf(a.state, i, q);
+    if (RK == 3 && a.fforce_x) {  // after every load of the stage (see k_update)
+      a.fforce_x[i] = pgU;
+      a.fforce_y[i] = 0.0f;
+      a.fforce_z[i] = 0.0f;
+    }
   }
   if (RK != 3) return;
 
+  // Per-block squared-residual sums (warp shuffle, then the block's warps in
+  // order); k_finish32 reduces them.
   __shared__ double red[kBlock / 32][4];
   __shared__ int any_bad;
-  __shared__ bool last;
   if (threadIdx.x == 0) any_bad = 0;
   __syncthreads();
   if (bad) atomicOr(&any_bad, 1);
@@ -377,45 +387,47 @@ __global__ void __launch_bounds__(kBlock) k_update32(const KernelArgs a) {
     double v = 0.0;
     for (int w = 0; w < kBlock / 32; w++) v += red[w][threadIdx.x];
     a.partial[4LL * blockIdx.x + threadIdx.x] = v;
-    __threadfence();  // only the writers of the partials need to publish them
   }
-  if (threadIdx.x == 0 && any_bad) atomicExch(&a.stats->diverged, 1);
+  if (threadIdx.x == 0 && any_bad) a.stats->diverged = 1;
+}
+
+// One block after the last stage: sums the per-block partials in a fixed
+// order, forms the rms norms of l2_norm_rms_moukallad (residuals.cpp:95-113)
+// and max_error (:139-147), records the step and tests convergence
+// (Solver_gpu.cu:870); a converged or diverged context halts.
+__global__ void __launch_bounds__(kFinishBlock) k_finish32(const KernelArgs a) {
+  if (halted(a)) return;
+  __shared__ double red[kFinishBlock / 32][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+  for (int b = threadIdx.x; b < a.nblk_update; b += kFinishBlock) {
+    const double2 p0 = __ldg(reinterpret_cast<const double2*>(a.partial + 4LL * b));
+    const double2 p1 = __ldg(reinterpret_cast<const double2*>(a.partial + 4LL * b) + 1);
+    v[0] += p0.x;
+    v[1] += p0.y;
+    v[2] += p1.x;
+    v[3] += p1.y;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const double w = warp_sum(v[c]);
+    if (lane == 0) red[warp][c] = w;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned int done = atomicAdd(&a.stats->block_counter, 1u);
-    last = (done == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  __shared__ double tot[4];
-  {
-    double v[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-#pragma unroll
-      for (int c = 0; c < 4; c++) v[c] += __ldcg(a.partial + 4LL * b + c);
-    }
-#pragma unroll
+    double tot[4];
     for (int c = 0; c < 4; c++) {
-      const double w = warp_sum(v[c]);
-      if (lane == 0) red[warp][c] = w;
+      tot[c] = 0.0;
+      for (int w = 0; w < kFinishBlock / 32; w++) tot[c] += red[w][c];
     }
-    __syncthreads();
-    if (threadIdx.x < 4) {
-      double t = 0.0;
-      for (int w = 0; w < kBlock / 32; w++) t += red[w][threadIdx.x];
-      tot[threadIdx.x] = t;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
     DevStats* st = a.stats;
     const double nC = (double)a.C;
     const double rho_rms = sqrt(tot[0] / nC) * a.inv_ref_rho;
     const double u_rms = sqrt(tot[1] / nC) * a.inv_ref_mom;
     const double v_rms = sqrt(tot[2] / nC) * a.inv_ref_mom;
     const double w_rms = sqrt(tot[3] / nC) * a.inv_ref_mom;
-    const double me = fmax(fmax(w_rms, u_rms), v_rms);
+    const double me = fmax(fmax(w_rms, u_rms), v_rms);  // residuals::max_error
     const long long t = st->steps;
     double* h = st->history[t % kHistoryCap];
     h[0] = (double)t;
@@ -426,7 +438,6 @@ __global__ void __launch_bounds__(kBlock) k_update32(const KernelArgs a) {
     h[5] = w_rms;
     for (int c = 0; c < 6; c++) st->last[c] = h[c];
     st->steps = t + 1;
-    st->block_counter = 0;
     if (!(me == me) || !(rho_rms == rho_rms)) st->diverged = 1;
     if (me < a.tolerance) {
       st->converged = 1;
@@ -563,7 +574,10 @@ void launch_update32(const KernelArgs& a, int rk, cudaStream_t s) {
     case 0: launch_update32_rk<0>(a, nb, s); break;
     case 1: launch_update32_rk<1>(a, nb, s); break;
     case 2: launch_update32_rk<2>(a, nb, s); break;
-    default: launch_update32_rk<3>(a, nb, s); break;
+    default:
+      launch_update32_rk<3>(a, nb, s);
+      k_finish32<<<1, kFinishBlock, 0, s>>>(a);
+      break;
   }
 }
 void launch_seed32(const KernelArgs& a, cudaStream_t s) {

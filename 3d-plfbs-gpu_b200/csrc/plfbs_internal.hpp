@@ -91,17 +91,19 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
 constexpr int kHistoryCap = 4096;   // per-step residual records kept on the device
 constexpr int kBlock = 256;         // threads per block of the cell kernels
 constexpr int kFluxBlock = 128;     // threads per block of the face-flux kernel (128 registers, 4 blocks/SM)
+constexpr int kFinishBlock = 1024;  // the one block that reduces the per-block residual sums
 
-// Run status shared by all kernels of a step, in device memory.
+// Run status shared by all kernels of a step, in device memory. The halt flag
+// is read by every block of every kernel; k_finish writes it once per step.
 struct DevStats {
-  unsigned int block_counter;  // last-block-done detection in the reduction
   int halt;                    // 1 once converged or diverged: kernels return at entry
   int converged;
   int diverged;
+  int pad0;
   long long steps;             // completed time steps
   long long converged_step;
   double last[6];              // t, max_error, rho, u, v, w rms of the last step
-  double history[kHistoryCap][6];
+  alignas(128) double history[kHistoryCap][6];
 };
 
 struct KernelArgs {

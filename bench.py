@@ -46,7 +46,7 @@ WORKLOAD = "sphere_channel_128x64x64_ibm3217_fp64"
 NX, NY, NZ = 128, 64, 64
 DIAM, CENTRE, NNODES = 16.0, (32.0, 32.0, 32.0), 3217
 U, RE, DT, STIFFNESS = 0.05, 100.0, 0.2, 0.5
-KERNELS_PER_STEP = 13  # ibm + 4 x (gradient, flux, update)
+KERNELS_PER_STEP = 14  # ibm + 4 x (gradient, flux, update) + finish
 
 # Algorithmic bytes per launch (FP64, perfect reuse): per face the geometry
 # (normal, area, streaming dt, owner/neighbour offsets: 72 B) and the flux
