@@ -288,6 +288,8 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   a.grad = p;
   if ((rc = dev_alloc(ctx, &p, (size_t)L.F * e4))) return fail(rc);
   a.flux = p;
+  if ((rc = dev_upload(ctx, &p, L.face_ids))) return fail(rc);
+  a.face_ids = static_cast<const int32_t*>(p);
   plfbs::Layout32 L32;
   if (fp32) {
     plfbs::build_layout32(L, cfg->ref_rho, cfg->max_velocity, L32);
@@ -297,8 +299,6 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     a.face1 = p;
     if ((rc = dev_upload(ctx, &p, L32.face2))) return fail(rc);
     a.face2 = p;
-    if ((rc = dev_upload(ctx, &p, L32.face_ids))) return fail(rc);
-    a.face_ids = static_cast<const int32_t*>(p);
     if ((rc = dev_upload(ctx, &p, L32.bc0))) return fail(rc);
     a.bc0 = p;
     if ((rc = dev_upload(ctx, &p, L32.bc1))) return fail(rc);

@@ -159,19 +159,35 @@ __device__ __forceinline__ double edot(const double* g) {
   return s;
 }
 
+// e . g of a gradient inside lattice_pair. The diagonal pairs (all of e's
+// components nonzero) come after the axis pairs and see each gradient as
+// (gx + gy, gx - gy, gz); every diagonal e . g is then one addition, and
+// rounds exactly as edot's (gx +- gy) +- gz.
+template <int EX, int EY, int EZ>
+__device__ __forceinline__ double gdot(const double* g) {
+  if (EX == 0 || EY == 0 || EZ == 0) return edot<EX, EY, EZ>(g);
+  static_assert(!(EX && EY && EZ) || EX == 1 || (EY == 1 && EZ == 1), "diagonal set");
+  if (EX == 1 && EY == 1) return EZ > 0 ? g[0] + g[2] : g[0] - g[2];
+  if (EX == 1) return g[1] + g[2];  // (1, -1, 1)
+  return g[2] - g[1];               // (-1, 1, 1)
+}
+
 // One opposite pair (k, k') of D3Q15 lattice nodes, e_k' = -e_k = -e, node k
 // at x_f - e dt_s (populate_lattice_macros, LBFS.cu:330-938). With s = e . n:
 // s > d1 takes node k from the owner side and k' from the neighbour side,
 // s < -d1 the reverse, otherwise both from the face average with averaged
 // gradients (the +-0.001 dt dead band, LBFS.cu:353-354). Their equilibria
 // (populate_feq, LBFS.cu:942-1038) are accumulated into the moments
-// rho_I, m = sum e f and P = sum e e^T f (xx, yy, zz, xy, xz, yz).
+// rho_I, m = sum e f and P = sum e e^T f (xx, yy, zz, xy, xz, yz). A diagonal
+// pair adds the same f_k + f_k' to rho_I, P_xx, P_yy and P_zz: those pairs sum
+// it once into D, which the caller adds to the four.
 template <int EX, int EY, int EZ>
 __device__ __forceinline__ void lattice_pair(const double si[4], const double sn[4],
                                              const double sc[4], const double g1[12],
                                              const double g2[12], const double n[3], double d1,
                                              double dt, double c45, double c15, double wgt,
-                                             double& rhoI, double m[3], double P[6]) {
+                                             double& rhoI, double m[3], double P[6], double& D) {
+  constexpr bool diag = EX != 0 && EY != 0 && EZ != 0;
   const double s = (EX ? (EX > 0 ? n[0] : -n[0]) : 0.0) + (EY ? (EY > 0 ? n[1] : -n[1]) : 0.0) +
                    (EZ ? (EZ > 0 ? n[2] : -n[2]) : 0.0);
   // Faces are sorted by their branch signature, so these branches are
@@ -180,20 +196,20 @@ __device__ __forceinline__ void lattice_pair(const double si[4], const double sn
   if (s > d1) {
 #pragma unroll
     for (int f = 0; f < 4; f++) {
-      qa[f] = fma(-edot<EX, EY, EZ>(g1 + 3 * f), dt, si[f]);
-      qb[f] = fma(edot<EX, EY, EZ>(g2 + 3 * f), dt, sn[f]);
+      qa[f] = fma(-gdot<EX, EY, EZ>(g1 + 3 * f), dt, si[f]);
+      qb[f] = fma(gdot<EX, EY, EZ>(g2 + 3 * f), dt, sn[f]);
     }
   } else if (s < -d1) {
 #pragma unroll
     for (int f = 0; f < 4; f++) {
-      qa[f] = fma(-edot<EX, EY, EZ>(g2 + 3 * f), dt, sn[f]);
-      qb[f] = fma(edot<EX, EY, EZ>(g1 + 3 * f), dt, si[f]);
+      qa[f] = fma(-gdot<EX, EY, EZ>(g2 + 3 * f), dt, sn[f]);
+      qb[f] = fma(gdot<EX, EY, EZ>(g1 + 3 * f), dt, si[f]);
     }
   } else {
     const double hdt = 0.5 * dt;  // e . (g1 + g2) / 2 dt
 #pragma unroll
     for (int f = 0; f < 4; f++) {
-      const double e = edot<EX, EY, EZ>(g1 + 3 * f) + edot<EX, EY, EZ>(g2 + 3 * f);
+      const double e = gdot<EX, EY, EZ>(g1 + 3 * f) + gdot<EX, EY, EZ>(g2 + 3 * f);
       qa[f] = fma(-e, hdt, sc[f]);
       qb[f] = fma(e, hdt, sc[f]);
     }
@@ -208,13 +224,17 @@ __device__ __forceinline__ void lattice_pair(const double si[4], const double sn
   const double fb =
       wgt * qb[0] * fma(-c15, u2b, fma(c45 * eub, eub, fma(3.0, eub, 1.0)));
   const double sum = fa + fb, dif = fa - fb;
-  rhoI += sum;
   if (EX) m[0] += EX > 0 ? dif : -dif;
   if (EY) m[1] += EY > 0 ? dif : -dif;
   if (EZ) m[2] += EZ > 0 ? dif : -dif;
-  if (EX) P[0] += sum;
-  if (EY) P[1] += sum;
-  if (EZ) P[2] += sum;
+  if (diag) {
+    D += sum;
+  } else {
+    rhoI += sum;
+    if (EX) P[0] += sum;
+    if (EY) P[1] += sum;
+    if (EZ) P[2] += sum;
+  }
   if (EX && EY) P[3] += (EX * EY > 0) ? sum : -sum;
   if (EX && EZ) P[4] += (EX * EZ > 0) ? sum : -sum;
   if (EY && EZ) P[5] += (EY * EZ > 0) ? sum : -sum;
@@ -231,16 +251,15 @@ __device__ __forceinline__ void lattice_pair(const double si[4], const double sn
 // The face flux is (momentum, mass) = ((sum e e^T f) n, (sum e f) . n) A.
 // A boundary face (neighbour > n_cells in the reference) takes both sides from
 // the boundary value and all gradients from the ghost (LBFS.cu:356-401).
-__global__ void __launch_bounds__(kFluxBlock, 4) k_flux(const KernelArgs a) {
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (halted(a)) return;
-  if (f >= a.F) return;
+__device__ __forceinline__ int2 face_ids(const KernelArgs& a, long long f) {
+  return __ldg(reinterpret_cast<const int2*>(a.face_ids) + f);
+}
+
+__device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, const int2 ids) {
   const d4 f0 = ld4(a.face0, f), f1 = ld4(a.face1, f), f2 = ld4(a.face2, f);
-  uint64_t ids;
-  memcpy(&ids, &f2.w, sizeof ids);
-  const int o = (int)(uint32_t)(ids & 0xffffffffu), nb = (int)(uint32_t)(ids >> 32);
+  const int o = ids.x, nb = ids.y;
   const double n[3] = {f0.x, f0.y, f0.z};
-  const double area = f0.w, dt = f1.x;
+  const double area = f0.w, dt = f1.x, f2w = f2.w;
   const double t1[3] = {f1.y, f1.z, f1.w}, t2[3] = {f2.x, f2.y, f2.z};
 
   const d4 qo = ld4(a.state, o);
@@ -296,15 +315,29 @@ __global__ void __launch_bounds__(kFluxBlock, 4) k_flux(const KernelArgs a) {
   double rhoI = w0 * sc[0] * fma(-c15, u2c, 1.0);
   double m[3] = {0.0, 0.0, 0.0};
   double P[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  lattice_pair<1, 0, 0>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w1, rhoI, m, P);
-  lattice_pair<0, 1, 0>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w1, rhoI, m, P);
-  lattice_pair<0, 0, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w1, rhoI, m, P);
-  lattice_pair<1, 1, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P);
-  lattice_pair<1, 1, -1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P);
-  lattice_pair<1, -1, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P);
-  lattice_pair<-1, 1, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P);
+  double D = 0.0;
+  lattice_pair<1, 0, 0>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w1, rhoI, m, P, D);
+  lattice_pair<0, 1, 0>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w1, rhoI, m, P, D);
+  lattice_pair<0, 0, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w1, rhoI, m, P, D);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {  // (gx, gy, gz) -> (gx + gy, gx - gy, gz), see gdot
+    const double s1 = g1[3 * k] + g1[3 * k + 1], r1 = g1[3 * k] - g1[3 * k + 1];
+    const double s2 = g2[3 * k] + g2[3 * k + 1], r2 = g2[3 * k] - g2[3 * k + 1];
+    g1[3 * k] = s1;
+    g1[3 * k + 1] = r1;
+    g2[3 * k] = s2;
+    g2[3 * k + 1] = r2;
+  }
+  lattice_pair<1, 1, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<1, 1, -1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<1, -1, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<-1, 1, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P, D);
+  rhoI += D;
+  P[0] += D;
+  P[1] += D;
+  P[2] += D;
 
-  const double tau = a.visc3 / dt * pg;
+  const double tau = f2w;  // 3 nu / (dt_s gamma), per face from the layout
   const double mn = m[0] * n[0] + m[1] * n[1] + m[2] * n[2];
   const double Pn[3] = {P[0] * n[0] + P[3] * n[1] + P[4] * n[2],
                         P[3] * n[0] + P[1] * n[1] + P[5] * n[2],
@@ -317,6 +350,27 @@ __global__ void __launch_bounds__(kFluxBlock, 4) k_flux(const KernelArgs a) {
   out.z = ((1.0 - tau) * fma(m[2], mnr, p3 * n[2]) + tau * Pn[2]) * area;
   out.w = mn * area;
   st4(a.flux, f, out);
+}
+
+// Persistent over the faces (grid stride): the owner/neighbour ids of a
+// thread's next face are loaded before its current face is computed, so the
+// next face's cell gathers do not wait behind a load of its face record.
+// Three blocks per SM leave 168 registers a thread, enough to hold a face's
+// gradients without spilling.
+__global__ void __launch_bounds__(kFluxBlock, 3) k_flux(const KernelArgs a) {
+  if (halted(a)) return;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= a.F) return;
+  int2 ids = face_ids(a, f);
+  for (;;) {
+    const long long fn = f + stride;
+    const int2 next = fn < a.F ? face_ids(a, fn) : make_int2(0, 0);
+    flux_face(a, (int)f, ids);
+    if (fn >= a.F) break;
+    f = fn;
+    ids = next;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -611,7 +665,8 @@ void launch_gradient(const KernelArgs& a, int precision, cudaStream_t s) {
 }
 void launch_flux(const KernelArgs& a, int precision, cudaStream_t s) {
   if (precision == PLFBS_FP32_DEVIATION) return launch_flux32(a, s);
-  k_flux<<<blocks_for(a.F, kFluxBlock), kFluxBlock, 0, s>>>(a);
+  static std::atomic<int> resident[kMaxDevices];
+  k_flux<<<persistent_blocks(k_flux, kFluxBlock, a.F, resident), kFluxBlock, 0, s>>>(a);
 }
 template <int RK>
 static void launch_update_rk(const KernelArgs& a, int nb, cudaStream_t s) {

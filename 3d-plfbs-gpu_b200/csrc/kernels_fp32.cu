@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(kFluxBlock, 4) k_flux32(const KernelArgs a) {
   lattice_pair32<1, -1, 1>(si, sn, sc, g1, g2, n, kc, w7, drhoI, m, P);
   lattice_pair32<-1, 1, 1>(si, sn, sc, g1, g2, n, kc, w7, drhoI, m, P);
 
-  const float tau = (float)a.visc3 / dt * pg;
+  const float tau = f2.w;  // 3 nu / (dt_s gamma), per face from the layout
   const float mn = m[0] * n[0] + m[1] * n[1] + m[2] * n[2];
   const float Pn[3] = {P[0] * n[0] + P[3] * n[1] + P[4] * n[2],
                        P[3] * n[0] + P[1] * n[1] + P[5] * n[2],

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -34,9 +35,10 @@ struct Layout {
   // Face records, 3 x 4 doubles per face (structure of arrays):
   //   face0 = (n.x, n.y, n.z, area)
   //   face1 = (streaming dt, t1.x, t1.y, t1.z)   t1 = owner centroid - face centroid
-  //   face2 = (t2.x, t2.y, t2.z, ids)            t2 = neighbour centroid - face centroid
-  // ids packs the new owner (low 32 bits) and new neighbour (high 32 bits).
+  //   face2 = (t2.x, t2.y, t2.z, tau)            t2 = neighbour centroid - face centroid,
+  //                                              tau = 3 nu / (dt_s gamma)
   std::vector<double> face0, face1, face2;  // [4F] each
+  std::vector<int32_t> face_ids;            // [2F] new owner, new neighbour (or C + bc)
 
   // Boundary records, 4 x 4 doubles per boundary face (structure of arrays):
   //   bc0 = raw boundary value (u, v, w, rho)
@@ -64,8 +66,7 @@ struct Layout {
 // in FP64 first), boundary values expressed as deviations (rho - rho0,
 // velocity / U), face ids moved to their own int2 array.
 struct Layout32 {
-  std::vector<float> face0, face1, face2;        // [4F] (n, A), (dt_s, t1), (t2, 0)
-  std::vector<int32_t> face_ids;                 // [2F] new owner, new neighbour
+  std::vector<float> face0, face1, face2;        // [4F] (n, A), (dt_s, t1), (t2, tau)
   std::vector<float> bc0, bc1, bc2, bc3;         // [4B]
   std::vector<float> st_wx, st_wy, st_wz;        // [K*C]
   std::vector<float> inv_volume;                 // [C]
@@ -92,6 +93,7 @@ constexpr int kHistoryCap = 4096;   // per-step residual records kept on the dev
 constexpr int kBlock = 256;         // threads per block of the cell kernels
 constexpr int kFluxBlock = 128;     // threads per block of the face-flux kernel (128 registers, 4 blocks/SM)
 constexpr int kFinishBlock = 1024;  // the one block that reduces the per-block residual sums
+constexpr int kMaxDevices = 64;     // per-device caches of launch shapes
 
 // Run status shared by all kernels of a step, in device memory. The halt flag
 // is read by every block of every kernel; k_finish writes it once per step.
@@ -158,5 +160,29 @@ void launch_gradient32(const KernelArgs& a, cudaStream_t stream);
 void launch_flux32(const KernelArgs& a, cudaStream_t stream);
 void launch_update32(const KernelArgs& a, int rk, cudaStream_t stream);
 void launch_seed32(const KernelArgs& a, cudaStream_t stream);
+
+#ifdef __CUDACC__
+// Blocks of a grid-stride kernel: as many as are resident on the device at
+// once (occupancy x SMs, cached per device), at most one per `block` items.
+template <typename Kernel>
+int persistent_blocks(Kernel kernel, int block, long long n, std::atomic<int>* cache) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) dev = 0;
+  int r = cache[dev].load(std::memory_order_relaxed);
+  if (r <= 0) {
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        per_sm <= 0 || sms <= 0) {
+      per_sm = 1;
+      sms = 148;
+    }
+    r = per_sm * sms;
+    cache[dev].store(r, std::memory_order_relaxed);
+  }
+  const long long need = (n + block - 1) / block;
+  return (int)(need < r ? (need > 0 ? need : 1) : r);
+}
+#endif
 
 }  // namespace plfbs

@@ -322,6 +322,8 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
   L.face0.assign(4 * (size_t)F, 0.0);
   L.face1.assign(4 * (size_t)F, 0.0);
   L.face2.assign(4 * (size_t)F, 0.0);
+  L.face_ids.assign(2 * (size_t)F, 0);
+  const double visc3 = cfg.visc * 3, pg = 1.0 / cfg.gamma;
   for (int k = 0; k < F; k++) {
     const int f = L.face_old_of_new[k];
     const int o = m.owner[f], nbo = m.neighbour[f];
@@ -343,8 +345,10 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
     c[0] = c2[0] - xf[0];  // cell_2 - interface_node, LBFS.cu:344
     c[1] = c2[1] - xf[1];
     c[2] = c2[2] - xf[2];
-    const uint64_t ids = (uint64_t)(uint32_t)newc(o) | ((uint64_t)(uint32_t)newcell(nbo) << 32);
-    std::memcpy(&c[3], &ids, sizeof ids);
+    // relaxation factor 3 nu / (dt_s gamma) (calculate_flux_at_interface, LBFS.cu:1042-1223)
+    c[3] = visc3 / m.streaming_dt[f] * pg;
+    L.face_ids[2 * (size_t)k] = newc(o);
+    L.face_ids[2 * (size_t)k + 1] = newcell(nbo);
   }
 
   // --- boundary records --------------------------------------------------------
@@ -448,15 +452,7 @@ void build_layout32(const Layout& L, double rho0, double uref, Layout32& o) {
   };
   o.face0 = cast(L.face0);
   o.face1 = cast(L.face1);
-  o.face2.assign(4 * F, 0.0f);
-  o.face_ids.resize(2 * F);
-  for (size_t k = 0; k < F; k++) {
-    for (int c = 0; c < 3; c++) o.face2[4 * k + c] = (float)L.face2[4 * k + c];
-    uint64_t ids;
-    std::memcpy(&ids, &L.face2[4 * k + 3], sizeof ids);
-    o.face_ids[2 * k] = (int32_t)(uint32_t)(ids & 0xffffffffu);
-    o.face_ids[2 * k + 1] = (int32_t)(uint32_t)(ids >> 32);
-  }
+  o.face2 = cast(L.face2);  // (t2, relaxation factor)
   // boundary values as deviations: velocity / U, rho - rho0
   auto dev = [&](const std::vector<double>& v) {
     std::vector<float> r(v.size());
