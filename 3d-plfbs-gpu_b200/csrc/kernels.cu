@@ -81,39 +81,58 @@ __device__ __forceinline__ d4 ghost_state(const d4& q, const d4& tgt, int types)
 // Gradient layout: 3 x d4 per cell = (rx, ry, rz, ux), (uy, uz, vx, vy),
 // (vz, wx, wy, wz).
 // ---------------------------------------------------------------------------
-// One thread per cell walking its stencil slots. (Loading all slots up front
-// needs ~100 registers and measured slower than this 62-register loop.)
+// One thread per cell. The neighbour ids of up to kStencilUnroll slots are
+// loaded first, then every slot's weights and neighbour state, so a cell waits
+// for two rounds of loads rather than two per slot; wider stencils fall back
+// to walking the slots.
+template <bool GHOSTS>
+__device__ __forceinline__ void gradient_slot(const KernelArgs& a, int i, long long s, int j,
+                                              const d4& qi, double g[12]) {
+  d4 qj;
+  if (!GHOSTS || j < a.C) {
+    qj = ld4(a.state, j);
+  } else {
+    const int b = j - a.C;
+    const d4 tgt = ld4(a.bc1, b);
+    const int types = (int)__ldg(reinterpret_cast<const double*>(a.bc3) + 4LL * b + 3);
+    qj = ghost_state(qi, tgt, types);
+    st4(a.state, j, qj);  // the ghost's only reader in this kernel is its owner
+  }
+  const double w[3] = {__ldg(static_cast<const double*>(a.st_wx) + s),
+                       __ldg(static_cast<const double*>(a.st_wy) + s),
+                       __ldg(static_cast<const double*>(a.st_wz) + s)};
+  const double d[4] = {qj.w - qi.w, qj.x - qi.x, qj.y - qi.y, qj.z - qi.z};
+#pragma unroll
+  for (int f = 0; f < 4; f++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) g[3 * f + c] = fma(w[c], d[f], g[3 * f + c]);
+}
+
+constexpr int kStencilUnroll = 8;
+
 __global__ void __launch_bounds__(kBlock) k_gradient(const KernelArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (halted(a)) return;
   if (i >= a.C) return;
   const d4 qi = ld4(a.state, i);
-  const double* wx = static_cast<const double*>(a.st_wx);
-  const double* wy = static_cast<const double*>(a.st_wy);
-  const double* wz = static_cast<const double*>(a.st_wz);
   double g[12];
 #pragma unroll
   for (int k = 0; k < 12; k++) g[k] = 0.0;
-  for (int k = 0; k < a.K; k++) {
-    const long long s = (long long)k * a.C + i;
-    const int j = __ldg(a.st_nbr + s);
-    if (j < 0) break;
-    d4 qj;
-    if (j < a.C) {
-      qj = ld4(a.state, j);
-    } else {
-      const int b = j - a.C;
-      const d4 tgt = ld4(a.bc1, b);
-      const int types = (int)__ldg(reinterpret_cast<const double*>(a.bc3) + 4LL * b + 3);
-      qj = ghost_state(qi, tgt, types);
-      st4(a.state, j, qj);
+  if (a.K <= kStencilUnroll) {
+    int jj[kStencilUnroll];
+#pragma unroll
+    for (int k = 0; k < kStencilUnroll; k++)
+      jj[k] = k < a.K ? __ldg(a.st_nbr + (long long)k * a.C + i) : -1;
+#pragma unroll
+    for (int k = 0; k < kStencilUnroll; k++)
+      if (jj[k] >= 0) gradient_slot<true>(a, i, (long long)k * a.C + i, jj[k], qi, g);
+  } else {
+    for (int k = 0; k < a.K; k++) {
+      const long long s = (long long)k * a.C + i;
+      const int j = __ldg(a.st_nbr + s);
+      if (j < 0) break;
+      gradient_slot<true>(a, i, s, j, qi, g);
     }
-    const double w[3] = {__ldg(wx + s), __ldg(wy + s), __ldg(wz + s)};
-    const double d[4] = {qj.w - qi.w, qj.x - qi.x, qj.y - qi.y, qj.z - qi.z};
-#pragma unroll
-    for (int f = 0; f < 4; f++)
-#pragma unroll
-      for (int c = 0; c < 3; c++) g[3 * f + c] = fma(w[c], d[f], g[3 * f + c]);
   }
   st4(a.grad, 3LL * i + 0, d4{g[0], g[1], g[2], g[3]});
   st4(a.grad, 3LL * i + 1, d4{g[4], g[5], g[6], g[7]});

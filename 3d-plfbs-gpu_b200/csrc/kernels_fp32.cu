@@ -135,6 +135,16 @@ __device__ __forceinline__ float edotf(const float* g) {
   return s;
 }
 
+// e . g of a gradient; diagonal pairs see (gx + gy, gx - gy, gz) (as gdot in
+// kernels.cu).
+template <int EX, int EY, int EZ>
+__device__ __forceinline__ float gdotf(const float* g) {
+  if (EX == 0 || EY == 0 || EZ == 0) return edotf<EX, EY, EZ>(g);
+  if (EX == 1 && EY == 1) return EZ > 0 ? g[0] + g[2] : g[0] - g[2];
+  if (EX == 1) return g[1] + g[2];  // (1, -1, 1)
+  return g[2] - g[1];               // (-1, 1, 1)
+}
+
 // Consts shared by the lattice pairs of one face.
 struct PairConst {
   float d1, dt, hdt;
@@ -154,26 +164,27 @@ __device__ __forceinline__ void lattice_pair32(const float si[4], const float sn
                                                const float sc[4], const float g1[12],
                                                const float g2[12], const float n[3],
                                                const PairConst& k, float wgt, float& drhoI,
-                                               float m[3], float P[6]) {
+                                               float m[3], float P[6], float& D) {
+  constexpr bool diag = EX != 0 && EY != 0 && EZ != 0;
   const float s = (EX ? (EX > 0 ? n[0] : -n[0]) : 0.0f) + (EY ? (EY > 0 ? n[1] : -n[1]) : 0.0f) +
                   (EZ ? (EZ > 0 ? n[2] : -n[2]) : 0.0f);
   float qa[4], qb[4];
   if (s > k.d1) {
 #pragma unroll
     for (int f = 0; f < 4; f++) {
-      qa[f] = fmaf(-edotf<EX, EY, EZ>(g1 + 3 * f), k.dt, si[f]);
-      qb[f] = fmaf(edotf<EX, EY, EZ>(g2 + 3 * f), k.dt, sn[f]);
+      qa[f] = fmaf(-gdotf<EX, EY, EZ>(g1 + 3 * f), k.dt, si[f]);
+      qb[f] = fmaf(gdotf<EX, EY, EZ>(g2 + 3 * f), k.dt, sn[f]);
     }
   } else if (s < -k.d1) {
 #pragma unroll
     for (int f = 0; f < 4; f++) {
-      qa[f] = fmaf(-edotf<EX, EY, EZ>(g2 + 3 * f), k.dt, sn[f]);
-      qb[f] = fmaf(edotf<EX, EY, EZ>(g1 + 3 * f), k.dt, si[f]);
+      qa[f] = fmaf(-gdotf<EX, EY, EZ>(g2 + 3 * f), k.dt, sn[f]);
+      qb[f] = fmaf(gdotf<EX, EY, EZ>(g1 + 3 * f), k.dt, si[f]);
     }
   } else {
 #pragma unroll
     for (int f = 0; f < 4; f++) {
-      const float e = edotf<EX, EY, EZ>(g1 + 3 * f) + edotf<EX, EY, EZ>(g2 + 3 * f);
+      const float e = gdotf<EX, EY, EZ>(g1 + 3 * f) + gdotf<EX, EY, EZ>(g2 + 3 * f);
       qa[f] = fmaf(-e, k.hdt, sc[f]);
       qb[f] = fmaf(e, k.hdt, sc[f]);
     }
@@ -181,13 +192,17 @@ __device__ __forceinline__ void lattice_pair32(const float si[4], const float sn
   const float fa = feq_dev(k, wgt, qa, edotf<EX, EY, EZ>(qa + 1));
   const float fb = feq_dev(k, wgt, qb, -edotf<EX, EY, EZ>(qb + 1));
   const float sum = fa + fb, dif = fa - fb;
-  drhoI += sum;
   if (EX) m[0] += EX > 0 ? dif : -dif;
   if (EY) m[1] += EY > 0 ? dif : -dif;
   if (EZ) m[2] += EZ > 0 ? dif : -dif;
-  if (EX) P[0] += sum;
-  if (EY) P[1] += sum;
-  if (EZ) P[2] += sum;
+  if (diag) {
+    D += sum;
+  } else {
+    drhoI += sum;
+    if (EX) P[0] += sum;
+    if (EY) P[1] += sum;
+    if (EZ) P[2] += sum;
+  }
   if (EX && EY) P[3] += (EX * EY > 0) ? sum : -sum;
   if (EX && EZ) P[4] += (EX * EZ > 0) ? sum : -sum;
   if (EY && EZ) P[5] += (EY * EZ > 0) ? sum : -sum;
@@ -195,12 +210,8 @@ __device__ __forceinline__ void lattice_pair32(const float si[4], const float sn
 
 // Face flux in deviation form (see the file comment); the same branches and
 // boundary handling as k_flux in kernels.cu.
-__global__ void __launch_bounds__(kFluxBlock, 4) k_flux32(const KernelArgs a) {
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (halted(a)) return;
-  if (f >= a.F) return;
+__device__ __forceinline__ void flux_face32(const KernelArgs& a, const int f, const int2 ids) {
   const f4 f0 = ldf(a.face0, f), f1 = ldf(a.face1, f), f2 = ldf(a.face2, f);
-  const int2 ids = __ldg(reinterpret_cast<const int2*>(a.face_ids) + f);
   const int o = ids.x, nb = ids.y;
   const float n[3] = {f0.x, f0.y, f0.z};
   const float area = f0.w, dt = f1.x;
@@ -262,13 +273,27 @@ __global__ void __launch_bounds__(kFluxBlock, 4) k_flux32(const KernelArgs a) {
   float drhoI = w0 * fmaf(kc.rho0 + sc[0], kc.U * (-kc.c15u * u2c), sc[0]);
   float m[3] = {0.0f, 0.0f, 0.0f};
   float P[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-  lattice_pair32<1, 0, 0>(si, sn, sc, g1, g2, n, kc, w1, drhoI, m, P);
-  lattice_pair32<0, 1, 0>(si, sn, sc, g1, g2, n, kc, w1, drhoI, m, P);
-  lattice_pair32<0, 0, 1>(si, sn, sc, g1, g2, n, kc, w1, drhoI, m, P);
-  lattice_pair32<1, 1, 1>(si, sn, sc, g1, g2, n, kc, w7, drhoI, m, P);
-  lattice_pair32<1, 1, -1>(si, sn, sc, g1, g2, n, kc, w7, drhoI, m, P);
-  lattice_pair32<1, -1, 1>(si, sn, sc, g1, g2, n, kc, w7, drhoI, m, P);
-  lattice_pair32<-1, 1, 1>(si, sn, sc, g1, g2, n, kc, w7, drhoI, m, P);
+  float D = 0.0f;
+  lattice_pair32<1, 0, 0>(si, sn, sc, g1, g2, n, kc, w1, drhoI, m, P, D);
+  lattice_pair32<0, 1, 0>(si, sn, sc, g1, g2, n, kc, w1, drhoI, m, P, D);
+  lattice_pair32<0, 0, 1>(si, sn, sc, g1, g2, n, kc, w1, drhoI, m, P, D);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {  // (gx, gy, gz) -> (gx + gy, gx - gy, gz), see gdotf
+    const float s1 = g1[3 * k] + g1[3 * k + 1], r1 = g1[3 * k] - g1[3 * k + 1];
+    const float s2 = g2[3 * k] + g2[3 * k + 1], r2 = g2[3 * k] - g2[3 * k + 1];
+    g1[3 * k] = s1;
+    g1[3 * k + 1] = r1;
+    g2[3 * k] = s2;
+    g2[3 * k + 1] = r2;
+  }
+  lattice_pair32<1, 1, 1>(si, sn, sc, g1, g2, n, kc, w7, drhoI, m, P, D);
+  lattice_pair32<1, 1, -1>(si, sn, sc, g1, g2, n, kc, w7, drhoI, m, P, D);
+  lattice_pair32<1, -1, 1>(si, sn, sc, g1, g2, n, kc, w7, drhoI, m, P, D);
+  lattice_pair32<-1, 1, 1>(si, sn, sc, g1, g2, n, kc, w7, drhoI, m, P, D);
+  drhoI += D;
+  P[0] += D;
+  P[1] += D;
+  P[2] += D;
 
   const float tau = f2.w;  // 3 nu / (dt_s gamma), per face from the layout
   const float mn = m[0] * n[0] + m[1] * n[1] + m[2] * n[2];
@@ -284,6 +309,25 @@ __global__ void __launch_bounds__(kFluxBlock, 4) k_flux32(const KernelArgs a) {
   out.z = ((1.0f - tau) * fmaf(m[2], mnr, p3 * n[2]) + tau * Pn[2]) * sA;
   out.w = mn * area;
   stf(a.flux, f, out);
+}
+
+// Persistent over the faces, next face's ids prefetched (as k_flux); six blocks
+// per SM (85 registers) measured fastest.
+__global__ void __launch_bounds__(kFluxBlock, 6) k_flux32(const KernelArgs a) {
+  if (halted(a)) return;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= a.F) return;
+  int2 ids = __ldg(reinterpret_cast<const int2*>(a.face_ids) + f);
+  for (;;) {
+    const long long fn = f + stride;
+    const int2 next =
+        fn < a.F ? __ldg(reinterpret_cast<const int2*>(a.face_ids) + fn) : make_int2(0, 0);
+    flux_face32(a, (int)f, ids);
+    if (fn >= a.F) break;
+    f = fn;
+    ids = next;
+  }
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -566,7 +610,8 @@ void launch_gradient32(const KernelArgs& a, cudaStream_t s) {
   k_gradient32<<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
 }
 void launch_flux32(const KernelArgs& a, cudaStream_t s) {
-  k_flux32<<<blocks_for(a.F, kFluxBlock), kFluxBlock, 0, s>>>(a);
+  static std::atomic<int> resident[kMaxDevices];
+  k_flux32<<<persistent_blocks(k_flux32, kFluxBlock, a.F, resident), kFluxBlock, 0, s>>>(a);
 }
 void launch_update32(const KernelArgs& a, int rk, cudaStream_t s) {
   const int nb = blocks_for(a.C, kBlock);
