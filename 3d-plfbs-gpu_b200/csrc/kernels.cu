@@ -13,8 +13,8 @@
 //                                 and tests convergence on the device
 //                                 [add, time_integration, square/total<256>,
 //                                  l2_norm_rms_moukallad]
-//   ibm       (thread per node)  interpolation, advection, spring force and
-//                                 spreading with warp-aggregated atomics
+//   ibm       (8 threads/node)   interpolation, advection, spring force and
+//                                 spreading with FP64 atomics
 //
 // All of them are bandwidth kernels (no dense contraction: tensor cores do not
 // apply). Memory per cell is laid out for coalesced 32-byte accesses.
@@ -577,8 +577,8 @@ __global__ void k_seed(const KernelArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// IBM (immersed_boundary_method.cu:13-90, 161-190, 244-295, 299-375), one
-// thread per node, once per time step before the RK stages.
+// IBM (immersed_boundary_method.cu:13-90, 161-190, 244-295, 299-375), once
+// per time step before the RK stages.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void stencil_origin(const KernelArgs& a, const double x[3],
                                                double r[3], int lo[3]) {
@@ -589,88 +589,71 @@ __device__ __forceinline__ void stencil_origin(const KernelArgs& a, const double
   for (int c = 0; c < 3; c++) lo[c] = (int)round(r[c]) - 1;
 }
 
-__global__ void __launch_bounds__(128) k_ibm(const KernelArgs a) {
-  const int nd = blockIdx.x * blockDim.x + threadIdx.x;
+// Eight threads per node, one per cell of its 2 x 2 x 2 stencil: each loads
+// its cell's state, the node's velocity is the sum over the eight (xor
+// butterfly, so every lane holds the same bits), every lane advances the node
+// and forms its force, and each lane spreads to its own cell with FP64
+// atomics. Lane 0 of a node writes the node's arrays.
+__global__ void __launch_bounds__(kIbmBlock) k_ibm(const KernelArgs a) {
   if (halted(a)) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nd = t >> 3, sub = t & 7;
   const bool active = nd < a.N;
   const int xc = a.ibm_xc, yc = a.ibm_yc;
-  double fx = 0.0, fy = 0.0, fz = 0.0;
-  double r[3];
-  int lo[3];
+  double x[3] = {0.0, 0.0, 0.0}, r[3] = {0.0, 0.0, 0.0};
+  int lo[3] = {0, 0, 0};
   if (active) {
-    double x[3] = {a.node_x[3 * nd], a.node_x[3 * nd + 1], a.node_x[3 * nd + 2]};
-    stencil_origin(a, x, r, lo);
-    double v[3] = {0.0, 0.0, 0.0};
-    for (int ii = lo[0]; ii <= lo[0] + 1; ii++)
-      for (int jj = lo[1]; jj <= lo[1] + 1; jj++)
-        for (int kk = lo[2]; kk <= lo[2] + 1; kk++) {
-          const long long cell = (long long)ii + (long long)jj * xc + (long long)kk * yc * xc;
-          if (cell < a.C && cell >= 0) {
-            const double wx = 1 - fabs(ii + 0.5 - r[0]);
-            const double wy = 1 - fabs(jj + 0.5 - r[1]);
-            const double wz = 1 - fabs(kk + 0.5 - r[2]);
-            const d4 q = ld4(a.state, a.ibm_map[cell]);
-            v[0] += q.x * wx * wy * wz * a.ibm_inv_dx3;
-            v[1] += q.y * wx * wy * wz * a.ibm_inv_dx3;
-            v[2] += q.z * wx * wy * wz * a.ibm_inv_dx3;
-          }
-        }
-    for (int c = 0; c < 3; c++) {
-      x[c] = a.node_x0[3 * nd + c] + v[c] * a.dt;
-      a.node_x[3 * nd + c] = x[c];
-      a.node_x0[3 * nd + c] = x[c];
-      a.node_vel[3 * nd + c] = v[c];
-    }
-    fx = (-a.ibm_area_k * (x[0] - a.node_ref[3 * nd]));
-    fy = (-a.ibm_area_k * (x[1] - a.node_ref[3 * nd + 1]));
-    fz = (-a.ibm_area_k * (x[2] - a.node_ref[3 * nd + 2]));
-    a.node_force[3 * nd] = fx;
-    a.node_force[3 * nd + 1] = fy;
-    a.node_force[3 * nd + 2] = fz;
+#pragma unroll
+    for (int c = 0; c < 3; c++) x[c] = a.node_x[3 * nd + c];
     stencil_origin(a, x, r, lo);
   }
-  // Spreading: for each of the 8 stencil slots the lanes whose targets
-  // coincide are grouped with __match_any_sync and their contributions are
-  // summed in-warp, so one atomic per distinct cell per slot reaches memory.
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-#pragma unroll 1
-  for (int s = 0; s < 8; s++) {
-    const int ii = active ? lo[0] + (s & 1) : 0;
-    const int jj = active ? lo[1] + ((s >> 1) & 1) : 0;
-    const int kk = active ? lo[2] + (s >> 2) : 0;
-    long long cell = (long long)ii + (long long)jj * xc + (long long)kk * yc * xc;
-    const bool hit = active && cell < a.C && cell >= 0;
-    double vx = 0.0, vy = 0.0, vz = 0.0;
-    if (hit) {
+  const int di = sub & 1, dj = (sub >> 1) & 1, dk = sub >> 2;
+  double v[3] = {0.0, 0.0, 0.0};
+  {
+    const int ii = lo[0] + di, jj = lo[1] + dj, kk = lo[2] + dk;
+    const long long cell = (long long)ii + (long long)jj * xc + (long long)kk * yc * xc;
+    if (active && cell < a.C && cell >= 0) {  // the reference's linear-index check
       const double wx = 1 - fabs(ii + 0.5 - r[0]);
       const double wy = 1 - fabs(jj + 0.5 - r[1]);
       const double wz = 1 - fabs(kk + 0.5 - r[2]);
-      vx = fx * wx * wy * wz * a.ibm_inv_dx3;
-      vy = fy * wx * wy * wz * a.ibm_inv_dx3;
-      vz = fz * wx * wy * wz * a.ibm_inv_dx3;
+      const d4 q = ld4(a.state, a.ibm_map[cell]);
+      v[0] = q.x * wx * wy * wz * a.ibm_inv_dx3;
+      v[1] = q.y * wx * wy * wz * a.ibm_inv_dx3;
+      v[2] = q.z * wx * wy * wz * a.ibm_inv_dx3;
     }
-    const long long key = hit ? cell : -1;
-    const unsigned peers = __match_any_sync(full, key);
-    const int leader = __ffs(peers) - 1;
-    double sx = 0.0, sy = 0.0, sz = 0.0;
-    // group sum by shuffles: each lane adds its peers' values in lane order
-    for (int src = 0; src < 32; src++) {
-      const double ox = __shfl_sync(full, vx, src);
-      const double oy = __shfl_sync(full, vy, src);
-      const double oz = __shfl_sync(full, vz, src);
-      if ((peers >> src) & 1u) {
-        sx += ox;
-        sy += oy;
-        sz += oz;
-      }
+  }
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1)
+#pragma unroll
+    for (int c = 0; c < 3; c++) v[c] += __shfl_xor_sync(full, v[c], o);
+  if (!active) return;
+  double fn[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    x[c] = a.node_x0[3 * nd + c] + v[c] * a.dt;
+    fn[c] = -a.ibm_area_k * (x[c] - a.node_ref[3 * nd + c]);
+  }
+  if (sub == 0) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      a.node_x[3 * nd + c] = x[c];
+      a.node_x0[3 * nd + c] = x[c];
+      a.node_vel[3 * nd + c] = v[c];
+      a.node_force[3 * nd + c] = fn[c];
     }
-    if (hit && lane == leader) {
-      const int c = a.ibm_map[cell];
-      atomicAdd(a.force_x + c, sx);
-      atomicAdd(a.force_y + c, sy);
-      atomicAdd(a.force_z + c, sz);
-    }
+  }
+  stencil_origin(a, x, r, lo);
+  const int ii = lo[0] + di, jj = lo[1] + dj, kk = lo[2] + dk;
+  const long long cell = (long long)ii + (long long)jj * xc + (long long)kk * yc * xc;
+  if (cell < a.C && cell >= 0) {
+    const double wx = 1 - fabs(ii + 0.5 - r[0]);
+    const double wy = 1 - fabs(jj + 0.5 - r[1]);
+    const double wz = 1 - fabs(kk + 0.5 - r[2]);
+    const int c = a.ibm_map[cell];
+    atomicAdd(a.force_x + c, fn[0] * wx * wy * wz * a.ibm_inv_dx3);
+    atomicAdd(a.force_y + c, fn[1] * wx * wy * wz * a.ibm_inv_dx3);
+    atomicAdd(a.force_z + c, fn[2] * wx * wy * wz * a.ibm_inv_dx3);
   }
 }
 
@@ -717,7 +700,7 @@ void launch_seed(const KernelArgs& a, int precision, cudaStream_t s) {
 }
 void launch_ibm(const KernelArgs& a, int precision, cudaStream_t s) {
   if (precision == PLFBS_FP32_DEVIATION) return launch_ibm32(a, s);
-  if (a.N > 0) k_ibm<<<blocks_for(a.N, 128), 128, 0, s>>>(a);
+  if (a.N > 0) k_ibm<<<blocks_for(8LL * a.N, kIbmBlock), kIbmBlock, 0, s>>>(a);
 }
 
 }  // namespace plfbs

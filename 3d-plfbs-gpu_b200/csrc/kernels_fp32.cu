@@ -67,37 +67,52 @@ __device__ __forceinline__ f4 ghost_state32(const f4& q, const f4& tgt, int type
 }
 
 // Gradient layout: 3 x float4 per cell: (rx ry rz ux)(uy uz vx vy)(vz wx wy wz).
+// Stencil slots as in k_gradient: neighbour ids first, then the slots.
+__device__ __forceinline__ void gradient_slot32(const KernelArgs& a, long long s, int j,
+                                                const f4& qi, float g[12]) {
+  f4 qj;
+  if (j < a.C) {
+    qj = ldf(a.state, j);
+  } else {
+    const int b = j - a.C;
+    const f4 tgt = ldf(a.bc1, b);
+    const int types = (int)__ldg(reinterpret_cast<const float*>(a.bc3) + 4LL * b + 3);
+    qj = ghost_state32(qi, tgt, types);
+    stf(a.state, j, qj);
+  }
+  const float w[3] = {__ldg(static_cast<const float*>(a.st_wx) + s),
+                      __ldg(static_cast<const float*>(a.st_wy) + s),
+                      __ldg(static_cast<const float*>(a.st_wz) + s)};
+  const float d[4] = {qj.w - qi.w, qj.x - qi.x, qj.y - qi.y, qj.z - qi.z};
+#pragma unroll
+  for (int f = 0; f < 4; f++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) g[3 * f + c] = fmaf(w[c], d[f], g[3 * f + c]);
+}
+
 __global__ void __launch_bounds__(kBlock) k_gradient32(const KernelArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (halted(a)) return;
   if (i >= a.C) return;
   const f4 qi = ldf(a.state, i);
-  const float* wx = static_cast<const float*>(a.st_wx);
-  const float* wy = static_cast<const float*>(a.st_wy);
-  const float* wz = static_cast<const float*>(a.st_wz);
   float g[12];
 #pragma unroll
   for (int k = 0; k < 12; k++) g[k] = 0.0f;
-  for (int k = 0; k < a.K; k++) {
-    const long long s = (long long)k * a.C + i;
-    const int j = __ldg(a.st_nbr + s);
-    if (j < 0) break;
-    f4 qj;
-    if (j < a.C) {
-      qj = ldf(a.state, j);
-    } else {
-      const int b = j - a.C;
-      const f4 tgt = ldf(a.bc1, b);
-      const int types = (int)__ldg(reinterpret_cast<const float*>(a.bc3) + 4LL * b + 3);
-      qj = ghost_state32(qi, tgt, types);
-      stf(a.state, j, qj);
+  constexpr int kUnroll = 8;
+  if (a.K <= kUnroll) {
+    int jj[kUnroll];
+#pragma unroll
+    for (int k = 0; k < kUnroll; k++) jj[k] = k < a.K ? __ldg(a.st_nbr + (long long)k * a.C + i) : -1;
+#pragma unroll
+    for (int k = 0; k < kUnroll; k++)
+      if (jj[k] >= 0) gradient_slot32(a, (long long)k * a.C + i, jj[k], qi, g);
+  } else {
+    for (int k = 0; k < a.K; k++) {
+      const long long s = (long long)k * a.C + i;
+      const int j = __ldg(a.st_nbr + s);
+      if (j < 0) break;
+      gradient_slot32(a, s, j, qi, g);
     }
-    const float w[3] = {__ldg(wx + s), __ldg(wy + s), __ldg(wz + s)};
-    const float d[4] = {qj.w - qi.w, qj.x - qi.x, qj.y - qi.y, qj.z - qi.z};
-#pragma unroll
-    for (int f = 0; f < 4; f++)
-#pragma unroll
-      for (int c = 0; c < 3; c++) g[3 * f + c] = fmaf(w[c], d[f], g[3 * f + c]);
   }
   stf(a.grad, 3LL * i + 0, f4{g[0], g[1], g[2], g[3]});
   stf(a.grad, 3LL * i + 1, f4{g[4], g[5], g[6], g[7]});
@@ -502,91 +517,75 @@ __global__ void k_seed32(const KernelArgs a) {
 // IBM with FP64 node positions and forces; velocities interpolated from the
 // FP32 state (times U) and forces spread as force / U in FP32, with the
 // warp-aggregated atomics of the FP64 kernel.
-__global__ void __launch_bounds__(128) k_ibm32(const KernelArgs a) {
-  const int nd = blockIdx.x * blockDim.x + threadIdx.x;
+// Eight threads per node (as k_ibm). Node quantities stay FP64; the state is
+// scaled by U when read and the spread force divided by U when written.
+__global__ void __launch_bounds__(kIbmBlock) k_ibm32(const KernelArgs a) {
   if (halted(a)) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nd = t >> 3, sub = t & 7;
   const bool active = nd < a.N;
   const int xc = a.ibm_xc, yc = a.ibm_yc;
   const double U = a.uref;
-  double fx = 0.0, fy = 0.0, fz = 0.0;
-  double r[3];
+  double x[3] = {0.0, 0.0, 0.0}, r[3] = {0.0, 0.0, 0.0};
   int lo[3] = {0, 0, 0};
-  auto origin = [&](const double x[3]) {
-    r[0] = (x[0] - a.origin[0]) / a.ibm_dx;
-    r[1] = fabs((x[1] - a.origin[1]) / a.ibm_dx);
-    r[2] = fabs((x[2] - a.origin[2]) / a.ibm_dx);
+  auto origin = [&](const double p[3]) {
+    r[0] = (p[0] - a.origin[0]) / a.ibm_dx;
+    r[1] = fabs((p[1] - a.origin[1]) / a.ibm_dx);
+    r[2] = fabs((p[2] - a.origin[2]) / a.ibm_dx);
 #pragma unroll
     for (int c = 0; c < 3; c++) lo[c] = (int)round(r[c]) - 1;
   };
   if (active) {
-    double x[3] = {a.node_x[3 * nd], a.node_x[3 * nd + 1], a.node_x[3 * nd + 2]};
+#pragma unroll
+    for (int c = 0; c < 3; c++) x[c] = a.node_x[3 * nd + c];
     origin(x);
-    double v[3] = {0.0, 0.0, 0.0};
-    for (int ii = lo[0]; ii <= lo[0] + 1; ii++)
-      for (int jj = lo[1]; jj <= lo[1] + 1; jj++)
-        for (int kk = lo[2]; kk <= lo[2] + 1; kk++) {
-          const long long cell = (long long)ii + (long long)jj * xc + (long long)kk * yc * xc;
-          if (cell < a.C && cell >= 0) {
-            const double wx = 1 - fabs(ii + 0.5 - r[0]);
-            const double wy = 1 - fabs(jj + 0.5 - r[1]);
-            const double wz = 1 - fabs(kk + 0.5 - r[2]);
-            const f4 q = ldf(a.state, a.ibm_map[cell]);
-            v[0] += (U * q.x) * wx * wy * wz * a.ibm_inv_dx3;
-            v[1] += (U * q.y) * wx * wy * wz * a.ibm_inv_dx3;
-            v[2] += (U * q.z) * wx * wy * wz * a.ibm_inv_dx3;
-          }
-        }
+  }
+  const int di = sub & 1, dj = (sub >> 1) & 1, dk = sub >> 2;
+  double v[3] = {0.0, 0.0, 0.0};
+  {
+    const int ii = lo[0] + di, jj = lo[1] + dj, kk = lo[2] + dk;
+    const long long cell = (long long)ii + (long long)jj * xc + (long long)kk * yc * xc;
+    if (active && cell < a.C && cell >= 0) {
+      const double wx = 1 - fabs(ii + 0.5 - r[0]);
+      const double wy = 1 - fabs(jj + 0.5 - r[1]);
+      const double wz = 1 - fabs(kk + 0.5 - r[2]);
+      const f4 q = ldf(a.state, a.ibm_map[cell]);
+      v[0] = (U * q.x) * wx * wy * wz * a.ibm_inv_dx3;
+      v[1] = (U * q.y) * wx * wy * wz * a.ibm_inv_dx3;
+      v[2] = (U * q.z) * wx * wy * wz * a.ibm_inv_dx3;
+    }
+  }
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1)
+#pragma unroll
+    for (int c = 0; c < 3; c++) v[c] += __shfl_xor_sync(full, v[c], o);
+  if (!active) return;
+  double fn[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    x[c] = a.node_x0[3 * nd + c] + v[c] * a.dt;
+    fn[c] = -a.ibm_area_k * (x[c] - a.node_ref[3 * nd + c]);
+  }
+  if (sub == 0) {
+#pragma unroll
     for (int c = 0; c < 3; c++) {
-      x[c] = a.node_x0[3 * nd + c] + v[c] * a.dt;
       a.node_x[3 * nd + c] = x[c];
       a.node_x0[3 * nd + c] = x[c];
       a.node_vel[3 * nd + c] = v[c];
+      a.node_force[3 * nd + c] = fn[c];
     }
-    fx = (-a.ibm_area_k * (x[0] - a.node_ref[3 * nd]));
-    fy = (-a.ibm_area_k * (x[1] - a.node_ref[3 * nd + 1]));
-    fz = (-a.ibm_area_k * (x[2] - a.node_ref[3 * nd + 2]));
-    a.node_force[3 * nd] = fx;
-    a.node_force[3 * nd + 1] = fy;
-    a.node_force[3 * nd + 2] = fz;
-    origin(x);
   }
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-#pragma unroll 1
-  for (int s = 0; s < 8; s++) {
-    const int ii = active ? lo[0] + (s & 1) : 0;
-    const int jj = active ? lo[1] + ((s >> 1) & 1) : 0;
-    const int kk = active ? lo[2] + (s >> 2) : 0;
-    const long long cell = (long long)ii + (long long)jj * xc + (long long)kk * yc * xc;
-    const bool hit = active && cell < a.C && cell >= 0;
-    float vx = 0.0f, vy = 0.0f, vz = 0.0f;
-    if (hit) {
-      const double wgt = (1 - fabs(ii + 0.5 - r[0])) * (1 - fabs(jj + 0.5 - r[1])) *
-                         (1 - fabs(kk + 0.5 - r[2])) * a.ibm_inv_dx3 / U;
-      vx = (float)(fx * wgt);
-      vy = (float)(fy * wgt);
-      vz = (float)(fz * wgt);
-    }
-    const long long key = hit ? cell : -1;
-    const unsigned peers = __match_any_sync(full, key);
-    const int leader = __ffs(peers) - 1;
-    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-    for (int src = 0; src < 32; src++) {
-      const float ox = __shfl_sync(full, vx, src);
-      const float oy = __shfl_sync(full, vy, src);
-      const float oz = __shfl_sync(full, vz, src);
-      if ((peers >> src) & 1u) {
-        sx += ox;
-        sy += oy;
-        sz += oz;
-      }
-    }
-    if (hit && lane == leader) {
-      const int c = a.ibm_map[cell];
-      atomicAdd(a.fforce_x + c, sx);
-      atomicAdd(a.fforce_y + c, sy);
-      atomicAdd(a.fforce_z + c, sz);
-    }
+  origin(x);
+  const int ii = lo[0] + di, jj = lo[1] + dj, kk = lo[2] + dk;
+  const long long cell = (long long)ii + (long long)jj * xc + (long long)kk * yc * xc;
+  if (cell < a.C && cell >= 0) {
+    const double wgt = (1 - fabs(ii + 0.5 - r[0])) * (1 - fabs(jj + 0.5 - r[1])) *
+                       (1 - fabs(kk + 0.5 - r[2])) * a.ibm_inv_dx3 / U;
+    const int c = a.ibm_map[cell];
+    atomicAdd(a.fforce_x + c, (float)(fn[0] * wgt));
+    atomicAdd(a.fforce_y + c, (float)(fn[1] * wgt));
+    atomicAdd(a.fforce_z + c, (float)(fn[2] * wgt));
   }
 }
 
@@ -629,7 +628,7 @@ void launch_seed32(const KernelArgs& a, cudaStream_t s) {
   k_seed32<<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
 }
 void launch_ibm32(const KernelArgs& a, cudaStream_t s) {
-  if (a.N > 0) k_ibm32<<<blocks_for(a.N, 128), 128, 0, s>>>(a);
+  if (a.N > 0) k_ibm32<<<blocks_for(8LL * a.N, kIbmBlock), kIbmBlock, 0, s>>>(a);
 }
 
 }  // namespace plfbs

@@ -93,6 +93,7 @@ constexpr int kHistoryCap = 4096;   // per-step residual records kept on the dev
 constexpr int kBlock = 256;         // threads per block of the cell kernels
 constexpr int kFluxBlock = 128;     // threads per block of the face-flux kernel (128 registers, 4 blocks/SM)
 constexpr int kFinishBlock = 1024;  // the one block that reduces the per-block residual sums
+constexpr int kIbmBlock = 256;      // IBM kernel: 32 nodes x 8 stencil cells per block
 constexpr int kMaxDevices = 64;     // per-device caches of launch shapes
 
 // Run status shared by all kernels of a step, in device memory. The halt flag
