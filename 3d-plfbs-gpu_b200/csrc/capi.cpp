@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -56,22 +57,55 @@ int set_err(plfbs_ctx* c, int code, const std::string& m) {
       return set_err(ctx, PLFBS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+// Device memory comes from one stream-ordered pool per device whose release
+// threshold is unbounded: plfbs_destroy returns a context's arrays to the pool
+// (no unmapping, which cost up to 0.8 s in a process's first frees) and the
+// next plfbs_create on that device reuses them. plfbs_release_cached trims it.
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pools[plfbs::kMaxDevices] = {};
+
+cudaMemPool_t device_pool(int device) {
+  std::lock_guard<std::mutex> g(g_pool_mutex);
+  if (device < 0 || device >= plfbs::kMaxDevices) return nullptr;
+  if (!g_pools[device]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&g_pools[device], &props) != cudaSuccess) return g_pools[device] = nullptr;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(g_pools[device], cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  return g_pools[device];
+}
+
+int pool_alloc(plfbs_ctx* ctx, void** dst, size_t n) {
+  cudaMemPool_t pool = device_pool(ctx->device);
+  if (!pool) return set_err(ctx, PLFBS_ERR_CUDA, "device memory pool creation failed");
+  CK(cudaMallocFromPoolAsync(dst, n, pool, ctx->stream));
+  ctx->allocs.push_back(*dst);
+  ctx->bytes += (int64_t)n;
+  return PLFBS_OK;
+}
+
+// Pageable-source copies: cudaMemcpyAsync returns once `src` has been staged,
+// so the caller may release it afterwards.
 template <typename T>
 int dev_upload(plfbs_ctx* ctx, void** dst, const std::vector<T>& src) {
   const size_t n = std::max<size_t>(src.size(), 1) * sizeof(T);
-  CK(cudaMalloc(dst, n));
-  ctx->allocs.push_back(*dst);
-  ctx->bytes += (int64_t)n;
-  if (!src.empty()) CK(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  int rc = pool_alloc(ctx, dst, n);
+  if (rc) return rc;
+  if (!src.empty())
+    CK(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice,
+                       ctx->stream));
   return PLFBS_OK;
 }
 
 int dev_alloc(plfbs_ctx* ctx, void** dst, size_t n) {
   n = std::max<size_t>(n, 16);
-  CK(cudaMalloc(dst, n));
-  ctx->allocs.push_back(*dst);
-  ctx->bytes += (int64_t)n;
-  CK(cudaMemset(*dst, 0, n));
+  int rc = pool_alloc(ctx, dst, n);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(*dst, 0, n, ctx->stream));
   return PLFBS_OK;
 }
 
@@ -399,12 +433,28 @@ void plfbs_destroy(plfbs_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
-  for (void* p : ctx->allocs) cudaFree(p);
+  for (void* p : ctx->allocs) cudaFreeAsync(p, ctx->stream);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->stats_host) cudaFreeHost(ctx->stats_host);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
+}
+
+int plfbs_release_cached(int32_t device) {
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> g(g_pool_mutex);
+    if (device < 0 || device >= plfbs::kMaxDevices)
+      return set_err(nullptr, PLFBS_ERR_ARG, "device index out of range");
+    pool = g_pools[device];
+  }
+  if (!pool) return PLFBS_OK;
+  cudaError_t e = cudaMemPoolTrimTo(pool, 0);
+  if (e != cudaSuccess)
+    return set_err(nullptr, PLFBS_ERR_CUDA, std::string("cudaMemPoolTrimTo: ") + cudaGetErrorString(e));
+  return PLFBS_OK;
 }
 
 int plfbs_set_state(plfbs_ctx* ctx, const double* rho, const double* u, const double* v,

@@ -28,7 +28,7 @@ EXPORTS = ("plfbs_create", "plfbs_set_state", "plfbs_run", "plfbs_get_state",
            "plfbs_get_gradients", "plfbs_get_face_flux", "plfbs_get_residual",
            "plfbs_ls_weights", "plfbs_profile_steps", "plfbs_memory_bytes",
            "plfbs_last_error", "plfbs_destroy", "plfbs_version",
-           "plfbs_residual_norms_noalloc")
+           "plfbs_residual_norms_noalloc", "plfbs_release_cached")
 
 
 class MeshView(C.Structure):
@@ -93,6 +93,8 @@ def lib():
         L.plfbs_memory_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
         L.plfbs_last_error.argtypes = [C.c_void_p]
         L.plfbs_destroy.argtypes = [C.c_void_p]
+        L.plfbs_release_cached.argtypes = [C.c_int32]
+        L.plfbs_release_cached.restype = C.c_int
         L.plfbs_residual_norms_noalloc.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_double,
                                                    C.c_void_p, C.c_void_p]
         _lib = L

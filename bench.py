@@ -388,6 +388,7 @@ def main():
                   "flux": prof["flux"] / (4 * args.profile_steps),
                   "update": prof["update"] / (4 * args.profile_steps)}
     total = sum(prof.values())
+    workload = WORKLOAD if args.precision == "fp64" else WORKLOAD.replace("fp64", "fp32dev")
     alg = algorithmic_bytes(ma.n_cells, ma.n_faces, ma.n_bc, fp32=args.precision == "fp32")
     peak, peak_kind = load_peaks()
     kern = {}
@@ -399,7 +400,7 @@ def main():
     dom = max(("gradient", "flux", "update"), key=lambda k: prof[k])
     roof = {"kernel": dom, "bound": "hbm", "achieved": kern[dom]["achieved_gbs"], "peak": peak,
             "unit": "GB/s", "frac": kern[dom]["frac"], "peak_kind": peak_kind,
-            "traffic": load_traffic(dom, WORKLOAD)}
+            "traffic": load_traffic(dom, workload)}
 
     # end to end through the C ABI from host buffers
     e2e = None
@@ -409,11 +410,18 @@ def main():
         t0 = time.perf_counter()
         s2 = capi.Solver(ma, rt, vt, val, solver_cfg(c, prec), ibm=ibm_cfg(nodes),
                          device=local_rank)
+        t1 = time.perf_counter()
         s2.set_state(state0)
+        t2 = time.perf_counter()
         st2, hist2 = s2.run(args.steps, history=True)
+        t3 = time.perf_counter()
         out = s2.get_state()
+        t4 = time.perf_counter()
         s2.close()
-        wall = max_over_ranks(time.perf_counter() - t0)
+        t5 = time.perf_counter()
+        wall = max_over_ranks(t5 - t0)
+        phases = {"create_s": t1 - t0, "set_state_s": t2 - t1, "run_s": t3 - t2,
+                  "get_state_s": t4 - t3, "destroy_s": t5 - t4}
         T = ma.total_cells
         mesh_bytes = (ma.n_faces * (4 + 4 + 8 + 24 + 24 + 8) + T * (8 + 24) +
                       (ma.n_cells + 1 + 2 * len(ma.stencil_cells)) * 4 + ma.n_bc * (4 + 4 + 32) +
@@ -423,7 +431,8 @@ def main():
         e2e = {"value": replica_throughput(world, ma.n_cells, args.steps, wall * 1e3),
                "unit": METRIC,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "wall_s": wall, "includes": "create+set_state+run+history+get_state+destroy"}
+               "wall_s": wall, "includes": "create+set_state+run+history+get_state+destroy",
+               "phases": phases}
         assert np.isfinite(out).all() and st2["steps_run"] == args.steps
     else:
         solver.close()
@@ -440,8 +449,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD if args.precision == "fp64"
-                           else WORKLOAD.replace("fp64", "fp32dev"), "cells": ma.n_cells, "faces": ma.n_faces,
+                "config": {"workload": workload, "cells": ma.n_cells, "faces": ma.n_faces,
                            "nodes": NNODES, "re": RE, "dt": DT,
                            "parallelism": "replicas" if world > 1 else "single",
                            "l2": "working set > L2 (no flush)"},

@@ -211,7 +211,18 @@ int plfbs_residual_norms_noalloc(const double* residual, int64_t n_cells, double
                                  double max_velocity, double* out, void* stream);
 
 const char* plfbs_last_error(const plfbs_ctx* ctx);  /* ctx may be NULL: global error */
+
+/* Frees the context (replaces the end of General_Purpose_Solver_mk_i; the
+ * reference never frees its managed buffers). Its device arrays return to a
+ * per-device memory pool of this library, which keeps them for the next
+ * plfbs_create on that device instead of unmapping them. */
 void plfbs_destroy(plfbs_ctx* ctx);
+
+/* Returns the memory cached in this library's pool for `device` to the driver
+ * (contexts still alive keep theirs). No counterpart in the reference.
+ * Errors are reported through plfbs_last_error(NULL). */
+int plfbs_release_cached(int32_t device);
+
 const char* plfbs_version(void);
 
 #ifdef __cplusplus

@@ -109,6 +109,13 @@ def _tets(n=4, seed=3):
     return cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min), c
 
 
+def test_release_cached_checks_device_index(plfbs_lib):
+    L = capi.lib()
+    assert L.plfbs_release_cached(-1) == capi.ERR_ARG
+    assert b"device index" in L.plfbs_last_error(None)
+    assert L.plfbs_release_cached(63) == 0  # no pool was made for it: nothing to do
+
+
 def test_tet_mesh_is_valid():
     """Jittered hexes split into 6 tets: conforming, positive, closed cells."""
     ma, c = _tets()

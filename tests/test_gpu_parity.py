@@ -89,6 +89,26 @@ def test_stage_path_equals_graph_path(plfbs_lib):
     np.testing.assert_array_equal(a.get_state(), b.get_state())
 
 
+def test_pooled_memory_reused_and_released(plfbs_lib):
+    """Contexts created after a destroy (pool reuse) and after
+    plfbs_release_cached (fresh memory) compute the same bits."""
+    d = golden_cases.build("graded")
+    out = []
+    for release in (False, False, True):
+        s = _solver(d, renumber=1)
+        s.set_state(d["state0"])
+        s.run(2)
+        out.append(s.get_state())
+        s.close()
+        if release:
+            assert capi.lib().plfbs_release_cached(0) == 0
+    np.testing.assert_array_equal(out[0], out[1])
+    s = _solver(d, renumber=1)
+    s.set_state(d["state0"])
+    s.run(2)
+    np.testing.assert_array_equal(out[0], s.get_state())
+
+
 def _cavity32(n=32):
     pm = cases.uniform_box(n, n, n, patch_types=["wall", "wall", "wall", "lid", "wall", "wall"])
     c = cases.Case(mesh_dir="", X=n, Y=n, Z=n, steps=10, dt=0.18, mach=0.1, reynolds=100,
