@@ -288,7 +288,8 @@ def run_reference_arm(args, rank, world):
     pm, c, ma, nodes, _ = build_case()
     value, sample = reference_cpu_throughput(pm, c, nodes, sample_steps=1)
     cfg = {"workload": WORKLOAD, "cells": ma.n_cells, "faces": ma.n_faces,
-           "nodes": NNODES, "parallelism": "replicas"}
+           "nodes": NNODES, "re": RE, "dt": DT,
+           "parallelism": "replicas" if world > 1 else "single"}
     if value is None:
         print(json.dumps({"impl": "reference", "unavailable": sample}))
         return 0
