@@ -33,6 +33,7 @@ struct plfbs_ctx {
   long long stages_done = 0;       // stages run through plfbs_run_stages in the current step
   bool debug = false;
   bool have_state = false;
+  uint64_t fingerprint = 0;  // of the caller's mesh, checked when a checkpoint is loaded
   std::string err;
 };
 
@@ -195,6 +196,22 @@ int download4(plfbs_ctx* ctx, const void* src, size_t n, std::vector<double>& ou
   return PLFBS_OK;
 }
 
+// FNV-1a over the mesh arrays that fix the internal numbering and geometry.
+uint64_t mesh_fingerprint(const plfbs_mesh_view& m) {
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&h](const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; i++) h = (h ^ b[i]) * 1099511628211ull;
+  };
+  const int32_t sizes[3] = {m.n_cells, m.n_faces, m.n_internal};
+  mix(sizes, sizeof sizes);
+  mix(m.owner, sizeof(int32_t) * (size_t)m.n_faces);
+  mix(m.neighbour, sizeof(int32_t) * (size_t)m.n_faces);
+  mix(m.face_area, sizeof(double) * (size_t)m.n_faces);
+  mix(m.cell_volume, sizeof(double) * (size_t)m.n_cells);
+  return h;
+}
+
 int check_ctx(plfbs_ctx* ctx) {
   if (!ctx) return set_err(nullptr, PLFBS_ERR_ARG, "null context");
   cudaError_t e = cudaSetDevice(ctx->device);
@@ -244,6 +261,7 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     delete ctx;
     return set_err(nullptr, rc, err);
   }
+  ctx->fingerprint = mesh_fingerprint(*mesh);  // arrays validated by build_layout
   const Layout& L = ctx->L;
   const bool fp32 = cfg->precision == PLFBS_FP32_DEVIATION;
   if (fp32 && L.K2 > 16) {
@@ -457,13 +475,14 @@ int plfbs_release_cached(int32_t device) {
   return PLFBS_OK;
 }
 
-int plfbs_set_state(plfbs_ctx* ctx, const double* rho, const double* u, const double* v,
-                    const double* w, int64_t n_total) {
-  TRY(check_ctx(ctx));
+namespace {
+
+// Uploads a state given in the caller's numbering (FP32 form: converted to
+// deviation units), resets the run status and seeds the RK accumulators.
+int seed_state(plfbs_ctx* ctx, const double* rho, const double* u, const double* v,
+               const double* w, bool conserved) {
   const Layout& L = ctx->L;
   const int64_t T = (int64_t)L.C + L.B;
-  if (!rho || !u || !v || !w || n_total != T)
-    return set_err(ctx, PLFBS_ERR_ARG, "set_state needs 4 arrays of n_cells + n_boundary values");
   if (ctx->cfg.precision == PLFBS_FP32_DEVIATION) {
     // deviation units: velocity / U, rho - rho0
     const double U = ctx->cfg.max_velocity, r0 = ctx->cfg.ref_rho;
@@ -492,8 +511,190 @@ int plfbs_set_state(plfbs_ctx* ctx, const double* rho, const double* u, const do
     CK(cudaStreamSynchronize(ctx->stream));
   }
   CK(cudaMemsetAsync(ctx->args.stats, 0, sizeof(DevStats), ctx->stream));
-  plfbs::launch_seed(ctx->args, ctx->cfg.precision, ctx->stream);
+  plfbs::launch_seed(ctx->args, ctx->cfg.precision, conserved, ctx->stream);
   CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(reset_force(ctx));
+  ctx->stages_done = 0;
+  ctx->have_state = true;
+  return PLFBS_OK;
+}
+
+}  // namespace
+
+int plfbs_set_state(plfbs_ctx* ctx, const double* rho, const double* u, const double* v,
+                    const double* w, int64_t n_total) {
+  TRY(check_ctx(ctx));
+  const int64_t T = (int64_t)ctx->L.C + ctx->L.B;
+  if (!rho || !u || !v || !w || n_total != T)
+    return set_err(ctx, PLFBS_ERR_ARG, "set_state needs 4 arrays of n_cells + n_boundary values");
+  return seed_state(ctx, rho, u, v, w, false);
+}
+
+int plfbs_warm_start(plfbs_ctx* ctx, const double* rho, const double* u, const double* v,
+                     const double* w, int64_t n_total, const double* node_x, int32_t n_nodes) {
+  TRY(check_ctx(ctx));
+  const int64_t T = (int64_t)ctx->L.C + ctx->L.B;
+  if (!rho || !u || !v || !w || n_total != T)
+    return set_err(ctx, PLFBS_ERR_ARG, "warm_start needs 4 arrays of n_cells + n_boundary values");
+  if (node_x && n_nodes != ctx->N) return set_err(ctx, PLFBS_ERR_ARG, "node count mismatch");
+  if (node_x && ctx->N > 0) {
+    const size_t n = 3 * (size_t)ctx->N * sizeof(double);
+    CK(cudaMemcpyAsync(ctx->args.node_x, node_x, n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->args.node_x0, node_x, n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(ctx->args.node_vel, 0, n, ctx->stream));
+    CK(cudaMemsetAsync(ctx->args.node_force, 0, n, ctx->stream));
+  }
+  return seed_state(ctx, rho, u, v, w, true);
+}
+
+// Checkpoint image: header, then in the caller's numbering the state
+// [n_cells + n_boundary][4] and the RK accumulator [n_cells][4] as the
+// context stores them (FP64, or FP32 deviation units), then the nodes'
+// positions, velocities and forces [n_nodes][3] (FP64).
+namespace {
+struct CheckpointHeader {
+  char magic[8];
+  int32_t version, precision;
+  int64_t n_cells, n_boundary, n_nodes, n_faces;
+  uint64_t fingerprint;
+  int32_t halt, converged, diverged, pad;
+  int64_t steps, converged_step;
+  double last[6];
+};
+const char kMagic[8] = {'P', 'L', 'F', 'B', 'S', 'C', 'K', '1'};
+
+int64_t checkpoint_size(const plfbs_ctx* ctx) {
+  const int64_t v = ctx->cfg.precision == PLFBS_FP32_DEVIATION ? 4 : 8;
+  const int64_t T = (int64_t)ctx->L.C + ctx->L.B;
+  return (int64_t)sizeof(CheckpointHeader) + 4 * v * (T + ctx->L.C) + 9 * 8 * (int64_t)ctx->N;
+}
+
+// Moves n records of `rec` bytes between the caller's order (host) and the
+// internal order; `to_host` gathers, otherwise scatters.
+void permute_records(const plfbs_ctx* ctx, int64_t n, size_t rec, const char* src, char* dst,
+                     bool to_host) {
+  const Layout& L = ctx->L;
+  for (int64_t o = 0; o < n; o++) {
+    const int64_t k = o < L.C ? L.cell_new_of_old[o] : L.C + L.bc_new_of_old[o - L.C];
+    if (to_host)
+      std::memcpy(dst + o * rec, src + k * rec, rec);
+    else
+      std::memcpy(dst + k * rec, src + o * rec, rec);
+  }
+}
+}  // namespace
+
+int plfbs_checkpoint_bytes(plfbs_ctx* ctx, int64_t* bytes) {
+  if (!ctx) return set_err(nullptr, PLFBS_ERR_ARG, "null context");
+  if (!bytes) return set_err(ctx, PLFBS_ERR_ARG, "null output");
+  *bytes = checkpoint_size(ctx);
+  return PLFBS_OK;
+}
+
+int plfbs_save_checkpoint(plfbs_ctx* ctx, void* buf, int64_t bytes) {
+  TRY(check_ctx(ctx));
+  if (!buf || bytes < checkpoint_size(ctx))
+    return set_err(ctx, PLFBS_ERR_ARG, "checkpoint buffer smaller than plfbs_checkpoint_bytes");
+  if (!ctx->have_state) return set_err(ctx, PLFBS_ERR_STATE, "checkpoint before set_state");
+  if (ctx->stages_done != 0)
+    return set_err(ctx, PLFBS_ERR_STATE, "checkpoint in the middle of a step (after run_stages)");
+  TRY(read_stats(ctx));
+  const Layout& L = ctx->L;
+  const size_t rec = ctx->cfg.precision == PLFBS_FP32_DEVIATION ? 16 : 32;
+  const int64_t T = (int64_t)L.C + L.B;
+  CheckpointHeader h{};
+  std::memcpy(h.magic, kMagic, sizeof kMagic);
+  h.version = 1;
+  h.precision = ctx->cfg.precision;
+  h.n_cells = L.C;
+  h.n_boundary = L.B;
+  h.n_nodes = ctx->N;
+  h.n_faces = L.F;
+  h.fingerprint = ctx->fingerprint;
+  const DevStats& st = *ctx->stats_host;
+  h.halt = st.halt;
+  h.converged = st.converged;
+  h.diverged = st.diverged;
+  h.steps = st.steps;
+  h.converged_step = st.converged_step;
+  for (int c = 0; c < 6; c++) h.last[c] = st.last[c];
+  char* out = static_cast<char*>(buf);
+  std::memcpy(out, &h, sizeof h);
+  out += sizeof h;
+  std::vector<char> raw(rec * (size_t)T);
+  CK(cudaMemcpyAsync(raw.data(), ctx->args.state, rec * (size_t)T, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  permute_records(ctx, T, rec, raw.data(), out, true);
+  out += rec * (size_t)T;
+  CK(cudaMemcpyAsync(raw.data(), ctx->args.t1, rec * (size_t)L.C, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  permute_records(ctx, L.C, rec, raw.data(), out, true);
+  out += rec * (size_t)L.C;
+  if (ctx->N > 0) {
+    const size_t n = 3 * (size_t)ctx->N * sizeof(double);
+    CK(cudaMemcpyAsync(out, ctx->args.node_x, n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(out + n, ctx->args.node_vel, n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(out + 2 * n, ctx->args.node_force, n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  return PLFBS_OK;
+}
+
+int plfbs_load_checkpoint(plfbs_ctx* ctx, const void* buf, int64_t bytes) {
+  TRY(check_ctx(ctx));
+  if (!buf || bytes < (int64_t)sizeof(CheckpointHeader))
+    return set_err(ctx, PLFBS_ERR_ARG, "checkpoint buffer too small");
+  CheckpointHeader h;
+  std::memcpy(&h, buf, sizeof h);
+  const Layout& L = ctx->L;
+  if (std::memcmp(h.magic, kMagic, sizeof kMagic) != 0 || h.version != 1)
+    return set_err(ctx, PLFBS_ERR_ARG, "not a plfbs checkpoint (magic/version)");
+  if (h.precision != ctx->cfg.precision)
+    return set_err(ctx, PLFBS_ERR_ARG, "checkpoint precision differs from the context's");
+  if (h.n_cells != L.C || h.n_boundary != L.B || h.n_nodes != ctx->N || h.n_faces != L.F ||
+      h.fingerprint != ctx->fingerprint)
+    return set_err(ctx, PLFBS_ERR_MESH, "checkpoint was written for another mesh or node set");
+  if (bytes < checkpoint_size(ctx))
+    return set_err(ctx, PLFBS_ERR_ARG, "checkpoint buffer truncated");
+  const size_t rec = ctx->cfg.precision == PLFBS_FP32_DEVIATION ? 16 : 32;
+  const int64_t T = (int64_t)L.C + L.B;
+  const char* in = static_cast<const char*>(buf) + sizeof h;
+  std::vector<char> raw(rec * (size_t)T);
+  permute_records(ctx, T, rec, in, raw.data(), false);
+  CK(cudaMemcpyAsync(ctx->args.state, raw.data(), rec * (size_t)T, cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  in += rec * (size_t)T;
+  permute_records(ctx, L.C, rec, in, raw.data(), false);
+  // at a step boundary t0 equals t1
+  CK(cudaMemcpyAsync(ctx->args.t1, raw.data(), rec * (size_t)L.C, cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaMemcpyAsync(ctx->args.t0, raw.data(), rec * (size_t)L.C, cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  in += rec * (size_t)L.C;
+  if (ctx->N > 0) {
+    const size_t n = 3 * (size_t)ctx->N * sizeof(double);
+    CK(cudaMemcpyAsync(ctx->args.node_x, in, n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->args.node_x0, in, n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->args.node_vel, in + n, n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->args.node_force, in + 2 * n, n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  DevStats& st = *ctx->stats_host;  // pinned host copy of the status header
+  std::memset(&st, 0, offsetof(DevStats, history));
+  st.halt = h.halt;
+  st.converged = h.converged;
+  st.diverged = h.diverged;
+  st.steps = h.steps;
+  st.converged_step = h.converged_step;
+  for (int c = 0; c < 6; c++) st.last[c] = h.last[c];
+  CK(cudaMemsetAsync(ctx->args.stats, 0, sizeof(DevStats), ctx->stream));
+  CK(cudaMemcpyAsync(ctx->args.stats, &st, offsetof(DevStats, history), cudaMemcpyHostToDevice,
+                     ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   TRY(reset_force(ctx));
   ctx->stages_done = 0;

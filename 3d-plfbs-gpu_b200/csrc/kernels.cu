@@ -568,10 +568,15 @@ __global__ void __launch_bounds__(kFinishBlock) k_finish(const KernelArgs a) {
 }
 
 // Seeds the RK accumulator from the state (Solver_gpu.cu:664): t0 = t1 = q.
+// The reference seeds the velocity state although the stages treat t0/t1 as
+// (rho u, rho v, rho w, rho); with conserved = true (warm starts, no reference
+// counterpart) the accumulators get the conserved variables instead.
+template <bool CONSERVED>
 __global__ void k_seed(const KernelArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.C) return;
-  const d4 q = ld4(a.state, i);
+  d4 q = ld4(a.state, i);
+  if (CONSERVED) q = d4{q.w * q.x, q.w * q.y, q.w * q.z, q.w};
   st4(a.t0, i, q);
   st4(a.t1, i, q);
 }
@@ -694,9 +699,12 @@ void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t s) {
       break;
   }
 }
-void launch_seed(const KernelArgs& a, int precision, cudaStream_t s) {
-  if (precision == PLFBS_FP32_DEVIATION) return launch_seed32(a, s);
-  k_seed<<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
+void launch_seed(const KernelArgs& a, int precision, bool conserved, cudaStream_t s) {
+  if (precision == PLFBS_FP32_DEVIATION) return launch_seed32(a, conserved, s);
+  if (conserved)
+    k_seed<true><<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
+  else
+    k_seed<false><<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
 }
 void launch_ibm(const KernelArgs& a, int precision, cudaStream_t s) {
   if (precision == PLFBS_FP32_DEVIATION) return launch_ibm32(a, s);

@@ -506,17 +506,23 @@ __global__ void __launch_bounds__(kFinishBlock) k_finish32(const KernelArgs a) {
   }
 }
 
+// As k_seed; the conserved accumulators in deviation units are
+// (rho u / U, rho v / U, rho w / U, rho - rho0).
+template <bool CONSERVED>
 __global__ void k_seed32(const KernelArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.C) return;
-  const f4 q = ldf(a.state, i);
+  f4 q = ldf(a.state, i);
+  if (CONSERVED) {
+    const float rho = a.rho0f + q.w;
+    q = f4{rho * q.x, rho * q.y, rho * q.z, q.w};
+  }
   stf(a.t0, i, q);
   stf(a.t1, i, q);
 }
 
 // IBM with FP64 node positions and forces; velocities interpolated from the
-// FP32 state (times U) and forces spread as force / U in FP32, with the
-// warp-aggregated atomics of the FP64 kernel.
+// FP32 state (times U) and forces spread as force / U in FP32.
 // Eight threads per node (as k_ibm). Node quantities stay FP64; the state is
 // scaled by U when read and the spread force divided by U when written.
 __global__ void __launch_bounds__(kIbmBlock) k_ibm32(const KernelArgs a) {
@@ -624,8 +630,11 @@ void launch_update32(const KernelArgs& a, int rk, cudaStream_t s) {
       break;
   }
 }
-void launch_seed32(const KernelArgs& a, cudaStream_t s) {
-  k_seed32<<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
+void launch_seed32(const KernelArgs& a, bool conserved, cudaStream_t s) {
+  if (conserved)
+    k_seed32<true><<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
+  else
+    k_seed32<false><<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
 }
 void launch_ibm32(const KernelArgs& a, cudaStream_t s) {
   if (a.N > 0) k_ibm32<<<blocks_for(8LL * a.N, kIbmBlock), kIbmBlock, 0, s>>>(a);

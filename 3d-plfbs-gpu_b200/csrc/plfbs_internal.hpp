@@ -155,12 +155,12 @@ void launch_ibm(const KernelArgs& a, int precision, cudaStream_t stream);
 void launch_gradient(const KernelArgs& a, int precision, cudaStream_t stream);
 void launch_flux(const KernelArgs& a, int precision, cudaStream_t stream);
 void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t stream);
-void launch_seed(const KernelArgs& a, int precision, cudaStream_t stream);
+void launch_seed(const KernelArgs& a, int precision, bool conserved, cudaStream_t stream);
 void launch_ibm32(const KernelArgs& a, cudaStream_t stream);
 void launch_gradient32(const KernelArgs& a, cudaStream_t stream);
 void launch_flux32(const KernelArgs& a, cudaStream_t stream);
 void launch_update32(const KernelArgs& a, int rk, cudaStream_t stream);
-void launch_seed32(const KernelArgs& a, cudaStream_t stream);
+void launch_seed32(const KernelArgs& a, bool conserved, cudaStream_t stream);
 
 #ifdef __CUDACC__
 // Blocks of a grid-stride kernel: as many as are resident on the device at

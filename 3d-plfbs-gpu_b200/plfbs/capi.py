@@ -28,7 +28,8 @@ EXPORTS = ("plfbs_create", "plfbs_set_state", "plfbs_run", "plfbs_get_state",
            "plfbs_get_gradients", "plfbs_get_face_flux", "plfbs_get_residual",
            "plfbs_ls_weights", "plfbs_profile_steps", "plfbs_memory_bytes",
            "plfbs_last_error", "plfbs_destroy", "plfbs_version",
-           "plfbs_residual_norms_noalloc", "plfbs_release_cached")
+           "plfbs_residual_norms_noalloc", "plfbs_release_cached", "plfbs_warm_start",
+           "plfbs_checkpoint_bytes", "plfbs_save_checkpoint", "plfbs_load_checkpoint")
 
 
 class MeshView(C.Structure):
@@ -94,6 +95,10 @@ def lib():
         L.plfbs_last_error.argtypes = [C.c_void_p]
         L.plfbs_destroy.argtypes = [C.c_void_p]
         L.plfbs_release_cached.argtypes = [C.c_int32]
+        L.plfbs_warm_start.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_int64, _dp, C.c_int32]
+        L.plfbs_checkpoint_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        L.plfbs_save_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+        L.plfbs_load_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
         L.plfbs_release_cached.restype = C.c_int
         L.plfbs_residual_norms_noalloc.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_double,
                                                    C.c_void_p, C.c_void_p]
@@ -267,6 +272,28 @@ class Solver:
         g = np.zeros((self.C, 4))
         self._check(lib().plfbs_get_residual(self.h, _d(g), self.C))
         return g
+
+    def warm_start(self, state, node_x=None):
+        """Start from `state` [T, 4] (u, v, w, rho) with conserved RK seeding and,
+        optionally, IBM node positions [N, 3]."""
+        q = np.ascontiguousarray(state, np.float64).reshape(self.T, 4)
+        cols = [np.ascontiguousarray(q[:, k]) for k in (3, 0, 1, 2)]
+        nx = None
+        if node_x is not None:
+            nx = np.ascontiguousarray(node_x, np.float64).reshape(self.N, 3)
+        self._check(lib().plfbs_warm_start(self.h, *[_d(c) for c in cols], self.T,
+                                           _d(nx) if nx is not None else None, self.N))
+
+    def checkpoint(self):
+        """The context's lossless checkpoint image (bytes)."""
+        n = C.c_int64()
+        self._check(lib().plfbs_checkpoint_bytes(self.h, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        self._check(lib().plfbs_save_checkpoint(self.h, buf, n.value))
+        return buf.raw
+
+    def restore(self, image):
+        self._check(lib().plfbs_load_checkpoint(self.h, image, len(image)))
 
     def nodes(self):
         x, v, f = (np.zeros((self.N, 3)) for _ in range(3))

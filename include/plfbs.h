@@ -145,6 +145,28 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh,
 int plfbs_set_state(plfbs_ctx* ctx, const double* rho, const double* u, const double* v,
                     const double* w, int64_t n_total);
 
+/* Starts a run from a field that is not uniform flow (a previous solution, a
+ * prediction). Like plfbs_set_state, except that the RK accumulators are
+ * seeded with the conserved variables (rho u, rho v, rho w, rho): the
+ * reference seeds them with the velocity state (Solver_gpu.cu:664), which is
+ * exact only where rho = 1 and perturbs a near-converged field by |rho - 1|.
+ * node_x [n_nodes][3] (or NULL to keep the current positions) sets the IBM
+ * node positions. Resets the step count. No counterpart in the reference. */
+int plfbs_warm_start(plfbs_ctx* ctx, const double* rho, const double* u, const double* v,
+                     const double* w, int64_t n_total, const double* node_x, int32_t n_nodes);
+
+/* Lossless checkpoint at a step boundary (replaces the 6-digit text output of
+ * Solution::output, Solution.cpp:221-251, as a restart source): the state,
+ * the RK accumulator, the IBM nodes and the run status, in the caller's
+ * numbering and the context's precision. plfbs_load_checkpoint into a context
+ * created from the same mesh, boundary conditions and precision continues the
+ * run bit for bit (IBM force spreading uses atomics, whose order can vary).
+ * The image is plfbs_checkpoint_bytes long; a mesh fingerprint, the sizes
+ * and the precision are checked on load. No counterpart in the reference. */
+int plfbs_checkpoint_bytes(plfbs_ctx* ctx, int64_t* bytes);
+int plfbs_save_checkpoint(plfbs_ctx* ctx, void* buf, int64_t bytes);
+int plfbs_load_checkpoint(plfbs_ctx* ctx, const void* buf, int64_t bytes);
+
 /* The time loop of Solver_gpu.cu:667-898: up to max_steps steps, stopping after
  * the first step whose max_error < tolerance (Solver_gpu.cu:870). Synchronous.
  * history (optional, may be NULL) receives 6 doubles per completed step:
