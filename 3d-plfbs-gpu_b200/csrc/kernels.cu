@@ -48,6 +48,14 @@ __device__ __forceinline__ void st4(void* base, long long i, const d4& v) {
   p[1] = make_double2(v.z, v.w);
 }
 
+// The same pointer, opaque to the compiler, so that a load through it is not
+// merged with an earlier load of the same address (a deliberate re-read).
+template <typename T>
+__device__ __forceinline__ const T* launder(const T* p) {
+  asm("mov.b64 %0, %0;" : "+l"(p));
+  return p;
+}
+
 // Whether the context has converged or diverged. One thread per block reads
 // the flag; every thread of the block must call this (it synchronises).
 __device__ __forceinline__ bool halted(const KernelArgs& a) {
@@ -191,6 +199,14 @@ __device__ __forceinline__ double gdot(const double* g) {
   return g[2] - g[1];               // (-1, 1, 1)
 }
 
+// Branch of a lattice pair from s = e . n (see lattice_pair), as two bits.
+template <int EX, int EY, int EZ>
+__device__ __forceinline__ unsigned pair_side(const double n[3], double d1) {
+  const double s = (EX ? (EX > 0 ? n[0] : -n[0]) : 0.0) + (EY ? (EY > 0 ? n[1] : -n[1]) : 0.0) +
+                   (EZ ? (EZ > 0 ? n[2] : -n[2]) : 0.0);
+  return s > d1 ? 1u : (s < -d1 ? 2u : 0u);
+}
+
 // One opposite pair (k, k') of D3Q15 lattice nodes, e_k' = -e_k = -e, node k
 // at x_f - e dt_s (populate_lattice_macros, LBFS.cu:330-938). With s = e . n:
 // s > d1 takes node k from the owner side and k' from the neighbour side,
@@ -203,22 +219,21 @@ __device__ __forceinline__ double gdot(const double* g) {
 template <int EX, int EY, int EZ>
 __device__ __forceinline__ void lattice_pair(const double si[4], const double sn[4],
                                              const double sc[4], const double g1[12],
-                                             const double g2[12], const double n[3], double d1,
-                                             double dt, double c45, double c15, double wgt,
-                                             double& rhoI, double m[3], double P[6], double& D) {
+                                             const double g2[12], int side, double dt,
+                                             double c45, double c15, double wgt, double& rhoI,
+                                             double m[3], double P[6], double& D) {
   constexpr bool diag = EX != 0 && EY != 0 && EZ != 0;
-  const double s = (EX ? (EX > 0 ? n[0] : -n[0]) : 0.0) + (EY ? (EY > 0 ? n[1] : -n[1]) : 0.0) +
-                   (EZ ? (EZ > 0 ? n[2] : -n[2]) : 0.0);
-  // Faces are sorted by their branch signature, so these branches are
-  // uniform across almost every warp; each computes only its own values.
+  // side (pair_side): 1 if s > d1, 2 if s < -d1, 0 in the dead band. Faces are
+  // sorted by their branch signature, so these branches are uniform across
+  // almost every warp; each computes only its own values.
   double qa[4], qb[4];
-  if (s > d1) {
+  if (side == 1) {
 #pragma unroll
     for (int f = 0; f < 4; f++) {
       qa[f] = fma(-gdot<EX, EY, EZ>(g1 + 3 * f), dt, si[f]);
       qb[f] = fma(gdot<EX, EY, EZ>(g2 + 3 * f), dt, sn[f]);
     }
-  } else if (s < -d1) {
+  } else if (side == 2) {
 #pragma unroll
     for (int f = 0; f < 4; f++) {
       qa[f] = fma(-gdot<EX, EY, EZ>(g2 + 3 * f), dt, sn[f]);
@@ -243,20 +258,35 @@ __device__ __forceinline__ void lattice_pair(const double si[4], const double sn
   const double fb =
       wgt * qb[0] * fma(-c15, u2b, fma(c45 * eub, eub, fma(3.0, eub, 1.0)));
   const double sum = fa + fb, dif = fa - fb;
-  if (EX) m[0] += EX > 0 ? dif : -dif;
-  if (EY) m[1] += EY > 0 ? dif : -dif;
-  if (EZ) m[2] += EZ > 0 ? dif : -dif;
+  // The axis pairs come first and each is the first to write its m and P
+  // component; (1, 1, 1) is the first diagonal pair: those writes assign.
+  constexpr bool first_diag = EX == 1 && EY == 1 && EZ == 1;
   if (diag) {
-    D += sum;
+    if (EX) m[0] += EX > 0 ? dif : -dif;
+    if (EY) m[1] += EY > 0 ? dif : -dif;
+    if (EZ) m[2] += EZ > 0 ? dif : -dif;
+    const double p3 = (EX * EY > 0) ? sum : -sum, p4 = (EX * EZ > 0) ? sum : -sum,
+                 p5 = (EY * EZ > 0) ? sum : -sum;
+    if (first_diag) {
+      D = sum;
+      P[3] = p3;
+      P[4] = p4;
+      P[5] = p5;
+    } else {
+      D += sum;
+      P[3] += p3;
+      P[4] += p4;
+      P[5] += p5;
+    }
   } else {
     rhoI += sum;
-    if (EX) P[0] += sum;
-    if (EY) P[1] += sum;
-    if (EZ) P[2] += sum;
+    if (EX) m[0] = EX > 0 ? dif : -dif;
+    if (EY) m[1] = EY > 0 ? dif : -dif;
+    if (EZ) m[2] = EZ > 0 ? dif : -dif;
+    if (EX) P[0] = sum;
+    if (EY) P[1] = sum;
+    if (EZ) P[2] = sum;
   }
-  if (EX && EY) P[3] += (EX * EY > 0) ? sum : -sum;
-  if (EX && EZ) P[4] += (EX * EZ > 0) ? sum : -sum;
-  if (EY && EZ) P[5] += (EY * EZ > 0) ? sum : -sum;
 }
 
 // Flux of one face (calc_face_flux, LBFS.cu:1592-1710 and
@@ -278,7 +308,7 @@ __device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, cons
   const d4 f0 = ld4(a.face0, f), f1 = ld4(a.face1, f), f2 = ld4(a.face2, f);
   const int o = ids.x, nb = ids.y;
   const double n[3] = {f0.x, f0.y, f0.z};
-  const double area = f0.w, dt = f1.x, f2w = f2.w;
+  const double dt = f1.x;
   const double t1[3] = {f1.y, f1.z, f1.w}, t2[3] = {f2.x, f2.y, f2.z};
 
   const d4 qo = ld4(a.state, o);
@@ -327,17 +357,24 @@ __device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, cons
     }
   }
 
-  const double pg = a.pg, d1 = 0.001 * dt, c45 = 4.5 * pg, c15 = 1.5 * pg;
+  const double pg = a.pg, c45 = 4.5 * pg, c15 = 1.5 * pg;
   const double w0 = 2.0 / 9.0, w1 = 1.0 / 9.0, w7 = 1.0 / 72.0;
+  // the seven branch decisions up front: n is not needed again until the end
+  unsigned sides;
+  {
+    const double d1 = 0.001 * dt;
+    sides = pair_side<1, 0, 0>(n, d1) | pair_side<0, 1, 0>(n, d1) << 2 |
+            pair_side<0, 0, 1>(n, d1) << 4 | pair_side<1, 1, 1>(n, d1) << 6 |
+            pair_side<1, 1, -1>(n, d1) << 8 | pair_side<1, -1, 1>(n, d1) << 10 |
+            pair_side<-1, 1, 1>(n, d1) << 12;
+  }
   // centre node (k = 0): e = 0
   const double u2c = fma(sc[3], sc[3], fma(sc[2], sc[2], sc[1] * sc[1]));
   double rhoI = w0 * sc[0] * fma(-c15, u2c, 1.0);
-  double m[3] = {0.0, 0.0, 0.0};
-  double P[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  double D = 0.0;
-  lattice_pair<1, 0, 0>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w1, rhoI, m, P, D);
-  lattice_pair<0, 1, 0>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w1, rhoI, m, P, D);
-  lattice_pair<0, 0, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w1, rhoI, m, P, D);
+  double m[3], P[6], D;  // first written by the pairs below (see lattice_pair)
+  lattice_pair<1, 0, 0>(si, sn, sc, g1, g2, sides & 3, dt, c45, c15, w1, rhoI, m, P, D);
+  lattice_pair<0, 1, 0>(si, sn, sc, g1, g2, sides >> 2 & 3, dt, c45, c15, w1, rhoI, m, P, D);
+  lattice_pair<0, 0, 1>(si, sn, sc, g1, g2, sides >> 4 & 3, dt, c45, c15, w1, rhoI, m, P, D);
 #pragma unroll
   for (int k = 0; k < 4; k++) {  // (gx, gy, gz) -> (gx + gy, gx - gy, gz), see gdot
     const double s1 = g1[3 * k] + g1[3 * k + 1], r1 = g1[3 * k] - g1[3 * k + 1];
@@ -347,26 +384,31 @@ __device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, cons
     g2[3 * k] = s2;
     g2[3 * k + 1] = r2;
   }
-  lattice_pair<1, 1, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P, D);
-  lattice_pair<1, 1, -1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P, D);
-  lattice_pair<1, -1, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P, D);
-  lattice_pair<-1, 1, 1>(si, sn, sc, g1, g2, n, d1, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<1, 1, 1>(si, sn, sc, g1, g2, sides >> 6 & 3, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<1, 1, -1>(si, sn, sc, g1, g2, sides >> 8 & 3, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<1, -1, 1>(si, sn, sc, g1, g2, sides >> 10 & 3, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<-1, 1, 1>(si, sn, sc, g1, g2, sides >> 12 & 3, dt, c45, c15, w7, rhoI, m, P, D);
   rhoI += D;
   P[0] += D;
   P[1] += D;
   P[2] += D;
 
-  const double tau = f2w;  // 3 nu / (dt_s gamma), per face from the layout
-  const double mn = m[0] * n[0] + m[1] * n[1] + m[2] * n[2];
-  const double Pn[3] = {P[0] * n[0] + P[3] * n[1] + P[4] * n[2],
-                        P[3] * n[0] + P[1] * n[1] + P[5] * n[2],
-                        P[4] * n[0] + P[5] * n[1] + P[2] * n[2]};
+  // n, A and the relaxation factor 3 nu / (dt_s gamma) are read again here
+  // (an L1 hit) rather than held in registers through the pairs.
+  const d4 g0 = ld4(launder(a.face0), f);
+  const double nf[3] = {g0.x, g0.y, g0.z};
+  const double area = g0.w;
+  const double tau = __ldg(static_cast<const double*>(launder(a.face2)) + 4LL * f + 3);
+  const double mn = m[0] * nf[0] + m[1] * nf[1] + m[2] * nf[2];
+  const double Pn[3] = {P[0] * nf[0] + P[3] * nf[1] + P[4] * nf[2],
+                        P[3] * nf[0] + P[1] * nf[1] + P[5] * nf[2],
+                        P[4] * nf[0] + P[5] * nf[1] + P[2] * nf[2]};
   const double p3 = rhoI * (1.0 / 3.0);
   const double mnr = mn / rhoI * pg;
   d4 out;
-  out.x = ((1.0 - tau) * fma(m[0], mnr, p3 * n[0]) + tau * Pn[0]) * area;
-  out.y = ((1.0 - tau) * fma(m[1], mnr, p3 * n[1]) + tau * Pn[1]) * area;
-  out.z = ((1.0 - tau) * fma(m[2], mnr, p3 * n[2]) + tau * Pn[2]) * area;
+  out.x = ((1.0 - tau) * fma(m[0], mnr, p3 * nf[0]) + tau * Pn[0]) * area;
+  out.y = ((1.0 - tau) * fma(m[1], mnr, p3 * nf[1]) + tau * Pn[1]) * area;
+  out.z = ((1.0 - tau) * fma(m[2], mnr, p3 * nf[2]) + tau * Pn[2]) * area;
   out.w = mn * area;
   st4(a.flux, f, out);
 }
@@ -374,9 +416,9 @@ __device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, cons
 // Persistent over the faces (grid stride): the owner/neighbour ids of a
 // thread's next face are loaded before its current face is computed, so the
 // next face's cell gathers do not wait behind a load of its face record.
-// Three blocks per SM leave 168 registers a thread, enough to hold a face's
-// gradients without spilling.
-__global__ void __launch_bounds__(kFluxBlock, 3) k_flux(const KernelArgs a) {
+// Four blocks per SM (128 registers, a few doubles spilled to L1) measured
+// faster than three without spills (73 vs 75 us): latency hiding wins.
+__global__ void __launch_bounds__(kFluxBlock, 4) k_flux(const KernelArgs a) {
   if (halted(a)) return;
   const long long stride = (long long)gridDim.x * blockDim.x;
   long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -164,14 +164,16 @@ __device__ __forceinline__ float gdotf(const float* g) {
 struct PairConst {
   float d1, dt, hdt;
   float rho0, U, c45u, c15u;  // c45u = 4.5 U / gamma, c15u = 1.5 U / gamma
+  float u3, c45uu, c15uu;     // 3 U, U c45u, U c15u
 };
 
 // Deviation part of the equilibrium at one node: w [drho + rho U phi].
 __device__ __forceinline__ float feq_dev(const PairConst& k, float wgt, const float q[4],
                                          float eu) {
   const float u2 = fmaf(q[3], q[3], fmaf(q[2], q[2], q[1] * q[1]));
-  const float phi = fmaf(-k.c15u, u2, fmaf(k.c45u * eu, eu, 3.0f * eu));
-  return wgt * fmaf(k.rho0 + q[0], k.U * phi, q[0]);
+  // U phi = U (3 eu + c45u eu^2 - c15u u2), with U folded into the constants
+  const float uphi = fmaf(eu, fmaf(k.c45uu, eu, k.u3), -k.c15uu * u2);
+  return wgt * fmaf(k.rho0 + q[0], uphi, q[0]);
 }
 
 template <int EX, int EY, int EZ>
@@ -282,6 +284,9 @@ __device__ __forceinline__ void flux_face32(const KernelArgs& a, const int f, co
   const float pg = (float)a.pg;
   kc.c45u = 4.5f * kc.U * pg;
   kc.c15u = 1.5f * kc.U * pg;
+  kc.u3 = 3.0f * kc.U;
+  kc.c45uu = kc.U * kc.c45u;
+  kc.c15uu = kc.U * kc.c15u;
   const float w0 = 2.0f / 9.0f, w1 = 1.0f / 9.0f, w7 = 1.0f / 72.0f;
   // centre node: e = 0
   const float u2c = fmaf(sc[3], sc[3], fmaf(sc[2], sc[2], sc[1] * sc[1]));
