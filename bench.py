@@ -266,6 +266,23 @@ def time_to_residual(args):
         out[name] = {"converged": bool(st["converged"]), "steps": st["steps_done"],
                      "device_s": st["kernel_ms"] / 1e3, "wall_s": wall,
                      "final_max_error": st["max_error"], "cd": cd, "cl": cl}
+    # FP32 from the trained network's prediction (plfbs/data/warmstart_params.npz);
+    # the same channel, sphere and Re (a member of the network's training family)
+    from plfbs import warmstart
+    if os.path.exists(warmstart.PARAMS):
+        centre = (2 * 8.0, 16.0, 16.0)
+        t0 = time.perf_counter()
+        ws = warmstart.WarmStarter()
+        t1 = time.perf_counter()
+        start = ws.start(100.0, centre)
+        infer = time.perf_counter() - t1
+        rec, q = ws.ch.solve(100.0, centre, capi.FP32_DEVIATION, args.time_to_residual,
+                             args.max_steps, start=start)
+        ws.close()
+        rec.update(nn_inference_s=infer, nn_setup_s=t1 - t0,
+                   wall_s_with_inference=rec["wall_s"] + infer)
+        out["fp32_nn"] = rec
+        states["fp32_nn"] = q
     a, b = states["fp64"], states["fp32"]
     err = {k: float(np.linalg.norm(b[:, i] - a[:, i]) / np.linalg.norm(a[:, i]))
            for i, k in enumerate(("u", "v", "w"))}
@@ -274,8 +291,11 @@ def time_to_residual(args):
             "unit": "s", "higher_is_better": False, "data": "synthetic",
             "config": {"workload": TTR_WORKLOAD, "cells": ma.n_cells, "faces": ma.n_faces,
                        "nodes": len(ibm["node_ref"]), "start": "uniform flow (cold)"},
-            "fp64": out["fp64"], "fp32": out["fp32"],
+            "fp64": out["fp64"], "fp32": out["fp32"], "fp32_nn": out.get("fp32_nn"),
             "speedup_fp32_over_fp64": out["fp64"]["wall_s"] / out["fp32"]["wall_s"],
+            "speedup_fp32_nn_over_fp64": (out["fp64"]["wall_s"] /
+                                          out["fp32_nn"]["wall_s_with_inference"]
+                                          if "fp32_nn" in out else None),
             "fp32_vs_fp64_rel_l2": err,
             "cd_rel_diff": abs(out["fp32"]["cd"] - out["fp64"]["cd"]) / abs(out["fp64"]["cd"])}
     print(json.dumps(line))
