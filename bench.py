@@ -302,6 +302,93 @@ def time_to_residual(args):
     return 0
 
 
+def compare_precisions(args):
+    """FP32 deviation form against the FP64 path on the other configurations:
+    `tets` = 64^3 unit hexes with interior nodes jittered (seeded), each split
+    into 6 tetrahedra (1,572,864 cells), Taylor-Green initial field (U 0.05),
+    Re 400 on L = 64, Dirichlet u = 0 walls, 500 steps of dt 0.05, exact-inverse
+    least squares (the reference's determinant is unstable on tets). Jitter
+    +-0.1 of the spacing: at +-0.2 the scheme diverges near t = 4.5 whatever
+    Re, U or dt (a mesh-quality instability), at +-0.1 and below it does not;
+    `scale` = 256 x 128 x 128 channel, sphere D 32 at (64, 64, 64) with 12,869
+    nodes, Re 200, 2000 steps. One JSON line: throughput, the flux kernel's
+    fraction of the measured HBM bandwidth, per-field relative L2 of FP32
+    against FP64, and (scale) Cd of both."""
+    from plfbs import capi
+    if args.compare == "tets":
+        n, u0, re, steps = 64, 0.05, 400.0, 500
+        pm = cases.jittered_tet_box(n, jitter=args.jitter, seed=11, patch_types=["wall"] * 6)
+        c = cases.Case(mesh_dir="", X=n, Y=n, Z=n, dt=args.compare_dt or 0.05, mach=u0,
+                       reynolds=re, ref_length=n,
+                       bcs=[cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann")])
+        ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
+        x = np.asarray(ma.cell_centroid).reshape(-1, 3) * (2 * np.pi / n)
+        state0 = np.zeros((ma.total_cells, 4))
+        state0[:, 0] = u0 * np.sin(x[:, 0]) * np.cos(x[:, 1]) * np.cos(x[:, 2])
+        state0[:, 1] = -u0 * np.cos(x[:, 0]) * np.sin(x[:, 1]) * np.cos(x[:, 2])
+        state0[:, 3] = 1.0
+        ibm, area, mode = None, None, capi.GRAD_EXACT_INVERSE
+        name = "tgv_tets_64cubed_jitter%g_re400" % args.jitter
+    else:
+        nx, ny, nz, d, re, steps = 256, 128, 128, 32.0, 200.0, 2000
+        pm = cases.uniform_box(nx, ny, nz, patch_types=["inlet", "outlet", "side", "side",
+                                                        "side", "side"])
+        c = cases.Case(mesh_dir="", X=nx, Y=ny, Z=nz, dt=DT, mach=U, reynolds=re,
+                       ref_length=d, tolerance=0.0,
+                       bcs=[cases.BC("inlet", 1, 1, 0, 0, "dirichlet", "neumann"),
+                            cases.BC("outlet", 1, 0, 0, 0, "neumann", "dirichlet"),
+                            cases.BC("side", 1, 0, 0, 0, "neumann", "neumann")])
+        ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
+        nodes = cases.fibonacci_sphere(12869, d / 2, (64.0, 64.0, 64.0))
+        ibm = dict(node_ref=nodes, stiffness=STIFFNESS, radius=d / 2, depth=d,
+                   object_nodes=len(nodes))
+        state0 = np.zeros((ma.total_cells, 4))
+        state0[:, 0] = U
+        state0[:, 3] = 1.0
+        area, mode = np.pi * d * d / 4, 0
+        name = "sphere_channel_256x128x128_ibm12869_re200"
+    rt, vt, val = cases.bc_arrays(ma, c)
+    peak, peak_kind = load_peaks()
+    out, states = {}, {}
+    for prec_name, prec in (("fp64", capi.FP64), ("fp32", capi.FP32_DEVIATION)):
+        cfg = solver_cfg(c, prec)
+        cfg["gradient_mode"] = mode
+        s = capi.Solver(ma, rt, vt, val, cfg, ibm=ibm)
+        s.set_state(state0)
+        st, _ = s.run(steps, history=False)
+        if st["rc"] != 0 or st["steps_done"] != steps:
+            print(json.dumps({"metric": "fp32-vs-fp64", "config": {"workload": name},
+                              "failed": "%s stopped after %d steps (status %d)"
+                              % (prec_name, st["steps_done"], st["rc"])}))
+            return 1
+        r = {"steps": int(st["steps_done"]), "ms_per_step": st["kernel_ms"] / steps,
+             "mcell_updates_per_s": ma.n_cells * steps / st["kernel_ms"] / 1e3}
+        prof = s.profile_steps(10)
+        flux_ms = prof["flux"] / 40
+        alg = algorithmic_bytes(ma.n_cells, ma.n_faces, ma.n_bc, fp32=prec_name == "fp32")
+        r["flux_ms"] = flux_ms
+        r["flux_hbm_frac"] = alg["flux"] / (flux_ms / 1e3) / 1e9 / peak
+        s.set_state(state0)
+        s.run(steps, history=False)  # the same state after exactly `steps` steps
+        if area:
+            r["cd"], r["cl"] = s.body_force(area)
+        states[prec_name] = s.get_state()
+        s.close()
+        out[prec_name] = r
+    a, b = states["fp64"][: ma.n_cells], states["fp32"][: ma.n_cells]
+    err = {k: float(np.linalg.norm(b[:, i] - a[:, i]) / np.linalg.norm(a[:, i]))
+           for i, k in enumerate(("u", "v", "w"))}
+    err["rho-rho0"] = float(np.linalg.norm(b[:, 3] - a[:, 3]) / np.linalg.norm(a[:, 3] - 1.0))
+    line = {"metric": "fp32-vs-fp64", "config": {"workload": name, "cells": ma.n_cells,
+                                                 "faces": ma.n_faces, "steps": steps},
+            "peak_gbs": peak, "peak_kind": peak_kind, "fp64": out["fp64"], "fp32": out["fp32"],
+            "fp32_vs_fp64_rel_l2": err}
+    if area:
+        line["cd_rel_diff"] = abs(out["fp32"]["cd"] - out["fp64"]["cd"]) / abs(out["fp64"]["cd"])
+    print(json.dumps(line))
+    return 0
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -350,6 +437,10 @@ def main():
                     help="instead of throughput: steps and time to max_error < this value, "
                          "FP64 vs FP32 from a cold start")
     ap.add_argument("--max-steps", type=int, default=100000)
+    ap.add_argument("--compare", choices=["tets", "scale"], default=None,
+                    help="instead of throughput: FP32 vs FP64 on another configuration")
+    ap.add_argument("--compare-dt", type=float, default=None, help="RK dt of the tets case")
+    ap.add_argument("--jitter", type=float, default=0.1, help="node jitter of the tets case")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -359,6 +450,8 @@ def main():
         return run_reference_arm(args, rank, world)
     if args.time_to_residual is not None:
         return time_to_residual(args) if rank == 0 else 0
+    if args.compare is not None:
+        return compare_precisions(args) if rank == 0 else 0
 
     dist = None
     if world > 1:
