@@ -289,6 +289,246 @@ __global__ void __launch_bounds__(kThreads, 2) k_mlp_fwd(const Fwd a) {
 }
 
 // ---------------------------------------------------------------------------
+// forward on the fifth-generation tensor cores (tcgen05). Operands sit in
+// shared memory in the canonical K-major layout without swizzle: 8-row x
+// 16-byte core matrices, the K-adjacent ones 128 B apart (leading byte
+// offset), 8-row groups K x 16 B apart (stride byte offset). One thread issues
+// the MMAs (128 x N x 16 each, BF16 in, FP32 accumulators in tensor memory)
+// and commits them to an mbarrier; a warp reads the 32 accumulator rows of
+// its lane quarter (warp % 4) with tcgen05.ld, one row per thread, warps w
+// and w + 4 taking the two halves of the columns.
+// ---------------------------------------------------------------------------
+constexpr int kTcThreads = 256;  // 8 warps: warps w and w + 4 share accumulator rows
+
+__device__ __forceinline__ uint32_t canon_off(int r, int k, int K) {
+  return (uint32_t)((r >> 3) * (K * 16) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+__device__ __forceinline__ uint64_t smem_desc(const void* base, int K) {
+  const uint64_t addr = su32(base);
+  return ((addr & 0x3FFFFull) >> 4) | ((uint64_t)(128 >> 4) << 16) |
+         ((uint64_t)((K * 16) >> 4) << 32) | (1ull << 46);
+}
+// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
+// K-major, N >> 3 and M >> 4.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
+                                     int accumulate) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                   su32(mbar))
+               : "memory");
+}
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(su32(mbar)), "r"(count)
+               : "memory");
+}
+// Waits for the mbarrier phase of the given parity; gives up (false) after a
+// bounded number of tries instead of spinning for ever.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
+  for (int i = 0; i < (1 << 22); i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(su32(mbar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, int ncols) {  // one whole warp
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                   su32(slot)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, int ncols) {  // the same warp
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+// 16 consecutive FP32 columns of this thread's row (lane) of the accumulator.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
+// As load_x, into the canonical layout.
+template <int MODE, int K1>
+__device__ __forceinline__ void load_x_canon(const Rows& a, int row0, unsigned char* As) {
+  constexpr int C4 = K1 / 4;
+  for (int q = threadIdx.x; q < TM * C4; q += kTcThreads) {
+    const int r = q / C4, c4 = q - r * C4, m = row0 + r;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (m < a.M) {
+      if (MODE == ENC) {
+        v = ldg4(a.x0 + (size_t)m * FP + 4 * c4);
+      } else if (MODE == DEC) {
+        v = ldg4(a.x0 + (size_t)m * H + 4 * c4);
+      } else if (MODE == EDGE) {
+        const int seg = c4 >> 4, cc = (c4 & 15) * 4;
+        const float* p = seg == 0 ? a.x0 + (size_t)m * H
+                                  : a.hs + (size_t)(seg == 1 ? a.src[m] : a.dst[m]) * H;
+        v = ldg4(p + cc);
+      } else {
+        const int seg = c4 >> 4, cc = (c4 & 15) * 4;
+        if (seg == 0) {
+          v = ldg4(a.x0 + (size_t)m * H + cc);
+        } else {
+          for (int k = a.in_off[m]; k < a.in_off[m + 1]; k++) {
+            const float4 e = ldg4(a.eagg + (size_t)a.in_idx[k] * H + cc);
+            v.x += e.x;
+            v.y += e.y;
+            v.z += e.z;
+            v.w += e.w;
+          }
+        }
+      }
+    }
+    st_bf16x4(reinterpret_cast<bf16*>(As + canon_off(r, 4 * c4, K1)), v);
+  }
+}
+
+template <int MODE, int K1, int NOUT>
+__global__ void __launch_bounds__(kTcThreads) k_mlp_fwd_tc(const Fwd a, int* err) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned char* As = smem;                       // [128][K1]
+  unsigned char* Hs = As + TM * K1 * 2;           // [128][64]
+  unsigned char* W1t = Hs + TM * H * 2;           // [64][K1]: W1 transposed
+  unsigned char* W2t = W1t + H * K1 * 2;          // [NOUT][64]: W2 transposed
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(W2t + NOUT * H * 2);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(mbar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < K1 * H; i += kTcThreads)
+    *reinterpret_cast<bf16*>(W1t + canon_off(i % H, i / H, K1)) = a.W1[i];
+  for (int i = tid; i < H * NOUT; i += kTcThreads)
+    *reinterpret_cast<bf16*>(W2t + canon_off(i % NOUT, i / NOUT, H)) = a.W2[i];
+  if (tid == 0) mbar_init(mbar, 1);
+  if (warp == 0) tmem_alloc(slot, 128);
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *slot, d1 = tmem, d2 = tmem + 64;
+  const int quarter = warp & 3, half = warp >> 2;
+  const uint32_t lanes = (uint32_t)(quarter * 32) << 16;  // this warp's 32 accumulator rows
+  const int r = quarter * 32 + lane;                       // this thread's row of the tile
+  uint32_t parity = 0;
+  bool ok = true;
+  const int ntiles = (a.x.M + TM - 1) / TM;
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int row0 = tile * TM, m = row0 + r;
+    load_x_canon<MODE, K1>(a.x, row0, As);
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int k0 = 0; k0 < K1; k0 += 16)
+        umma(d1, smem_desc(As + k0 * 16, K1), smem_desc(W1t + k0 * 16, K1),
+             idesc_bf16(TM, H), k0 > 0);
+      umma_commit(mbar);
+    }
+    __syncwarp();
+    ok = mbar_wait(mbar, parity);
+    parity ^= 1u;
+    tc_fence_after();
+#pragma unroll
+    for (int c0 = 32 * half; c0 < 32 * half + 32; c0 += 16) {
+      float v[16];
+      tmem_ld16(d1 + lanes + c0, v);
+      __align__(16) bf16 hb[16];
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        v[i] += a.b1[c0 + i];
+        hb[i] = __float2bfloat16_rn(fmaxf(v[i], 0.f));
+      }
+      if (a.z1 && m < a.x.M) {
+        float4* z = reinterpret_cast<float4*>(a.z1 + (size_t)m * H + c0);
+#pragma unroll
+        for (int i = 0; i < 4; i++) z[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+      }
+      *reinterpret_cast<uint4*>(Hs + canon_off(r, c0, H)) = *reinterpret_cast<const uint4*>(hb);
+      *reinterpret_cast<uint4*>(Hs + canon_off(r, c0 + 8, H)) =
+          *reinterpret_cast<const uint4*>(hb + 8);
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int k0 = 0; k0 < H; k0 += 16)
+        umma(d2, smem_desc(Hs + k0 * 16, H), smem_desc(W2t + k0 * 16, H), idesc_bf16(TM, NOUT),
+             k0 > 0);
+      umma_commit(mbar);
+    }
+    __syncwarp();
+    ok = ok && mbar_wait(mbar, parity);
+    parity ^= 1u;
+    tc_fence_after();
+#pragma unroll
+    for (int c0 = 32 * half; c0 < 32 * half + 32 && c0 < NOUT; c0 += 16) {
+      float v[16];
+      tmem_ld16(d2 + lanes + c0, v);
+      if (m < a.x.M) {
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          v[i] += a.b2[c0 + i];
+          if (MODE == EDGE || MODE == NODE) v[i] += a.x.x0[(size_t)m * H + c0 + i];
+        }
+        float4* y = reinterpret_cast<float4*>(a.y + (size_t)m * NOUT + c0);
+#pragma unroll
+        for (int i = 0; i < 4; i++) y[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+      }
+    }
+    tc_fence_before();
+    ok = __syncthreads_and(ok);  // operands and accumulators free for the next tile
+  }
+  if (!ok && tid == 0) atomicExch(err, 1);
+  tc_fence_after();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 128);
+}
+
+// Shared memory of a launch: the operands, and at least 60 KB so that no SM
+// holds more than three blocks, whose 3 x 128 tensor-memory columns fit in
+// the 512 an SM has (tcgen05.alloc would otherwise wait for a block to end).
+template <int K1, int NOUT>
+constexpr size_t tc_smem() {
+  return std::max<size_t>(2 * (size_t)(TM * K1 + TM * H + H * K1 + NOUT * H) + 16, 61440);
+}
+
+// ---------------------------------------------------------------------------
 // backward
 // ---------------------------------------------------------------------------
 struct Bwd {
@@ -597,6 +837,8 @@ struct plfbs_gnn {
         *ddst = nullptr, *dagg = nullptr, *part = nullptr;
   double* loss_part = nullptr;
   int loss_blocks = 0;
+  int use_tc = 0;           // forward on tcgen05 (1) or mma.sync (0)
+  int* tc_err = nullptr;    // set by the tcgen05 kernel if an MMA wait gave up
   std::string err;
 };
 
@@ -644,6 +886,13 @@ int set_smem(plfbs_gnn* g) {
   return 0;
 }
 
+template <int MODE, int K1, int NOUT>
+int set_smem_tc(plfbs_gnn* g) {
+  GCK(cudaFuncSetAttribute(k_mlp_fwd_tc<MODE, K1, NOUT>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem<K1, NOUT>()));
+  return 0;
+}
+
 int grid_for(plfbs_gnn* g, int M, int per_sm) {
   const int tiles = (M + TM - 1) / TM;
   return std::max(1, std::min(tiles, g->sms * per_sm));
@@ -652,6 +901,14 @@ int grid_for(plfbs_gnn* g, int M, int per_sm) {
 template <int MODE, int K1, int NOUT>
 int launch_fwd(plfbs_gnn* g, const Mlp& p, const Rows& x, float* z1, float* y) {
   Fwd a{x, p.W1, p.b1, p.W2, p.b2, z1, y};
+  if (g->use_tc) {
+    // two blocks per SM: 2 x 98 KB of shared memory, 2 x 128 tensor-memory columns
+    k_mlp_fwd_tc<MODE, K1, NOUT><<<grid_for(g, x.M, 2), kTcThreads, tc_smem<K1, NOUT>(),
+                                   g->stream>>>(
+        a, g->tc_err);
+    GCK(cudaGetLastError());
+    return 0;
+  }
   k_mlp_fwd<MODE, K1, NOUT><<<grid_for(g, x.M, 2), kThreads, fwd_smem<K1, NOUT>(), g->stream>>>(a);
   GCK(cudaGetLastError());
   return 0;
@@ -698,6 +955,15 @@ int forward(plfbs_gnn* g, bool train) {
   }
   Rows rd{N, g->h[L], nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   GTRY((launch_fwd<DEC, H, FP>(g, g->mlps[2 * L + 2], rd, train ? g->z_dec : nullptr, g->y)));
+  if (g->use_tc) {
+    int flag = 0;
+    GCK(cudaMemcpyAsync(&flag, g->tc_err, sizeof flag, cudaMemcpyDeviceToHost, g->stream));
+    GCK(cudaStreamSynchronize(g->stream));
+    if (flag) {
+      GCK(cudaMemsetAsync(g->tc_err, 0, sizeof flag, g->stream));
+      return gerr(g, PLFBS_ERR_CUDA, "a tensor-core MMA did not complete within its wait limit");
+    }
+  }
   return 0;
 }
 
@@ -803,8 +1069,11 @@ int plfbs_gnn_create(const plfbs_gnn_shape* shape, const int32_t* src, const int
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail(gerr(g, PLFBS_ERR_CUDA, "stream creation failed"));
   if ((rc = set_smem<ENC, FP, H>(g)) || (rc = set_smem<EDGE, 3 * H, H>(g)) ||
-      (rc = set_smem<NODE, 2 * H, H>(g)) || (rc = set_smem<DEC, H, FP>(g)))
+      (rc = set_smem<NODE, 2 * H, H>(g)) || (rc = set_smem<DEC, H, FP>(g)) ||
+      (rc = set_smem_tc<ENC, FP, H>(g)) || (rc = set_smem_tc<EDGE, 3 * H, H>(g)) ||
+      (rc = set_smem_tc<NODE, 2 * H, H>(g)) || (rc = set_smem_tc<DEC, H, FP>(g)))
     return fail(rc);
+  if ((rc = galloc(g, &g->tc_err, 1))) return fail(rc);
   // parameter layout
   auto add = [&](int mode, int K1, int NOUT, int kin, int o) {
     Mlp p;
@@ -946,6 +1215,13 @@ int plfbs_gnn_train_step(plfbs_gnn* g, const float* node_features, const float* 
   GCK(cudaGetLastError());
   GTRY(pack_all(g));
   GCK(cudaStreamSynchronize(g->stream));
+  return PLFBS_OK;
+}
+
+int plfbs_gnn_set_tensor_cores(plfbs_gnn* g, int32_t kind) {
+  if (!g) return gerr(nullptr, PLFBS_ERR_ARG, "null network");
+  if (kind != 0 && kind != 1) return gerr(g, PLFBS_ERR_ARG, "kind is 0 (mma.sync) or 1 (tcgen05)");
+  g->use_tc = kind;
   return PLFBS_OK;
 }
 

@@ -23,7 +23,8 @@ HIDDEN = 64
 
 EXPORTS = ("plfbs_gnn_create", "plfbs_gnn_param_count", "plfbs_gnn_set_params",
            "plfbs_gnn_get_params", "plfbs_gnn_forward", "plfbs_gnn_gradients",
-           "plfbs_gnn_train_step", "plfbs_gnn_last_error", "plfbs_gnn_destroy")
+           "plfbs_gnn_train_step", "plfbs_gnn_last_error", "plfbs_gnn_destroy",
+           "plfbs_gnn_set_tensor_cores")
 
 
 class Shape(C.Structure):
@@ -50,6 +51,7 @@ def lib():
         L.plfbs_gnn_last_error.argtypes = [C.c_void_p]
         L.plfbs_gnn_last_error.restype = C.c_char_p
         L.plfbs_gnn_destroy.argtypes = [C.c_void_p]
+        L.plfbs_gnn_set_tensor_cores.argtypes = [C.c_void_p, C.c_int32]
         _bound = True
     return L
 
@@ -151,6 +153,10 @@ class GraphNet:
         p = np.zeros(self.n_params, np.float32)
         self._check(lib().plfbs_gnn_get_params(self.h, _f(p), p.size))
         return p
+
+    def set_tensor_cores(self, kind):
+        """0: mma.sync forward, 1: tcgen05 forward."""
+        self._check(lib().plfbs_gnn_set_tensor_cores(self.h, int(kind)))
 
     def forward(self, x):
         x = np.ascontiguousarray(x, np.float32)

@@ -31,11 +31,13 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
+@pytest.mark.parametrize("kind", [0, 1], ids=["mma_sync", "tcgen05"])
 @pytest.mark.parametrize("layers", [1, 3])
-def test_forward_loss_and_gradients_match_reference(plfbs_lib, layers):
+def test_forward_loss_and_gradients_match_reference(plfbs_lib, layers, kind):
     ma, src, dst, ef, x = _graph()
     p = gnn.init_params(NF, EF, layers, OUT, seed=7, residual_scale=0.5)
     net = gnn.GraphNet(src, dst, ef, ma.n_cells, NF, layers, OUT)
+    net.set_tensor_cores(kind)
     assert net.n_params == p.size
     net.set_params(p)
     np.testing.assert_array_equal(net.get_params(), p)
@@ -73,3 +75,20 @@ def test_training_reduces_the_loss(plfbs_lib):
         last2 = net2.train_step(x, t, 2e-3)
     assert last2 == last
     np.testing.assert_array_equal(net.get_params(), net2.get_params())
+
+
+def test_tcgen05_forward_matches_mma_sync(plfbs_lib):
+    """The two tensor-core paths take the same BF16 operands; their FP32 sums
+    differ only in order. Larger graph: several 128-row tiles per block."""
+    ma, src, dst, ef, x = _graph(24, 20, 18)
+    p = gnn.init_params(NF, EF, 4, OUT, seed=5, residual_scale=0.5)
+    net = gnn.GraphNet(src, dst, ef, ma.n_cells, NF, 4, OUT)
+    net.set_params(p)
+    y0 = net.forward(x)
+    net.set_tensor_cores(1)
+    y1 = net.forward(x)
+    y2 = net.forward(x)
+    np.testing.assert_array_equal(y1, y2)  # deterministic
+    assert _rel(y1, y0) < 2e-3
+    with pytest.raises(gnn.GnnError):
+        net.set_tensor_cores(2)
