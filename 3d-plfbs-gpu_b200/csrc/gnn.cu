@@ -381,40 +381,51 @@ __device__ __forceinline__ void tc_fence_after() {
 __device__ __forceinline__ void fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
+// 256-bit global accesses (one full 32-byte sector per thread); p 32-byte aligned.
+__device__ __forceinline__ void ldg8(const float* p, float (&v)[8]) {
+  asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
+                 "=f"(v[6]), "=f"(v[7])
+               : "l"(p));
+}
+__device__ __forceinline__ void stg8(float* p, const float* v) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};\n" ::"l"(p), "f"(v[0]),
+               "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+               : "memory");
+}
 
-// As load_x, into the canonical layout.
+// As load_x, into the canonical layout: each thread moves one 8-element
+// (16-byte) core-matrix row, consecutive threads taking consecutive rows, so
+// that a warp's stores fill four whole core matrices (no bank conflicts) and
+// each thread reads one full 32-byte sector.
 template <int MODE, int K1>
 __device__ __forceinline__ void load_x_canon(const Rows& a, int row0, unsigned char* As) {
-  constexpr int C4 = K1 / 4;
-  for (int q = threadIdx.x; q < TM * C4; q += kTcThreads) {
-    const int r = q / C4, c4 = q - r * C4, m = row0 + r;
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  constexpr int C8 = K1 / 8;
+  for (int q = threadIdx.x; q < TM * C8; q += kTcThreads) {
+    const int r = q % TM, k = 8 * (q / TM), m = row0 + r;
+    float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (m < a.M) {
-      if (MODE == ENC) {
-        v = ldg4(a.x0 + (size_t)m * FP + 4 * c4);
-      } else if (MODE == DEC) {
-        v = ldg4(a.x0 + (size_t)m * H + 4 * c4);
-      } else if (MODE == EDGE) {
-        const int seg = c4 >> 4, cc = (c4 & 15) * 4;
-        const float* p = seg == 0 ? a.x0 + (size_t)m * H
-                                  : a.hs + (size_t)(seg == 1 ? a.src[m] : a.dst[m]) * H;
-        v = ldg4(p + cc);
-      } else {
-        const int seg = c4 >> 4, cc = (c4 & 15) * 4;
-        if (seg == 0) {
-          v = ldg4(a.x0 + (size_t)m * H + cc);
-        } else {
-          for (int k = a.in_off[m]; k < a.in_off[m + 1]; k++) {
-            const float4 e = ldg4(a.eagg + (size_t)a.in_idx[k] * H + cc);
-            v.x += e.x;
-            v.y += e.y;
-            v.z += e.z;
-            v.w += e.w;
-          }
+      if (MODE == NODE && k >= H) {
+        for (int e = a.in_off[m]; e < a.in_off[m + 1]; e++) {
+          float u[8];
+          ldg8(a.eagg + (size_t)a.in_idx[e] * H + (k - H), u);
+#pragma unroll
+          for (int i = 0; i < 8; i++) v[i] += u[i];
         }
+      } else {
+        const float* p;
+        if (MODE == ENC)
+          p = a.x0 + (size_t)m * FP + k;
+        else if (MODE == EDGE && k >= H)
+          p = a.hs + (size_t)(k < 2 * H ? a.src[m] : a.dst[m]) * H + (k & (H - 1));
+        else
+          p = a.x0 + (size_t)m * H + k;
+        ldg8(p, v);
       }
     }
-    st_bf16x4(reinterpret_cast<bf16*>(As + canon_off(r, 4 * c4, K1)), v);
+    __nv_bfloat162 b[4] = {__floats2bfloat162_rn(v[0], v[1]), __floats2bfloat162_rn(v[2], v[3]),
+                           __floats2bfloat162_rn(v[4], v[5]), __floats2bfloat162_rn(v[6], v[7])};
+    *reinterpret_cast<uint4*>(As + canon_off(r, k, K1)) = *reinterpret_cast<const uint4*>(b);
   }
 }
 
@@ -473,9 +484,8 @@ __global__ void __launch_bounds__(kTcThreads) k_mlp_fwd_tc(const Fwd a, int* err
         hb[i] = __float2bfloat16_rn(fmaxf(v[i], 0.f));
       }
       if (a.z1 && m < a.x.M) {
-        float4* z = reinterpret_cast<float4*>(a.z1 + (size_t)m * H + c0);
-#pragma unroll
-        for (int i = 0; i < 4; i++) z[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+        stg8(a.z1 + (size_t)m * H + c0, v);
+        stg8(a.z1 + (size_t)m * H + c0 + 8, v + 8);
       }
       *reinterpret_cast<uint4*>(Hs + canon_off(r, c0, H)) = *reinterpret_cast<const uint4*>(hb);
       *reinterpret_cast<uint4*>(Hs + canon_off(r, c0 + 8, H)) =
@@ -501,14 +511,20 @@ __global__ void __launch_bounds__(kTcThreads) k_mlp_fwd_tc(const Fwd a, int* err
       float v[16];
       tmem_ld16(d2 + lanes + c0, v);
       if (m < a.x.M) {
+        if (MODE == EDGE || MODE == NODE) {  // residual: the row's own previous state
+          float p0[8], p1[8];
+          ldg8(a.x.x0 + (size_t)m * H + c0, p0);
+          ldg8(a.x.x0 + (size_t)m * H + c0 + 8, p1);
 #pragma unroll
-        for (int i = 0; i < 16; i++) {
-          v[i] += a.b2[c0 + i];
-          if (MODE == EDGE || MODE == NODE) v[i] += a.x.x0[(size_t)m * H + c0 + i];
+          for (int i = 0; i < 8; i++) {
+            v[i] += p0[i];
+            v[8 + i] += p1[i];
+          }
         }
-        float4* y = reinterpret_cast<float4*>(a.y + (size_t)m * NOUT + c0);
 #pragma unroll
-        for (int i = 0; i < 4; i++) y[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+        for (int i = 0; i < 16; i++) v[i] += a.b2[c0 + i];
+        stg8(a.y + (size_t)m * NOUT + c0, v);
+        stg8(a.y + (size_t)m * NOUT + c0 + 8, v + 8);
       }
     }
     tc_fence_before();
@@ -837,7 +853,7 @@ struct plfbs_gnn {
         *ddst = nullptr, *dagg = nullptr, *part = nullptr;
   double* loss_part = nullptr;
   int loss_blocks = 0;
-  int use_tc = 0;           // forward on tcgen05 (1) or mma.sync (0)
+  int use_tc = 1;           // forward on tcgen05 (1, measured faster) or mma.sync (0)
   int* tc_err = nullptr;    // set by the tcgen05 kernel if an MMA wait gave up
   std::string err;
 };

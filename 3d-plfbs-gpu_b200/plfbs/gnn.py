@@ -155,7 +155,7 @@ class GraphNet:
         return p
 
     def set_tensor_cores(self, kind):
-        """0: mma.sync forward, 1: tcgen05 forward."""
+        """1: tcgen05 forward (the default), 0: mma.sync forward."""
         self._check(lib().plfbs_gnn_set_tensor_cores(self.h, int(kind)))
 
     def forward(self, x):

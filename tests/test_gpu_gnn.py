@@ -84,6 +84,7 @@ def test_tcgen05_forward_matches_mma_sync(plfbs_lib):
     p = gnn.init_params(NF, EF, 4, OUT, seed=5, residual_scale=0.5)
     net = gnn.GraphNet(src, dst, ef, ma.n_cells, NF, 4, OUT)
     net.set_params(p)
+    net.set_tensor_cores(0)
     y0 = net.forward(x)
     net.set_tensor_cores(1)
     y1 = net.forward(x)
