@@ -31,21 +31,33 @@ struct __align__(32) d4 {
   double x, y, z, w;
 };
 
+// Records of four doubles move as one 256-bit access (a whole 32-byte
+// sector per thread; every record array is 32-byte aligned): half the load
+// and store instructions of two 128-bit halves (step 0.541 -> 0.502 ms).
+// Read-only data: non-coherent load the compiler may schedule freely.
 __device__ __forceinline__ d4 ld4(const void* base, long long i) {
-  const double2* p = reinterpret_cast<const double2*>(base) + 2 * i;
-  double2 a = __ldg(p), b = __ldg(p + 1);
-  return d4{a.x, a.y, b.x, b.y};
+  const double* p = reinterpret_cast<const double*>(base) + 4 * i;
+  d4 v;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
+      : "l"(p));
+  return v;
 }
-// Plain (coherent) load, for data the same kernel also writes.
+// Coherent load, for data the same kernel also writes (kept in order).
 __device__ __forceinline__ d4 ld4rw(const void* base, long long i) {
-  const double2* p = reinterpret_cast<const double2*>(base) + 2 * i;
-  double2 a = p[0], b = p[1];
-  return d4{a.x, a.y, b.x, b.y};
+  const double* p = reinterpret_cast<const double*>(base) + 4 * i;
+  d4 v;
+  asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
+               : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
+               : "l"(p)
+               : "memory");
+  return v;
 }
 __device__ __forceinline__ void st4(void* base, long long i, const d4& v) {
-  double2* p = reinterpret_cast<double2*>(base) + 2 * i;
-  p[0] = make_double2(v.x, v.y);
-  p[1] = make_double2(v.z, v.w);
+  double* p = reinterpret_cast<double*>(base) + 4 * i;
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(v.x), "d"(v.y), "d"(v.z),
+               "d"(v.w)
+               : "memory");
 }
 
 // The same pointer, opaque to the compiler, so that a load through it is not
