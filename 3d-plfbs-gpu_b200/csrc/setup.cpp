@@ -2,11 +2,13 @@
 // weights, locality renumbering and the packed face / boundary / stencil /
 // gather records the kernels read.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <numeric>
 #include <queue>
 #include <sstream>
+#include <thread>
 
 #include "plfbs_internal.hpp"
 
@@ -70,6 +72,34 @@ std::vector<int32_t> rcm_order(int C, int Fi, const int32_t* owner, const int32_
 // z, (1,1,1), (1,1,-1), (1,-1,1), (-1,1,1)) the branch the flux kernel takes:
 // 1 if e.n > 0.001 dt, 2 if e.n < -0.001 dt, 0 in the dead band
 // (LBFS.cu:353-354); packed base 3.
+// body(i) for i in [0, n) on up to 16 host threads in contiguous chunks (the
+// per-cell and per-face loops of the layout are independent); serial for
+// small n or when no thread can be started.
+template <typename Body>
+void parallel_for(int n, const Body& body, int serial_below = 32768) {
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int nt = (int)std::min(16u, hw ? hw : 1u);
+  if (nt <= 1 || n < serial_below) {
+    for (int i = 0; i < n; i++) body(i);
+    return;
+  }
+  const int chunk = (n + nt - 1) / nt;
+  std::vector<std::thread> th;
+  int lo = 0;
+  for (; lo < n; lo += chunk) {
+    const int hi = std::min(n, lo + chunk);
+    try {
+      th.emplace_back([lo, hi, &body] {
+        for (int i = lo; i < hi; i++) body(i);
+      });
+    } catch (...) {
+      break;  // run what is left on this thread
+    }
+  }
+  for (int i = lo; i < n; i++) body(i);
+  for (auto& t : th) t.join();
+}
+
 int upwind_signature(const double* n, double dt) {
   static const int E[7][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 1},
                               {1, 1, -1}, {1, -1, 1}, {-1, 1, 1}};
@@ -95,7 +125,8 @@ int upwind_signature(const double* n, double dt) {
 int ls_weights(const plfbs_mesh_view& m, int mode, double* lhs_inv, double* rhs,
                std::string& err) {
   const int C = m.n_cells;
-  for (int i = 0; i < C; i++) {
+  std::atomic<int> bad(C);  // first cell with a singular matrix
+  parallel_for(C, [&](int i) {
     double L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     const double* ci = m.cell_centroid + 3 * (size_t)i;
     double max_area = 0.0, max_disp = 0.0;
@@ -153,9 +184,14 @@ int ls_weights(const plfbs_mesh_view& m, int mode, double* lhs_inv, double* rhs,
     o[7] = 1 / det * (b * g - a * h);
     o[8] = 1 / det * (a * e - b * dd);
     if (!finite(o[0]) || !finite(o[4]) || !finite(o[8])) {
-      err = msg("singular least-squares matrix for cell", i, 0);
-      return PLFBS_ERR_MESH;
+      int cur = bad.load();
+      while (i < cur && !bad.compare_exchange_weak(cur, i)) {
+      }
     }
+  });
+  if (bad.load() < C) {
+    err = msg("singular least-squares matrix for cell", bad.load(), 0);
+    return PLFBS_ERR_MESH;
   }
   return PLFBS_OK;
 }
@@ -285,16 +321,44 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
   std::vector<int32_t> fint(Fi), fbnd(B);
   std::iota(fint.begin(), fint.end(), 0);
   std::iota(fbnd.begin(), fbnd.end(), Fi);
-  std::vector<int32_t> sig(Fi);
-  for (int f = 0; f < Fi; f++) sig[f] = upwind_signature(m.face_normal + 3 * (size_t)f, m.streaming_dt[f]);
   constexpr int kFaceWindow = 4096;
-  std::stable_sort(fint.begin(), fint.end(), [&](int a, int b) {
-    const int oa = newc(m.owner[a]), ob = newc(m.owner[b]);
-    if (oa / kFaceWindow != ob / kFaceWindow) return oa / kFaceWindow < ob / kFaceWindow;
-    if (sig[a] != sig[b]) return sig[a] < sig[b];
-    if (oa != ob) return oa < ob;
-    return newc(m.neighbour[a]) < newc(m.neighbour[b]);
+  // one 64-bit key per face: window (high bits), signature (< 3^7, 12 bits),
+  // owner within the window (12 bits); then the new neighbour and the face.
+  struct FaceKey {
+    uint64_t key;
+    int32_t nb, f;
+  };
+  std::vector<FaceKey> keys(Fi);
+  parallel_for(Fi, [&](int f) {
+    const uint64_t o = (uint64_t)newc(m.owner[f]);
+    const uint64_t sig =
+        (uint64_t)upwind_signature(m.face_normal + 3 * (size_t)f, m.streaming_dt[f]);
+    keys[f] = FaceKey{((o / kFaceWindow) << 24) | (sig << 12) | (o % kFaceWindow),
+                      newc(m.neighbour[f]), f};
   });
+  // the window is the leading key: bucket by window, then sort the windows
+  // side by side
+  const int nwin = (C + kFaceWindow - 1) / kFaceWindow;
+  std::vector<int> woff(nwin + 1, 0);
+  for (const FaceKey& k : keys) woff[(k.key >> 24) + 1]++;
+  for (int w = 0; w < nwin; w++) woff[w + 1] += woff[w];
+  std::vector<FaceKey> sorted(Fi);
+  {
+    std::vector<int> pos(woff.begin(), woff.end() - 1);
+    for (const FaceKey& k : keys) sorted[pos[k.key >> 24]++] = k;
+  }
+  parallel_for(
+      nwin,
+      [&](int w) {
+        std::sort(sorted.begin() + woff[w], sorted.begin() + woff[w + 1],
+                  [](const FaceKey& a, const FaceKey& b) {
+                    if (a.key != b.key) return a.key < b.key;
+                    if (a.nb != b.nb) return a.nb < b.nb;
+                    return a.f < b.f;
+                  });
+      },
+      2);
+  for (int k = 0; k < Fi; k++) fint[k] = sorted[k].f;
   std::stable_sort(fbnd.begin(), fbnd.end(),
                    [&](int a, int b) { return newc(m.owner[a]) < newc(m.owner[b]); });
   L.face_old_of_new.resize(F);
@@ -324,7 +388,7 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
   L.face2.assign(4 * (size_t)F, 0.0);
   L.face_ids.assign(2 * (size_t)F, 0);
   const double visc3 = cfg.visc * 3, pg = 1.0 / cfg.gamma;
-  for (int k = 0; k < F; k++) {
+  parallel_for(F, [&](int k) {
     const int f = L.face_old_of_new[k];
     const int o = m.owner[f], nbo = m.neighbour[f];
     const double* n = m.face_normal + 3 * (size_t)f;
@@ -349,7 +413,7 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
     c[3] = visc3 / m.streaming_dt[f] * pg;
     L.face_ids[2 * (size_t)k] = newc(o);
     L.face_ids[2 * (size_t)k + 1] = newcell(nbo);
-  }
+  });
 
   // --- boundary records --------------------------------------------------------
   L.bc0.assign(4 * (size_t)B, 0.0);
@@ -395,7 +459,7 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
   L.st_wx.assign((size_t)K * C, 0.0);
   L.st_wy.assign((size_t)K * C, 0.0);
   L.st_wz.assign((size_t)K * C, 0.0);
-  for (int io = 0; io < C; io++) {
+  parallel_for(C, [&](int io) {
     const int in = newc(io);
     const double* Li = &lhs[9 * (size_t)io];
     int slot = 0;
@@ -407,7 +471,7 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
       L.st_wy[s] = Li[3] * r[0] + Li[4] * r[1] + Li[5] * r[2];
       L.st_wz[s] = Li[6] * r[0] + Li[7] * r[1] + Li[8] * r[2];
     }
-  }
+  });
 
   // --- face -> cell gather ------------------------------------------------------
   std::vector<int32_t> nf(C, 0);
