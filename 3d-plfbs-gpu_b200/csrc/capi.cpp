@@ -33,6 +33,8 @@ struct plfbs_ctx {
   long long stages_done = 0;       // stages run through plfbs_run_stages in the current step
   bool debug = false;
   bool have_state = false;
+  int* wall_buf = nullptr;   // device wall list of plfbs_wall_forces (grown on demand)
+  int wall_cap = 0;
   uint64_t fingerprint = 0;  // of the caller's mesh, checked when a checkpoint is loaded
   std::string err;
 };
@@ -458,6 +460,59 @@ void plfbs_destroy(plfbs_ctx* ctx) {
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
+}
+
+int plfbs_wall_forces(plfbs_ctx* ctx, const int32_t* wall_bc, int32_t n_wall, double* cd,
+                      double* cl) {
+  TRY(check_ctx(ctx));
+  if (!cd || !cl || n_wall < 0 || (n_wall > 0 && !wall_bc))
+    return set_err(ctx, PLFBS_ERR_ARG, "wall_forces needs the wall list and two outputs");
+  if (!ctx->have_state) return set_err(ctx, PLFBS_ERR_STATE, "wall_forces before set_state");
+  const Layout& L = ctx->L;
+  std::vector<int> walls(std::max(n_wall, 1) + 4, 0);  // [0, 4): a zero halt word, see below
+  for (int k = 0; k < n_wall; k++) {
+    const int i = wall_bc[k];
+    if (i < 0 || i >= L.B) return set_err(ctx, PLFBS_ERR_ARG, "wall index out of range");
+    const int b = L.bc_new_of_old[i];
+    const int vt = (int)L.bc3[4 * (size_t)b + 3] >> 8;
+    if (vt != 1 && vt != 2)
+      return set_err(ctx, PLFBS_ERR_BC, "wall faces need velocity type 1 (Dirichlet) or 2 (Neumann)");
+    walls[4 + k] = b;
+  }
+  // wall_buf: ints [0, 4) zero (a halt flag that reads 0), [4, 4 + n) the
+  // walls, then (16-byte aligned) the two sums
+  const size_t sums_at = ((size_t)(n_wall + 4) * sizeof(int) + 15) & ~(size_t)15;
+  if (!ctx->wall_buf || ctx->wall_cap < n_wall) {
+    void* p = nullptr;
+    TRY(dev_alloc(ctx, &p, sums_at + 2 * sizeof(double)));
+    ctx->wall_buf = static_cast<int*>(p);
+    ctx->wall_cap = n_wall;
+  }
+  int* dev_walls = ctx->wall_buf;
+  double* dev_out = reinterpret_cast<double*>(reinterpret_cast<char*>(dev_walls) + sums_at);
+  CK(cudaMemcpyAsync(dev_walls, walls.data(), (size_t)(n_wall + 4) * sizeof(int),
+                     cudaMemcpyHostToDevice, ctx->stream));
+  // gradients (and ghost states) of the current state, as the reference's
+  // update_unstructured_bcs + Get_LS_Gradients before cylinder_post_processing;
+  // a halted (converged) context still recomputes them: its copy of the
+  // arguments reads the halt flag from the zero word
+  plfbs::KernelArgs a = ctx->args;
+  a.stats = reinterpret_cast<plfbs::DevStats*>(dev_walls);
+  plfbs::launch_gradient(a, ctx->cfg.precision, ctx->stream);
+  CK(cudaGetLastError());
+  const double g = ctx->cfg.gamma;
+  plfbs::launch_wall_forces(ctx->args, ctx->cfg.precision, dev_walls + 4, n_wall,
+                            ctx->cfg.visc * g, g, dev_out, ctx->stream);
+  CK(cudaGetLastError());
+  double out[2];
+  CK(cudaMemcpyAsync(out, dev_out, sizeof out, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  // post_processing.cpp:168-169: drag on Y Z, lift on X Z
+  *cd = 2 * out[0] / ctx->cfg.ref_rho / (ctx->cfg.max_velocity * ctx->cfg.max_velocity) /
+        ctx->cfg.lengths[1] / ctx->cfg.lengths[2];
+  *cl = 2 * out[1] / ctx->cfg.ref_rho / (ctx->cfg.max_velocity * ctx->cfg.max_velocity) /
+        ctx->cfg.lengths[0] / ctx->cfg.lengths[2];
+  return PLFBS_OK;
 }
 
 int plfbs_release_cached(int32_t device) {

@@ -716,6 +716,95 @@ __global__ void __launch_bounds__(kIbmBlock) k_ibm(const KernelArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Wall forces of post_processing::cylinder_post_processing
+// (post_processing.cpp:50-173) over the listed boundary faces (internal bc
+// indices), from the current state and gradients (the reference calls it
+// after update_unstructured_bcs and Get_LS_Gradients on the host, so the
+// ghost gradients follow the host rules of gradients.cpp:441-463 and 592-645:
+// Dirichlet velocity 2 (u_b - u_o) / |d| times the face normal, Neumann the
+// owner's gradient times (1 - n)). Per face: p = rho_o gamma / 3,
+//   drag += ((p - nu gamma du/dx) n_x - nu gamma du/dy n_y) A
+//   lift += (nu gamma dv/dx n_x - (p - nu gamma dv/dy) n_y) A.
+// One block; the partial sums are added in a fixed order. out[2] = {drag, lift}.
+// ---------------------------------------------------------------------------
+constexpr int kWallBlock = 1024;
+
+__global__ void __launch_bounds__(kWallBlock) k_wall_forces(const KernelArgs a, const int* walls,
+                                                            int n, int fp32, double visc_g,
+                                                            double gamma, double* out) {
+  __shared__ double red[kWallBlock / 32][2];
+  double dr = 0.0, li = 0.0;
+  const long long Fi = (long long)a.F - a.B;  // boundary face of bc b: Fi + b
+  for (int k = threadIdx.x; k < n; k += kWallBlock) {
+    const int b = walls[k];
+    const long long f = Fi + b;
+    const int o = a.face_ids[2 * f];
+    double nx, ny, area, rho, uo, vo, ub, vb, dmag, gux, guy, gvx, gvy;
+    int types;
+    if (fp32) {  // deviation units: velocity / U, rho - rho0
+      const float4 f0 = reinterpret_cast<const float4*>(a.face0)[f];
+      const float4 q = reinterpret_cast<const float4*>(a.state)[o];
+      const float4 bv = reinterpret_cast<const float4*>(a.bc0)[b];
+      const float4 dd = reinterpret_cast<const float4*>(a.bc2)[b];
+      const float4 nm = reinterpret_cast<const float4*>(a.bc3)[b];
+      const float4 g0 = reinterpret_cast<const float4*>(a.grad)[3LL * o];
+      const float4 g1 = reinterpret_cast<const float4*>(a.grad)[3LL * o + 1];
+      const double U = a.uref;
+      nx = f0.x; ny = f0.y; area = f0.w;
+      rho = a.rho0 + q.w;
+      uo = U * q.x; vo = U * q.y; ub = U * bv.x; vb = U * bv.y;
+      dmag = dd.w;
+      types = (int)nm.w;
+      gux = U * g0.w; guy = U * g1.x; gvx = U * g1.z; gvy = U * g1.w;
+    } else {
+      const d4 f0 = ld4(a.face0, f), q = ld4(a.state, o), bv = ld4(a.bc0, b), dd = ld4(a.bc2, b),
+               nm = ld4(a.bc3, b), g0 = ld4(a.grad, 3LL * o), g1 = ld4(a.grad, 3LL * o + 1);
+      nx = f0.x; ny = f0.y; area = f0.w;
+      rho = q.w;
+      uo = q.x; vo = q.y; ub = bv.x; vb = bv.y;
+      dmag = dd.w;
+      types = (int)nm.w;
+      gux = g0.w; guy = g1.x; gvx = g1.z; gvy = g1.w;
+    }
+    double ux, uy, vx, vy;
+    if ((types >> 8) == 1) {  // Dirichlet velocity: get_ghost_grads
+      const double du = 2 * (ub - uo), dv = 2 * (vb - vo);
+      ux = du / dmag * nx;
+      uy = du / dmag * ny;
+      vx = dv / dmag * nx;
+      vy = dv / dmag * ny;
+    } else {  // Neumann velocity (the host checked the type)
+      ux = gux * (1 - nx);
+      uy = guy * (1 - ny);
+      vx = gvx * (1 - nx);
+      vy = gvy * (1 - ny);
+    }
+    const double p = rho / 3.0 * gamma;
+    dr = dr + ((p - visc_g * ux) * nx - visc_g * uy * ny) * area;
+    li = li + (visc_g * vx * nx - (p - visc_g * vy) * ny) * area;
+  }
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    dr += __shfl_down_sync(0xffffffffu, dr, s);
+    li += __shfl_down_sync(0xffffffffu, li, s);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5][0] = dr;
+    red[threadIdx.x >> 5][1] = li;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double d = 0.0, l = 0.0;
+    for (int w = 0; w < kWallBlock / 32; w++) {
+      d += red[w][0];
+      l += red[w][1];
+    }
+    out[0] = d;
+    out[1] = l;
+  }
+}
+
 inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
 }  // namespace
@@ -763,6 +852,12 @@ void launch_seed(const KernelArgs& a, int precision, bool conserved, cudaStream_
 void launch_ibm(const KernelArgs& a, int precision, cudaStream_t s) {
   if (precision == PLFBS_FP32_DEVIATION) return launch_ibm32(a, s);
   if (a.N > 0) k_ibm<<<blocks_for(8LL * a.N, kIbmBlock), kIbmBlock, 0, s>>>(a);
+}
+
+void launch_wall_forces(const KernelArgs& a, int precision, const int* walls, int n,
+                        double visc_gamma, double gamma, double* out, cudaStream_t s) {
+  k_wall_forces<<<1, kWallBlock, 0, s>>>(a, walls, n, precision == PLFBS_FP32_DEVIATION ? 1 : 0,
+                                          visc_gamma, gamma, out);
 }
 
 }  // namespace plfbs

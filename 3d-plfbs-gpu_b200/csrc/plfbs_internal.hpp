@@ -156,6 +156,8 @@ void launch_gradient(const KernelArgs& a, int precision, cudaStream_t stream);
 void launch_flux(const KernelArgs& a, int precision, cudaStream_t stream);
 void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t stream);
 void launch_seed(const KernelArgs& a, int precision, bool conserved, cudaStream_t stream);
+void launch_wall_forces(const KernelArgs& a, int precision, const int* walls, int n,
+                        double visc_gamma, double gamma, double* out, cudaStream_t stream);
 void launch_ibm32(const KernelArgs& a, cudaStream_t stream);
 void launch_gradient32(const KernelArgs& a, cudaStream_t stream);
 void launch_flux32(const KernelArgs& a, cudaStream_t stream);

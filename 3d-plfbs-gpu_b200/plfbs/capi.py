@@ -29,7 +29,8 @@ EXPORTS = ("plfbs_create", "plfbs_set_state", "plfbs_run", "plfbs_get_state",
            "plfbs_ls_weights", "plfbs_profile_steps", "plfbs_memory_bytes",
            "plfbs_last_error", "plfbs_destroy", "plfbs_version",
            "plfbs_residual_norms_noalloc", "plfbs_release_cached", "plfbs_warm_start",
-           "plfbs_checkpoint_bytes", "plfbs_save_checkpoint", "plfbs_load_checkpoint")
+           "plfbs_checkpoint_bytes", "plfbs_save_checkpoint", "plfbs_load_checkpoint",
+           "plfbs_wall_forces")
 
 
 class MeshView(C.Structure):
@@ -97,6 +98,7 @@ def lib():
         L.plfbs_release_cached.argtypes = [C.c_int32]
         L.plfbs_warm_start.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_int64, _dp, C.c_int32]
         L.plfbs_checkpoint_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        L.plfbs_wall_forces.argtypes = [C.c_void_p, _ip, C.c_int32, _dp, _dp]
         L.plfbs_save_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
         L.plfbs_load_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
         L.plfbs_release_cached.restype = C.c_int
@@ -283,6 +285,13 @@ class Solver:
             nx = np.ascontiguousarray(node_x, np.float64).reshape(self.N, 3)
         self._check(lib().plfbs_warm_start(self.h, *[_d(c) for c in cols], self.T,
                                            _d(nx) if nx is not None else None, self.N))
+
+    def wall_forces(self, wall_bc):
+        """(Cd, Cl) over the boundary faces `wall_bc` (caller numbering)."""
+        w = np.ascontiguousarray(wall_bc, np.int32)
+        cd, cl = C.c_double(), C.c_double()
+        self._check(lib().plfbs_wall_forces(self.h, _i(w), len(w), C.byref(cd), C.byref(cl)))
+        return cd.value, cl.value
 
     def checkpoint(self):
         """The context's lossless checkpoint image (bytes)."""

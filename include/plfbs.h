@@ -155,6 +155,20 @@ int plfbs_set_state(plfbs_ctx* ctx, const double* rho, const double* u, const do
 int plfbs_warm_start(plfbs_ctx* ctx, const double* rho, const double* u, const double* v,
                      const double* w, int64_t n_total, const double* node_x, int32_t n_nodes);
 
+/* Drag and lift coefficients over the wall faces of a body-fitted mesh, as
+ * post_processing::cylinder_post_processing (post_processing.cpp:50-173)
+ * computes them at the end of a run (Solver_gpu.cu:881-884), on the device
+ * and from the current state: the ghost states and the gradients are
+ * recomputed first, and the wall ghost gradients follow the reference's host
+ * rules (Dirichlet velocity 2 (u_b - u_o) / |d| times the face normal,
+ * Neumann the owner's gradient times (1 - n)). wall_bc [n_wall] lists the
+ * walls as boundary-face indices in the caller's numbering (the reference's
+ * bc_types[i] == "wall"); their velocity type must be 1 or 2. Normalisation
+ * of the reference: Cd = 2 D / (rho_ref U^2 Y Z), Cl = 2 L / (rho_ref U^2 X Z)
+ * with X, Y, Z = plfbs_config.lengths. Leaves the step state unchanged. */
+int plfbs_wall_forces(plfbs_ctx* ctx, const int32_t* wall_bc, int32_t n_wall, double* cd,
+                      double* cl);
+
 /* Lossless checkpoint at a step boundary (replaces the 6-digit text output of
  * Solution::output, Solution.cpp:221-251, as a restart source): the state,
  * the RK accumulator, the IBM nodes and the run status, in the caller's

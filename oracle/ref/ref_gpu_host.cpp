@@ -230,6 +230,7 @@ void gpu_solver::General_Purpose_Solver_mk_i(
   std::vector<double> history;  // per step: t, max_error, rho, u, v, w rms
   clone_a_to_b(n_cells, temp_soln.data(), soln_t1.data());  // Solver_gpu.cu:664
   int t_done = timesteps;
+  bool converged = false;
   for (int t = 0; t < timesteps; t++) {
     clone_a_to_b(n_cells, soln_t1.data(), soln_t0.data());
     get_cfl_device(n_cells, temp_soln.data(), cell_volume.data(), dt_local.data(),
@@ -331,10 +332,20 @@ void gpu_solver::General_Purpose_Solver_mk_i(
     history.insert(history.end(), row, row + 6);
     if (conv.max_error() < tol) {  // Solver_gpu.cu:870
       t_done = t + 1;
+      converged = true;
       break;
     }
   }
   soln.clone(temp_soln.data());
+  double wall_forces[2] = {0.0, 0.0};
+  if (converged) {
+    // Solver_gpu.cu:881-884: host ghost update, host gradients, wall forces
+    soln.update_unstructured_bcs(bcs, Mesh, domain, t_done - 1);
+    grads.Get_LS_Gradients(bcs, Mesh, domain, soln, globals);
+    pp.cylinder_post_processing(Mesh, globals, grads, bcs, soln, domain, wall_shear_stress);
+    wall_forces[0] = pp.drag_coef;
+    wall_forces[1] = pp.lift_coef;
+  }
   if (!dump.empty()) {
     dump_d(dump, "final_state", &temp_soln[0].x, {(size_t)total, 4});
     dump_d(dump, "final_t1", &soln_t1[0].x, {(size_t)total, 4});
@@ -347,7 +358,7 @@ void gpu_solver::General_Purpose_Solver_mk_i(
       for (int k = 0; k < 9; k++) nd[(size_t)n * 9 + k] = v[k];
     }
     dump_d(dump, "final_nodes", nd.data(), {(size_t)n_nodes, 9});
+    dump_d(dump, "wall_forces", wall_forces, {2});  // Cd, Cl (zero unless converged)
   }
-  (void)source; (void)quad_bcs_orig; (void)mg; (void)residual; (void)fmg; (void)pp;
-  (void)wall_shear_stress;
+  (void)source; (void)quad_bcs_orig; (void)mg; (void)residual; (void)fmg;
 }

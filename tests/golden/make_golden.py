@@ -8,7 +8,8 @@ golden_cases.py and keeps the dumps the tests compare against: the reference's
 pre-processed mesh arrays and least-squares weights, the ghost states,
 gradients, face fluxes, residuals and state after the first RK stage, the body
 force and Lagrangian nodes after the first IBM update, and the state, RK
-accumulator, residual history and nodes after the last step.
+accumulator, residual history and nodes after the last step, and (for a run
+that converges) the wall drag and lift coefficients of cylinder_post_processing.
 """
 
 from __future__ import annotations
@@ -30,7 +31,7 @@ KEEP = ("sizes", "owner", "neighbour", "stencil", "face_area", "streaming_dt", "
         "face_centroid", "cell_volume", "cell_centroid", "lhs_inv", "rhs_w", "bc_value",
         "bc_rho_type", "bc_vel_type", "state_init", "params", "s0_force", "s0_nodes",
         "s0_state_bc", "s0_grad", "s0_face_flux", "s0_residual", "s0_state_rk",
-        "final_state", "final_t1", "history", "steps_done", "final_nodes")
+        "final_state", "final_t1", "history", "steps_done", "final_nodes", "wall_forces")
 
 
 def main():
