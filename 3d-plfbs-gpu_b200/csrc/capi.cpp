@@ -8,6 +8,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -36,6 +37,7 @@ struct plfbs_ctx {
   int* wall_buf = nullptr;   // device wall list of plfbs_wall_forces (grown on demand)
   int wall_cap = 0;
   uint64_t fingerprint = 0;  // of the caller's mesh, checked when a checkpoint is loaded
+  int32_t* face_order = nullptr;  // device [F]: caller face of each device face
   std::string err;
 };
 
@@ -198,20 +200,141 @@ int download4(plfbs_ctx* ctx, const void* src, size_t n, std::vector<double>& ou
   return PLFBS_OK;
 }
 
-// FNV-1a over the mesh arrays that fix the internal numbering and geometry.
-uint64_t mesh_fingerprint(const plfbs_mesh_view& m) {
-  uint64_t h = 1469598103934665603ull;
-  auto mix = [&h](const void* p, size_t n) {
-    const unsigned char* b = static_cast<const unsigned char*>(p);
-    for (size_t i = 0; i < n; i++) h = (h ^ b[i]) * 1099511628211ull;
-  };
-  const int32_t sizes[3] = {m.n_cells, m.n_faces, m.n_internal};
-  mix(sizes, sizeof sizes);
-  mix(m.owner, sizeof(int32_t) * (size_t)m.n_faces);
-  mix(m.neighbour, sizeof(int32_t) * (size_t)m.n_faces);
-  mix(m.face_area, sizeof(double) * (size_t)m.n_faces);
-  mix(m.cell_volume, sizeof(double) * (size_t)m.n_cells);
-  return h;
+// Device memory that lives only while the layout is built: returned to the
+// pool (stream-ordered) when the builder returns, on every path.
+struct ScratchList {
+  plfbs_ctx* ctx;
+  std::vector<void*> v;
+  explicit ScratchList(plfbs_ctx* c) : ctx(c) {}
+  ~ScratchList() {
+    for (void* p : v) cudaFreeAsync(p, ctx->stream);
+  }
+  template <typename T>
+  int alloc(T** dst, size_t bytes, bool zero) {
+    cudaMemPool_t pool = device_pool(ctx->device);
+    if (!pool) return set_err(ctx, PLFBS_ERR_CUDA, "device memory pool creation failed");
+    void* p = nullptr;
+    CK(cudaMallocFromPoolAsync(&p, std::max<size_t>(bytes, 16), pool, ctx->stream));
+    v.push_back(p);
+    if (zero) CK(cudaMemsetAsync(p, 0, std::max<size_t>(bytes, 16), ctx->stream));
+    *dst = static_cast<T*>(p);
+    return PLFBS_OK;
+  }
+  template <typename T>
+  int upload(const T** dst, const T* src, size_t count) {
+    T* p = nullptr;
+    TRY(alloc(&p, count * sizeof(T), false));
+    if (count) CK(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    *dst = p;
+    return PLFBS_OK;
+  }
+};
+
+// The face, stencil and gather arrays of a context, built on the device from
+// the caller's mesh arrays (layout.cu); sets args' layout pointers, L.K2 and
+// the mesh fingerprint.
+int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
+  Layout& L = ctx->L;
+  KernelArgs& a = ctx->args;
+  const bool fp32 = ctx->cfg.precision == PLFBS_FP32_DEVIATION;
+  const size_t C = L.C, F = L.F, Fi = L.Fi, B = L.B, T = C + B;
+  const size_t nnz = (size_t)m.stencil_offsets[C];
+  const size_t nwin = (C + plfbs::kFaceWindow - 1) / plfbs::kFaceWindow;
+  const size_t es = fp32 ? sizeof(float) : sizeof(double);
+  ScratchList S(ctx);
+  plfbs::DevMesh d{};
+  d.C = L.C;
+  d.F = L.F;
+  d.Fi = L.Fi;
+  d.B = L.B;
+  TRY(S.upload(&d.owner, m.owner, F));
+  TRY(S.upload(&d.neighbour, m.neighbour, F));
+  TRY(S.upload(&d.area, m.face_area, F));
+  TRY(S.upload(&d.normal, m.face_normal, 3 * F));
+  TRY(S.upload(&d.fcen, m.face_centroid, 3 * F));
+  TRY(S.upload(&d.sdt, m.streaming_dt, F));
+  TRY(S.upload(&d.vol, m.cell_volume, C));
+  TRY(S.upload(&d.ccen, m.cell_centroid, 3 * T));
+  TRY(S.upload(&d.st_off, m.stencil_offsets, C + 1));
+  TRY(S.upload(&d.st_cells, m.stencil_cells, nnz));
+  TRY(S.upload(&d.st_faces, m.stencil_faces, nnz));
+  TRY(S.upload(&d.bc_new, L.bc_new_of_old.data(), B));
+  TRY(S.upload(&d.bc_old, L.bc_old_of_new.data(), B));
+  void* p = nullptr;
+  TRY(dev_upload(ctx, &p, L.cell_new_of_old));  // kept: the IBM kernels map caller cells with it
+  d.cell_new = static_cast<const int32_t*>(p);
+  plfbs::LayoutScratch s{};
+  TRY(S.alloc(&s.own_cnt, 4 * C, true));
+  TRY(S.alloc(&s.own_off, 4 * C, false));
+  TRY(S.alloc(&s.cursor, 4 * C, true));
+  TRY(S.alloc(&s.deg, 4 * C, true));
+  TRY(S.alloc(&s.gcnt, 4 * C, true));
+  TRY(S.alloc(&s.wsum, 4 * nwin, false));
+  TRY(S.alloc(&s.wbase, 4 * (nwin + 1), false));
+  TRY(S.alloc(&s.seg, 4 * Fi, false));
+  TRY(S.alloc(&s.sig, 2 * Fi, false));
+  TRY(S.alloc(&s.info, 4 * sizeof(int32_t), false));
+  TRY(S.alloc(&s.fingerprint, sizeof(unsigned long long), true));
+  const int32_t info0[4] = {L.C, 0, 0, 0};
+  CK(cudaMemcpyAsync(s.info, info0, sizeof info0, cudaMemcpyHostToDevice, ctx->stream));
+
+  TRY(pool_alloc(ctx, &p, 4 * F));
+  ctx->face_order = static_cast<int32_t*>(p);
+  TRY(pool_alloc(ctx, &p, 8 * F));
+  int32_t* face_ids = static_cast<int32_t*>(p);
+  void* face[3];
+  for (void*& f : face) TRY(pool_alloc(ctx, &f, 4 * es * F));
+  TRY(pool_alloc(ctx, &p, 4 * (size_t)L.K * C));
+  int32_t* st_nbr = static_cast<int32_t*>(p);
+  CK(cudaMemsetAsync(st_nbr, 0xff, 4 * (size_t)L.K * C, ctx->stream));
+  void* w[3];
+  for (void*& x : w) TRY(dev_alloc(ctx, &x, es * L.K * C));
+  void* inv_volume = nullptr;
+  TRY(pool_alloc(ctx, &inv_volume, es * C));
+
+  plfbs::launch_layout_order(d, s, ctx->face_order, ctx->stream);
+  plfbs::launch_layout_records(d, s, ctx->cfg.precision, ctx->cfg.gradient_mode,
+                               ctx->cfg.visc * 3, 1.0 / ctx->cfg.gamma, ctx->face_order, face_ids,
+                               face[0], face[1], face[2], st_nbr, w[0], w[1], w[2], inv_volume,
+                               ctx->stream);
+  CK(cudaGetLastError());
+  struct {
+    int32_t info[4];
+    unsigned long long fp;
+  } back;
+  CK(cudaMemcpyAsync(back.info, s.info, sizeof back.info, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(&back.fp, s.fingerprint, sizeof back.fp, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (back.info[0] < L.C) {
+    std::ostringstream e;
+    e << "singular least-squares matrix for cell (index " << back.info[0] << ", value 0)";
+    return set_err(ctx, PLFBS_ERR_MESH, e.str());
+  }
+  L.K2 = back.info[1];
+  if (fp32 && L.K2 > 16)
+    return set_err(ctx, PLFBS_ERR_MESH, "the FP32 form handles cells with at most 16 faces");
+  TRY(pool_alloc(ctx, &p, 4 * (size_t)L.K2 * C));
+  int32_t* gather = static_cast<int32_t*>(p);
+  CK(cudaMemsetAsync(gather, 0xff, 4 * (size_t)L.K2 * C, ctx->stream));
+  plfbs::launch_layout_gather(d, s, face_ids, gather, ctx->stream);
+  CK(cudaGetLastError());
+  // sizes folded into the device's sum over the arrays
+  uint64_t h = back.fp;
+  for (int64_t v : {(int64_t)L.C, (int64_t)L.F, (int64_t)L.Fi}) h = (h ^ (uint64_t)v) * 1099511628211ull;
+  ctx->fingerprint = h;
+  a.K2 = L.K2;
+  a.face_ids = face_ids;
+  a.face0 = face[0];
+  a.face1 = face[1];
+  a.face2 = face[2];
+  a.st_nbr = st_nbr;
+  a.st_wx = w[0];
+  a.st_wy = w[1];
+  a.st_wz = w[2];
+  a.gather = gather;
+  a.inv_volume = inv_volume;
+  a.ibm_map = d.cell_new;
+  return PLFBS_OK;
 }
 
 int check_ctx(plfbs_ctx* ctx) {
@@ -243,6 +366,106 @@ int plfbs_ls_weights(const plfbs_mesh_view* mesh, int32_t gradient_mode, double*
   return rc;
 }
 
+}  // extern "C"
+
+namespace {
+
+int check_device(int device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0)
+    return set_err(nullptr, PLFBS_ERR_NO_DEVICE, "no CUDA device with that index");
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10)
+    return set_err(nullptr, PLFBS_ERR_NO_DEVICE,
+                   "this library is built for sm_100a (B200); device major != 10");
+  return PLFBS_OK;
+}
+
+int polymesh_geometry(plfbs_ctx* ctx, const plfbs_polymesh_view& pm, double ref_dt,
+                      plfbs_mesh_arrays& out) {
+  const size_t P = pm.n_points, F = pm.n_faces, Fi = pm.n_internal, C = pm.n_cells;
+  const size_t B = F - Fi, T = C + B, nnz = 2 * Fi + B;
+  const size_t nwin = (C + plfbs::kFaceWindow - 1) / plfbs::kFaceWindow;
+  ScratchList S(ctx);
+  plfbs::DevPolyMesh d{};
+  d.P = pm.n_points;
+  d.F = pm.n_faces;
+  d.Fi = pm.n_internal;
+  d.C = pm.n_cells;
+  TRY(S.upload(&d.points, pm.points, 3 * P));
+  TRY(S.upload(&d.face_offsets, pm.face_offsets, F + 1));
+  TRY(S.upload(&d.face_points, pm.face_points, (size_t)pm.face_offsets[F]));
+  TRY(S.upload(&d.owner, pm.owner, F));
+  TRY(S.upload(&d.neighbour, pm.neighbour, Fi));
+  plfbs::GeometryOut o{};
+  TRY(S.alloc(&o.area, 8 * F, false));
+  TRY(S.alloc(&o.normal, 24 * F, false));
+  TRY(S.alloc(&o.fcen, 24 * F, false));
+  TRY(S.alloc(&o.sdt, 8 * F, false));
+  TRY(S.alloc(&o.vol, 8 * T, false));
+  TRY(S.alloc(&o.ccen, 24 * T, false));
+  TRY(S.alloc(&o.st_off, 4 * (C + 1), false));
+  TRY(S.alloc(&o.st_cells, 4 * nnz, false));
+  TRY(S.alloc(&o.st_faces, 4 * nnz, false));
+  plfbs::GeometryScratch g{};
+  TRY(S.alloc(&g.fcsum, 24 * F, false));
+  TRY(S.alloc(&g.cnt, 4 * C, true));
+  TRY(S.alloc(&g.cursor, 4 * C, true));
+  TRY(S.alloc(&g.own_off, 4 * C, false));
+  TRY(S.alloc(&g.wsum, 4 * nwin, false));
+  TRY(S.alloc(&g.wbase, 4 * (nwin + 1), false));
+  TRY(S.alloc(&g.info, 16, true));
+  plfbs::launch_polymesh_geometry(d, ref_dt, o, g, ctx->stream);
+  CK(cudaGetLastError());
+  auto down = [&](void* dst, const void* src, size_t bytes) {
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+  };
+  CK(down(out.face_area, o.area, 8 * F));
+  CK(down(out.face_normal, o.normal, 24 * F));
+  CK(down(out.face_centroid, o.fcen, 24 * F));
+  CK(down(out.streaming_dt, o.sdt, 8 * F));
+  CK(down(out.cell_volume, o.vol, 8 * T));
+  CK(down(out.cell_centroid, o.ccen, 24 * T));
+  CK(down(out.stencil_offsets, o.st_off, 4 * (C + 1)));
+  CK(down(out.stencil_cells, o.st_cells, 4 * nnz));
+  CK(down(out.stencil_faces, o.st_faces, 4 * nnz));
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::memcpy(out.owner, pm.owner, 4 * F);
+  if (Fi) std::memcpy(out.neighbour, pm.neighbour, 4 * Fi);
+  for (size_t f = Fi; f < F; f++) out.neighbour[f] = (int32_t)(C + f - Fi);
+  return PLFBS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int plfbs_polymesh_geometry(const plfbs_polymesh_view* mesh, double visc, double gamma,
+                            double fneq_min, int32_t device, plfbs_mesh_arrays* out) {
+  if (!mesh || !out || !out->owner || !out->neighbour || !out->face_area || !out->face_normal ||
+      !out->face_centroid || !out->streaming_dt || !out->cell_volume || !out->cell_centroid ||
+      !out->stencil_offsets || !out->stencil_cells || !out->stencil_faces)
+    return set_err(nullptr, PLFBS_ERR_ARG, "null argument");
+  if (!std::isfinite(visc) || !(gamma > 0) || !std::isfinite(fneq_min))
+    return set_err(nullptr, PLFBS_ERR_ARG, "geometry needs finite visc, fneq_min and gamma > 0");
+  std::string err;
+  int rc = plfbs::validate_polymesh(*mesh, err);
+  if (rc) return set_err(nullptr, rc, err);
+  if ((rc = check_device(device))) return rc;
+  // calc_face_delta_t: the cap 3 nu / (gamma fneq_min) (none when fneq_min is 0)
+  const double ref_dt = fneq_min != 0 ? visc * 3 / gamma / fneq_min : HUGE_VAL;
+  plfbs_ctx tmp;
+  tmp.device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking) != cudaSuccess)
+    return set_err(nullptr, PLFBS_ERR_CUDA, "stream creation failed");
+  rc = polymesh_geometry(&tmp, *mesh, ref_dt, *out);
+  cudaStreamSynchronize(tmp.stream);  // the scratch frees are stream-ordered
+  cudaStreamDestroy(tmp.stream);
+  if (rc) g_err = tmp.err;
+  return rc;
+}
+
 int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plfbs_bc_view* bc,
                  const plfbs_ibm_view* ibm, int device, plfbs_ctx** out) {
   if (!cfg || !mesh || !bc || !out) return set_err(nullptr, PLFBS_ERR_ARG, "null argument");
@@ -258,18 +481,13 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   ctx->device = device;
   ctx->cfg = *cfg;
   std::string err;
-  int rc = plfbs::build_layout(*cfg, *mesh, *bc, ctx->L, err);
+  int rc = plfbs::prepare_layout(*cfg, *mesh, *bc, ctx->L, err);
   if (rc) {
     delete ctx;
     return set_err(nullptr, rc, err);
   }
-  ctx->fingerprint = mesh_fingerprint(*mesh);  // arrays validated by build_layout
   const Layout& L = ctx->L;
   const bool fp32 = cfg->precision == PLFBS_FP32_DEVIATION;
-  if (fp32 && L.K2 > 16) {
-    delete ctx;
-    return set_err(nullptr, PLFBS_ERR_MESH, "the FP32 form handles cells with at most 16 faces");
-  }
   const int N = (ibm && ibm->n_nodes > 0) ? ibm->n_nodes : 0;
   if (N > 0) {
     if (!ibm->x || !ibm->x_ref || ibm->object_nodes <= 0 || !(cfg->domain_dt > 0) ||
@@ -279,7 +497,7 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
                      "IBM needs node arrays, object_nodes > 0, domain_dt > 0 and lengths > 0");
     }
   }
-  // validation and layout need no GPU; the device is checked last
+  // validation needs no GPU; the device is checked before the layout is built
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) {
     delete ctx;
@@ -311,7 +529,6 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   a.F = L.F;
   a.B = L.B;
   a.K = L.K;
-  a.K2 = L.K2;
   a.quirk_b = L.quirk_b;
   a.N = N;
   a.nblk_update = (L.C + plfbs::kBlock - 1) / plfbs::kBlock;
@@ -342,32 +559,19 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   a.grad = p;
   if ((rc = dev_alloc(ctx, &p, (size_t)L.F * e4))) return fail(rc);
   a.flux = p;
-  if ((rc = dev_upload(ctx, &p, L.face_ids))) return fail(rc);
-  a.face_ids = static_cast<const int32_t*>(p);
-  plfbs::Layout32 L32;
+  if ((rc = build_device_layout(ctx, *mesh))) return fail(rc);
   if (fp32) {
-    plfbs::build_layout32(L, cfg->ref_rho, cfg->max_velocity, L32);
-    if ((rc = dev_upload(ctx, &p, L32.face0))) return fail(rc);
-    a.face0 = p;
-    if ((rc = dev_upload(ctx, &p, L32.face1))) return fail(rc);
-    a.face1 = p;
-    if ((rc = dev_upload(ctx, &p, L32.face2))) return fail(rc);
-    a.face2 = p;
-    if ((rc = dev_upload(ctx, &p, L32.bc0))) return fail(rc);
+    plfbs::BoundaryRecords32 b32;
+    plfbs::boundary_records32(L, cfg->ref_rho, cfg->max_velocity, b32);
+    if ((rc = dev_upload(ctx, &p, b32.bc0))) return fail(rc);
     a.bc0 = p;
-    if ((rc = dev_upload(ctx, &p, L32.bc1))) return fail(rc);
+    if ((rc = dev_upload(ctx, &p, b32.bc1))) return fail(rc);
     a.bc1 = p;
-    if ((rc = dev_upload(ctx, &p, L32.bc2))) return fail(rc);
+    if ((rc = dev_upload(ctx, &p, b32.bc2))) return fail(rc);
     a.bc2 = p;
-    if ((rc = dev_upload(ctx, &p, L32.bc3))) return fail(rc);
+    if ((rc = dev_upload(ctx, &p, b32.bc3))) return fail(rc);
     a.bc3 = p;
   } else {
-    if ((rc = dev_upload(ctx, &p, L.face0))) return fail(rc);
-    a.face0 = p;
-    if ((rc = dev_upload(ctx, &p, L.face1))) return fail(rc);
-    a.face1 = p;
-    if ((rc = dev_upload(ctx, &p, L.face2))) return fail(rc);
-    a.face2 = p;
     if ((rc = dev_upload(ctx, &p, L.bc0))) return fail(rc);
     a.bc0 = p;
     if ((rc = dev_upload(ctx, &p, L.bc1))) return fail(rc);
@@ -377,31 +581,6 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     if ((rc = dev_upload(ctx, &p, L.bc3))) return fail(rc);
     a.bc3 = p;
   }
-  if ((rc = dev_upload(ctx, &p, L.st_nbr))) return fail(rc);
-  a.st_nbr = static_cast<const int32_t*>(p);
-  if (fp32) {
-    if ((rc = dev_upload(ctx, &p, L32.st_wx))) return fail(rc);
-    a.st_wx = p;
-    if ((rc = dev_upload(ctx, &p, L32.st_wy))) return fail(rc);
-    a.st_wy = p;
-    if ((rc = dev_upload(ctx, &p, L32.st_wz))) return fail(rc);
-    a.st_wz = p;
-  } else {
-    if ((rc = dev_upload(ctx, &p, L.st_wx))) return fail(rc);
-    a.st_wx = p;
-    if ((rc = dev_upload(ctx, &p, L.st_wy))) return fail(rc);
-    a.st_wy = p;
-    if ((rc = dev_upload(ctx, &p, L.st_wz))) return fail(rc);
-    a.st_wz = p;
-  }
-  if ((rc = dev_upload(ctx, &p, L.gather))) return fail(rc);
-  a.gather = static_cast<const int32_t*>(p);
-  if (fp32) {
-    if ((rc = dev_upload(ctx, &p, L32.inv_volume))) return fail(rc);
-  } else {
-    if ((rc = dev_upload(ctx, &p, L.inv_volume))) return fail(rc);
-  }
-  a.inv_volume = p;
   if ((rc = dev_alloc(ctx, &p, (size_t)a.nblk_update * 4 * sizeof(double)))) return fail(rc);
   a.partial = static_cast<double*>(p);
   if ((rc = dev_alloc(ctx, &p, sizeof(DevStats)))) return fail(rc);
@@ -438,8 +617,6 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     a.node_vel = static_cast<double*>(p);
     if ((rc = dev_alloc(ctx, &p, 3 * (size_t)N * sizeof(double)))) return fail(rc);
     a.node_force = static_cast<double*>(p);
-    if ((rc = dev_upload(ctx, &p, L.cell_new_of_old))) return fail(rc);
-    a.ibm_map = static_cast<const int32_t*>(p);
     if ((rc = reset_force(ctx))) return fail(rc);
   }
   if ((rc = capture_step(ctx))) return fail(rc);
@@ -923,14 +1100,60 @@ int plfbs_get_face_flux(plfbs_ctx* ctx, double* flux, int32_t n_faces) {
   if (!flux || n_faces != L.F) return set_err(ctx, PLFBS_ERR_ARG, "face flux: need 4 n_faces");
   std::vector<double> g;
   TRY(download4(ctx, ctx->args.flux, (size_t)L.F, g, true));
+  std::vector<int32_t> order(L.F);
+  CK(cudaMemcpyAsync(order.data(), ctx->face_order, 4 * (size_t)L.F, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   if (ctx->cfg.precision == PLFBS_FP32_DEVIATION) {
-    // add back the constant rho0/3 n A the deviation form leaves out
+    // add back the constant rho0/3 n A the deviation form leaves out (from the
+    // FP32 face records: debug output, rounding of n A is ~6e-8 relative)
+    std::vector<float> f0(4 * (size_t)L.F);
+    CK(cudaMemcpyAsync(f0.data(), ctx->args.face0, f0.size() * sizeof(float),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     const double p3 = ctx->cfg.ref_rho / 3.0;
     for (int k = 0; k < L.F; k++)
-      for (int c = 0; c < 3; c++) g[4 * (size_t)k + c] += p3 * L.face0[4 * (size_t)k + c] * L.face0[4 * (size_t)k + 3];
+      for (int c = 0; c < 3; c++)
+        g[4 * (size_t)k + c] += p3 * (double)f0[4 * (size_t)k + c] * (double)f0[4 * (size_t)k + 3];
   }
-  for (int f = 0; f < L.F; f++)
-    std::memcpy(flux + 4 * (size_t)f, &g[4 * (size_t)L.face_new_of_old[f]], 4 * sizeof(double));
+  for (int k = 0; k < L.F; k++)
+    std::memcpy(flux + 4 * (size_t)order[k], &g[4 * (size_t)k], 4 * sizeof(double));
+  return PLFBS_OK;
+}
+
+int plfbs_get_layout(plfbs_ctx* ctx, int32_t* sizes, int32_t* cell_order, int32_t* face_order,
+                     int32_t* stencil_nbr, double* stencil_w, int32_t* gather) {
+  TRY(check_ctx(ctx));
+  const Layout& L = ctx->L;
+  const KernelArgs& a = ctx->args;
+  if (!sizes) return set_err(ctx, PLFBS_ERR_ARG, "layout: null sizes");
+  sizes[0] = L.K;
+  sizes[1] = L.K2;
+  const size_t C = L.C, KC = (size_t)L.K * C;
+  if (cell_order) std::memcpy(cell_order, L.cell_old_of_new.data(), 4 * C);
+  if (face_order)
+    CK(cudaMemcpyAsync(face_order, ctx->face_order, 4 * (size_t)L.F, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  if (stencil_nbr)
+    CK(cudaMemcpyAsync(stencil_nbr, a.st_nbr, 4 * KC, cudaMemcpyDeviceToHost, ctx->stream));
+  if (gather)
+    CK(cudaMemcpyAsync(gather, a.gather, 4 * (size_t)L.K2 * C, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  if (stencil_w) {
+    const void* w[3] = {a.st_wx, a.st_wy, a.st_wz};
+    for (int c = 0; c < 3; c++) {
+      double* out = stencil_w + c * KC;
+      if (ctx->cfg.precision == PLFBS_FP32_DEVIATION) {
+        std::vector<float> f(KC);
+        CK(cudaMemcpyAsync(f.data(), w[c], 4 * KC, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (size_t i = 0; i < KC; i++) out[i] = f[i];
+      } else {
+        CK(cudaMemcpyAsync(out, w[c], 8 * KC, cudaMemcpyDeviceToHost, ctx->stream));
+      }
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
   return PLFBS_OK;
 }
 

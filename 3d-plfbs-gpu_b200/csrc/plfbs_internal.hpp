@@ -22,6 +22,9 @@ namespace plfbs {
 // new order. The permutations map both ways so that every public entry point
 // reads and writes the caller's numbering.
 // ---------------------------------------------------------------------------
+// Host-side part of a context's layout: sizes, the permutations between the
+// caller's numbering and the device's, and the boundary records (built on
+// the host; the face, stencil and gather arrays are built on the device).
 struct Layout {
   int C = 0, F = 0, Fi = 0, B = 0;
   int K = 0;      // gradient-stencil slots per cell (max stencil size)
@@ -30,15 +33,6 @@ struct Layout {
 
   std::vector<int32_t> cell_new_of_old, cell_old_of_new;  // [C]
   std::vector<int32_t> bc_new_of_old, bc_old_of_new;      // [B]
-  std::vector<int32_t> face_new_of_old, face_old_of_new;  // [F]
-
-  // Face records, 3 x 4 doubles per face (structure of arrays):
-  //   face0 = (n.x, n.y, n.z, area)
-  //   face1 = (streaming dt, t1.x, t1.y, t1.z)   t1 = owner centroid - face centroid
-  //   face2 = (t2.x, t2.y, t2.z, tau)            t2 = neighbour centroid - face centroid,
-  //                                              tau = 3 nu / (dt_s gamma)
-  std::vector<double> face0, face1, face2;  // [4F] each
-  std::vector<int32_t> face_ids;            // [2F] new owner, new neighbour (or C + bc)
 
   // Boundary records, 4 x 4 doubles per boundary face (structure of arrays):
   //   bc0 = raw boundary value (u, v, w, rho)
@@ -46,32 +40,115 @@ struct Layout {
   //   bc2 = (d.x, d.y, d.z, |d|) unit owner->ghost direction and distance
   //   bc3 = (1-|n.x|, 1-|n.y|, 1-|n.z|, types) types = rho_type | vel_type << 8
   std::vector<double> bc0, bc1, bc2, bc3;  // [4B] each
-
-  // Gradient stencil in slot-major (ELL) layout: slot k of cell i at k*C + i.
-  // Neighbour -1 marks an empty slot. Weights are the precombined
-  // LHS^-1 . RHS_e (three arrays, x/y/z).
-  std::vector<int32_t> st_nbr;                 // [K*C]
-  std::vector<double> st_wx, st_wy, st_wz;     // [K*C]
-
-  // Face-to-cell gather, slot-major: (face << 1) | (cell is the neighbour), -1 empty.
-  std::vector<int32_t> gather;                 // [K2*C]
-  std::vector<double> inv_volume;              // [C]
-
-  // Cell centroids in the new numbering, kept for host-side diagnostics.
-  std::vector<double> centroid;                // [3(C+B)]
 };
 
-// FP32 copies of the layout for the deviation form (PLFBS_FP32_DEVIATION):
-// geometry and weights rounded once from the FP64 records (weights are built
-// in FP64 first), boundary values expressed as deviations (rho - rho0,
-// velocity / U), face ids moved to their own int2 array.
-struct Layout32 {
-  std::vector<float> face0, face1, face2;        // [4F] (n, A), (dt_s, t1), (t2, tau)
+// Device layout (layout.cu), per context:
+//   face0 = (n.x, n.y, n.z, area)                 [F] double4 (FP32 form: float4)
+//   face1 = (streaming dt, t1.x, t1.y, t1.z)      t1 = owner centroid - face centroid
+//   face2 = (t2.x, t2.y, t2.z, tau)               t2 = neighbour centroid - face centroid,
+//                                                 tau = 3 nu / (dt_s gamma)
+//   face_ids = (new owner, new neighbour or C + new bc)   [F] int2
+//   st_nbr, st_wx, st_wy, st_wz: gradient stencil, slot k of cell i at k*C + i,
+//     neighbour -1 in empty slots, weights the precombined LHS^-1 . RHS_e
+//   gather: (face << 1) | (cell is the neighbour), slot-major [K2*C], -1 empty
+//   inv_volume [C]
+// Faces: internal ones by (owner window of kFaceWindow new cells, upwind
+// signature, new owner, new neighbour, caller face), then boundary faces by
+// new boundary index. Within a window, faces of one signature take the same
+// branches in the flux kernel and the window keeps the cells they read
+// resident in L2 across the signature classes.
+constexpr int kFaceWindow = 4096;
+
+// The caller's mesh arrays copied to the device, plus the renumbering.
+struct DevMesh {
+  int C, F, Fi, B;
+  const int32_t* owner;      // [F]
+  const int32_t* neighbour;  // [F]
+  const double* area;        // [F]
+  const double* normal;      // [3F]
+  const double* fcen;        // [3F]
+  const double* sdt;         // [F]
+  const double* vol;         // [C]
+  const double* ccen;        // [3(C+B)]
+  const int32_t* st_off;     // [C+1]
+  const int32_t* st_cells;   // [nnz]
+  const int32_t* st_faces;   // [nnz]
+  const int32_t* cell_new;   // [C] caller cell -> new
+  const int32_t* bc_new;     // [B] caller boundary face -> new
+  const int32_t* bc_old;     // [B] new boundary face -> caller
+};
+
+// Device scratch of the layout build, zeroed before use except seg and sig.
+struct LayoutScratch {
+  int32_t* own_cnt;   // [C] internal faces per new owner
+  int32_t* own_off;   // [C] offset of an owner's faces within its window
+  int32_t* cursor;    // [C]
+  int32_t* deg;       // [C] faces per new cell
+  int32_t* gcnt;      // [C]
+  int32_t* wsum;      // [windows]
+  int32_t* wbase;     // [windows + 1]
+  int32_t* seg;       // [Fi] internal faces grouped by owner
+  uint16_t* sig;      // [Fi]
+  int32_t* info;      // [0] first cell with a singular LS matrix (C if none), [1] max faces per cell
+  unsigned long long* fingerprint;
+};
+
+// Internal face order (face_order[k] = caller face; boundary entries are
+// filled by launch_layout_records), the gather width and the fingerprint.
+void launch_layout_order(const DevMesh& m, const LayoutScratch& s, int32_t* face_order,
+                         cudaStream_t stream);
+// Face records, ids, stencil weights and inverse volumes.
+void launch_layout_records(const DevMesh& m, const LayoutScratch& s, int precision, int mode,
+                           double visc3, double pg, int32_t* face_order, int32_t* face_ids,
+                           void* face0, void* face1, void* face2, int32_t* st_nbr, void* st_wx,
+                           void* st_wy, void* st_wz, void* inv_volume, cudaStream_t stream);
+// The face-to-cell gather (pre-filled with -1).
+void launch_layout_gather(const DevMesh& m, const LayoutScratch& s, const int32_t* face_ids,
+                          int32_t* gather, cudaStream_t stream);
+
+// A polyMesh on the device: single-precision points, faces as vertex lists.
+struct DevPolyMesh {
+  int P, F, Fi, C;
+  const float* points;        // [3P]
+  const int32_t* face_offsets;  // [F+1]
+  const int32_t* face_points;   // [face_offsets[F]]
+  const int32_t* owner;       // [F]
+  const int32_t* neighbour;   // [Fi]
+};
+// Device outputs of the geometry build (plfbs_mesh_view's arrays; owner and
+// neighbour are the caller's).
+struct GeometryOut {
+  double* area;      // [F]
+  double* normal;    // [3F]
+  double* fcen;      // [3F]
+  double* sdt;       // [F]
+  double* vol;       // [C+B]
+  double* ccen;      // [3(C+B)]
+  int32_t* st_off;   // [C+1]
+  int32_t* st_cells; // [2Fi + B]
+  int32_t* st_faces; // [2Fi + B]
+};
+struct GeometryScratch {
+  double* fcsum;     // [3F] un-normalised face centroid sums
+  int32_t* cnt;      // [C] faces per cell (zeroed)
+  int32_t* cursor;   // [C] (zeroed)
+  int32_t* own_off;  // [C]
+  int32_t* wsum;     // [windows]
+  int32_t* wbase;    // [windows + 1]
+  int32_t* info;     // [2] (zeroed)
+};
+void launch_polymesh_geometry(const DevPolyMesh& pm, double ref_dt, const GeometryOut& o,
+                              const GeometryScratch& s, cudaStream_t stream);
+// Host checks of a polyMesh's indices (setup.cpp).
+int validate_polymesh(const plfbs_polymesh_view& pm, std::string& err);
+
+// FP32 boundary records for the deviation form (PLFBS_FP32_DEVIATION):
+// rounded once from the FP64 records, values as deviations (rho - rho0,
+// velocity / U).
+struct BoundaryRecords32 {
   std::vector<float> bc0, bc1, bc2, bc3;         // [4B]
-  std::vector<float> st_wx, st_wy, st_wz;        // [K*C]
-  std::vector<float> inv_volume;                 // [C]
 };
-void build_layout32(const Layout& L, double rho0, double uref, Layout32& L32);
+void boundary_records32(const Layout& L, double rho0, double uref, BoundaryRecords32& o);
 
 // Least-squares weights exactly as gradients::pre_fill_LHS_and_RHS_matrix
 // (gradients.cpp:214-313): lhs_inv [9C], rhs [3 nnz], caller numbering.
@@ -81,9 +158,10 @@ int ls_weights(const plfbs_mesh_view& m, int mode, double* lhs_inv, double* rhs,
 // The error string plfbs_last_error(NULL) returns (capi.cpp).
 void set_global_error(const std::string& m);
 
-// Validate the views and build the device layout.
-int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bc,
-                 Layout& L, std::string& err);
+// Validate the views, renumber the cells, order the boundary faces and build
+// their records (setup.cpp).
+int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bc,
+                   Layout& L, std::string& err);
 
 // ---------------------------------------------------------------------------
 // Device side

@@ -1,6 +1,6 @@
-// Host-side preparation of a case for the device: validation, least-squares
-// weights, locality renumbering and the packed face / boundary / stencil /
-// gather records the kernels read.
+// Host-side preparation of a case for the device: validation, locality
+// renumbering, boundary order and records, and the host-only least-squares
+// weights export. The O(faces) layout is built on the device (layout.cu).
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -23,7 +23,10 @@ std::string msg(const char* what, long long i, long long v) {
 
 inline bool finite(double x) { return std::isfinite(x); }
 
-// Reverse Cuthill-McKee over the interior-cell graph of the internal faces.
+// Reverse Cuthill-McKee over the interior-cell graph of the internal faces:
+// start cells by ascending degree (stable), breadth-first, the unvisited
+// neighbours of each cell appended by ascending degree (stable, in face
+// order), the whole order reversed.
 std::vector<int32_t> rcm_order(int C, int Fi, const int32_t* owner, const int32_t* nb) {
   std::vector<int32_t> deg(C, 0);
   for (int f = 0; f < Fi; f++) {
@@ -31,47 +34,54 @@ std::vector<int32_t> rcm_order(int C, int Fi, const int32_t* owner, const int32_
     deg[nb[f]]++;
   }
   std::vector<int64_t> off(C + 1, 0);
-  for (int i = 0; i < C; i++) off[i + 1] = off[i] + deg[i];
-  std::vector<int32_t> adj(off[C]);
-  std::vector<int64_t> pos(off.begin(), off.end() - 1);
-  for (int f = 0; f < Fi; f++) {
-    adj[pos[owner[f]]++] = nb[f];
-    adj[pos[nb[f]]++] = owner[f];
+  int dmax = 0;
+  for (int i = 0; i < C; i++) {
+    off[i + 1] = off[i] + deg[i];
+    dmax = std::max(dmax, deg[i]);
   }
-  std::vector<int32_t> by_degree(C);
-  std::iota(by_degree.begin(), by_degree.end(), 0);
-  std::stable_sort(by_degree.begin(), by_degree.end(),
-                   [&](int a, int b) { return deg[a] < deg[b]; });
+  std::vector<int32_t> adj(off[C]);
+  {
+    std::vector<int64_t> pos(off.begin(), off.end() - 1);
+    for (int f = 0; f < Fi; f++) {
+      adj[pos[owner[f]]++] = nb[f];
+      adj[pos[nb[f]]++] = owner[f];
+    }
+  }
+  // counting sort of the cells by degree (stable)
+  std::vector<int32_t> dstart(dmax + 2, 0), by_degree(C);
+  for (int i = 0; i < C; i++) dstart[deg[i] + 1]++;
+  for (int d = 0; d <= dmax; d++) dstart[d + 1] += dstart[d];
+  for (int i = 0; i < C; i++) by_degree[dstart[deg[i]]++] = i;
   std::vector<char> seen(C, 0);
   std::vector<int32_t> order;
   order.reserve(C);
-  std::vector<int32_t> nbrs;
+  size_t head = 0;
   for (int s : by_degree) {
     if (seen[s]) continue;
-    std::queue<int32_t> q;
-    q.push(s);
     seen[s] = 1;
-    while (!q.empty()) {
-      int v = q.front();
-      q.pop();
-      order.push_back(v);
-      nbrs.assign(adj.begin() + off[v], adj.begin() + off[v + 1]);
-      std::stable_sort(nbrs.begin(), nbrs.end(), [&](int a, int b) { return deg[a] < deg[b]; });
-      for (int w : nbrs)
-        if (!seen[w]) {
-          seen[w] = 1;
-          q.push(w);
+    order.push_back(s);
+    while (head < order.size()) {
+      const int v = order[head++];
+      const size_t first = order.size();
+      for (int64_t e = off[v]; e < off[v + 1]; e++) {
+        const int w = adj[e];
+        if (seen[w]) continue;
+        seen[w] = 1;
+        // insert by degree after equal degrees (stable insertion sort)
+        order.push_back(w);
+        size_t j = order.size() - 1;
+        while (j > first && deg[order[j - 1]] > deg[w]) {
+          order[j] = order[j - 1];
+          j--;
         }
+        order[j] = w;
+      }
     }
   }
   std::reverse(order.begin(), order.end());
   return order;  // order[new] = old
 }
 
-// For each of the 7 opposite lattice pairs of D3Q15 (first members e = x, y,
-// z, (1,1,1), (1,1,-1), (1,-1,1), (-1,1,1)) the branch the flux kernel takes:
-// 1 if e.n > 0.001 dt, 2 if e.n < -0.001 dt, 0 in the dead band
-// (LBFS.cu:353-354); packed base 3.
 // body(i) for i in [0, n) on up to 16 host threads in contiguous chunks (the
 // per-cell and per-face loops of the layout are independent); serial for
 // small n or when no thread can be started.
@@ -98,18 +108,6 @@ void parallel_for(int n, const Body& body, int serial_below = 32768) {
   }
   for (int i = lo; i < n; i++) body(i);
   for (auto& t : th) t.join();
-}
-
-int upwind_signature(const double* n, double dt) {
-  static const int E[7][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 1},
-                              {1, 1, -1}, {1, -1, 1}, {-1, 1, 1}};
-  const double d1 = 0.001 * dt;
-  int sig = 0, p3 = 1;
-  for (int p = 0; p < 7; p++, p3 *= 3) {
-    const double s = E[p][0] * n[0] + E[p][1] * n[1] + E[p][2] * n[2];
-    sig += p3 * (s > d1 ? 1 : (s < -d1 ? 2 : 0));
-  }
-  return sig;
 }
 
 }  // namespace
@@ -196,8 +194,66 @@ int ls_weights(const plfbs_mesh_view& m, int mode, double* lhs_inv, double* rhs,
   return PLFBS_OK;
 }
 
-int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bcv,
-                 Layout& L, std::string& err) {
+// The first index in [0, n) for which bad(i) holds, or n; bad() runs on up
+// to 16 host threads.
+template <typename Bad>
+int first_bad(int n, const Bad& bad) {
+  std::atomic<int> first(n);
+  parallel_for(n, [&](int i) {
+    if (!bad(i)) return;
+    int cur = first.load();
+    while (i < cur && !first.compare_exchange_weak(cur, i)) {
+    }
+  });
+  return first.load();
+}
+
+int validate_polymesh(const plfbs_polymesh_view& pm, std::string& err) {
+  const int P = pm.n_points, F = pm.n_faces, Fi = pm.n_internal, C = pm.n_cells;
+  if (P <= 0 || C <= 0 || F <= 0 || Fi < 0 || Fi > F) {
+    err = "polyMesh sizes must satisfy n_points, n_cells, n_faces > 0, 0 <= n_internal <= n_faces";
+    return PLFBS_ERR_ARG;
+  }
+  if (!pm.points || !pm.face_offsets || !pm.face_points || !pm.owner || (Fi > 0 && !pm.neighbour)) {
+    err = "null polyMesh array";
+    return PLFBS_ERR_ARG;
+  }
+  if ((long long)F * 2 >= (1LL << 31)) {
+    err = "too many faces";
+    return PLFBS_ERR_MESH;
+  }
+  if (pm.face_offsets[0] != 0) {
+    err = "face_offsets[0] must be 0";
+    return PLFBS_ERR_MESH;
+  }
+  const int bn = first_bad(F, [&](int f) { return pm.face_offsets[f + 1] - pm.face_offsets[f] < 3; });
+  if (bn < F) {
+    err = msg("face with fewer than 3 vertices (or decreasing offsets)", bn,
+              pm.face_offsets[bn + 1] - pm.face_offsets[bn]);
+    return PLFBS_ERR_MESH;
+  }
+  const int bp = first_bad(F, [&](int f) {
+    for (int k = pm.face_offsets[f]; k < pm.face_offsets[f + 1]; k++)
+      if (pm.face_points[k] < 0 || pm.face_points[k] >= P) return true;
+    return false;
+  });
+  if (bp < F) {
+    err = msg("face vertex out of range", bp, 0);
+    return PLFBS_ERR_MESH;
+  }
+  const int bo = first_bad(F, [&](int f) {
+    if (pm.owner[f] < 0 || pm.owner[f] >= C) return true;
+    return f < Fi && (pm.neighbour[f] < 0 || pm.neighbour[f] >= C || pm.neighbour[f] == pm.owner[f]);
+  });
+  if (bo < F) {
+    err = msg("face owner or neighbour out of range", bo, pm.owner[bo]);
+    return PLFBS_ERR_MESH;
+  }
+  return PLFBS_OK;
+}
+
+int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bcv,
+                   Layout& L, std::string& err) {
   const int C = m.n_cells, F = m.n_faces, Fi = m.n_internal;
   if (C <= 0 || F <= 0 || Fi < 0 || Fi > F) {
     err = "mesh sizes must satisfy n_cells > 0, n_faces > 0, 0 <= n_internal <= n_faces";
@@ -214,68 +270,85 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
     err = "null boundary array";
     return PLFBS_ERR_ARG;
   }
+  if ((long long)F * 2 >= (1LL << 31)) {
+    err = "too many faces for the 31-bit gather encoding";
+    return PLFBS_ERR_MESH;
+  }
   L.C = C;
   L.F = F;
   L.Fi = Fi;
   L.B = B;
   const long long T = (long long)C + B;
-  // --- mesh consistency ---------------------------------------------------
-  for (int f = 0; f < F; f++) {
-    if (m.owner[f] < 0 || m.owner[f] >= C) {
-      err = msg("face owner out of range", f, m.owner[f]);
-      return PLFBS_ERR_MESH;
-    }
+  // --- mesh consistency (first failing index in loop order) ----------------
+  auto face_problem = [&](int f) -> int {
+    if (m.owner[f] < 0 || m.owner[f] >= C) return 1;
     if (f < Fi) {
-      if (m.neighbour[f] < 0 || m.neighbour[f] >= C || m.neighbour[f] == m.owner[f]) {
-        err = msg("internal face neighbour out of range", f, m.neighbour[f]);
-        return PLFBS_ERR_MESH;
-      }
+      if (m.neighbour[f] < 0 || m.neighbour[f] >= C || m.neighbour[f] == m.owner[f]) return 2;
     } else if (m.neighbour[f] != C + (f - Fi)) {
-      err = msg("boundary face neighbour must be n_cells + face - n_internal", f, m.neighbour[f]);
-      return PLFBS_ERR_MESH;
+      return 3;
     }
     if (!(m.face_area[f] > 0) || !finite(m.face_area[f]) || !(m.streaming_dt[f] > 0) ||
         !finite(m.face_normal[3 * (size_t)f]) || !finite(m.face_normal[3 * (size_t)f + 1]) ||
-        !finite(m.face_normal[3 * (size_t)f + 2])) {
-      err = msg("face area, streaming dt or normal not positive/finite", f, 0);
-      return PLFBS_ERR_MESH;
-    }
+        !finite(m.face_normal[3 * (size_t)f + 2]))
+      return 4;
+    return 0;
+  };
+  const int bf = first_bad(F, [&](int f) { return face_problem(f) != 0; });
+  if (bf < F) {
+    static const char* what[5] = {"", "face owner out of range",
+                                  "internal face neighbour out of range",
+                                  "boundary face neighbour must be n_cells + face - n_internal",
+                                  "face area, streaming dt or normal not positive/finite"};
+    const int code = face_problem(bf);
+    err = msg(what[code], bf, code == 1 ? m.owner[bf] : code == 4 ? 0 : m.neighbour[bf]);
+    return PLFBS_ERR_MESH;
   }
-  for (int i = 0; i < C; i++)
-    if (!(m.cell_volume[i] > 0) || !finite(m.cell_volume[i])) {
-      err = msg("cell volume not positive", i, 0);
-      return PLFBS_ERR_MESH;
-    }
+  const int bv = first_bad(C, [&](int i) { return !(m.cell_volume[i] > 0) || !finite(m.cell_volume[i]); });
+  if (bv < C) {
+    err = msg("cell volume not positive", bv, 0);
+    return PLFBS_ERR_MESH;
+  }
   if (m.stencil_offsets[0] != 0) {
     err = "stencil_offsets[0] must be 0";
     return PLFBS_ERR_MESH;
   }
-  int K = 0;
-  for (int i = 0; i < C; i++) {
-    const int e0 = m.stencil_offsets[i], e1 = m.stencil_offsets[i + 1];
-    if (e1 < e0) {
-      err = msg("stencil offsets decrease", i, e1);
-      return PLFBS_ERR_MESH;
-    }
-    K = std::max(K, e1 - e0);
-    for (int e = e0; e < e1; e++) {
-      const int j = m.stencil_cells[e], f = m.stencil_faces[e];
-      if (j < 0 || j >= T || f < 0 || f >= F) {
-        err = msg("stencil entry out of range", e, j);
-        return PLFBS_ERR_MESH;
-      }
-      const bool ok = (m.owner[f] == i && m.neighbour[f] == j) ||
-                      (f < Fi && m.neighbour[f] == i && m.owner[f] == j);
-      if (!ok) {
-        err = msg("stencil entry is not a face neighbour", e, j);
+  const int bo = first_bad(C, [&](int i) { return m.stencil_offsets[i + 1] < m.stencil_offsets[i]; });
+  if (bo < C) {
+    err = msg("stencil offsets decrease", bo, m.stencil_offsets[bo + 1]);
+    return PLFBS_ERR_MESH;
+  }
+  // first bad stencil entry of each cell (entries of cell i lie in
+  // [offsets[i], offsets[i+1]), so the first failing cell holds the first
+  // failing entry)
+  auto entry_problem = [&](int e, int i) -> int {
+    const int j = m.stencil_cells[e], f = m.stencil_faces[e];
+    if (j < 0 || j >= T || f < 0 || f >= F) return 1;
+    const bool ok = (m.owner[f] == i && m.neighbour[f] == j) ||
+                    (f < Fi && m.neighbour[f] == i && m.owner[f] == j);
+    return ok ? 0 : 2;
+  };
+  const int bs = first_bad(C, [&](int i) {
+    for (int e = m.stencil_offsets[i]; e < m.stencil_offsets[i + 1]; e++)
+      if (entry_problem(e, i)) return true;
+    return false;
+  });
+  if (bs < C) {
+    for (int e = m.stencil_offsets[bs]; e < m.stencil_offsets[bs + 1]; e++) {
+      const int code = entry_problem(e, bs);
+      if (code) {
+        err = msg(code == 1 ? "stencil entry out of range" : "stencil entry is not a face neighbour",
+                  e, m.stencil_cells[e]);
         return PLFBS_ERR_MESH;
       }
     }
   }
+  int K = 0;
+  for (int i = 0; i < C; i++) K = std::max(K, m.stencil_offsets[i + 1] - m.stencil_offsets[i]);
   if (K == 0) {
     err = "empty gradient stencil";
     return PLFBS_ERR_MESH;
   }
+  L.K = K;
   for (int b = 0; b < B; b++) {
     const int rt = bcv.rho_type[b], vt = bcv.vel_type[b];
     if (rt != 1 && rt != 2) {
@@ -295,12 +368,6 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
       }
   }
 
-  // --- least-squares weights (caller numbering) ------------------------------
-  const int nnz = m.stencil_offsets[C];
-  std::vector<double> lhs(9 * (size_t)C), rhs(3 * (size_t)nnz);
-  int rc = ls_weights(m, cfg.gradient_mode, lhs.data(), rhs.data(), err);
-  if (rc) return rc;
-
   // --- renumbering ---------------------------------------------------------
   L.cell_old_of_new.resize(C);
   L.cell_new_of_old.resize(C);
@@ -310,110 +377,21 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
     std::iota(L.cell_old_of_new.begin(), L.cell_old_of_new.end(), 0);
   }
   for (int i = 0; i < C; i++) L.cell_new_of_old[L.cell_old_of_new[i]] = i;
-  auto newc = [&](int old) { return L.cell_new_of_old[old]; };
 
-  // Internal faces by (owner window, upwind signature, new owner, new
-  // neighbour): within each window of kFaceWindow owners, faces with the same
-  // signature take the same branches in the flux kernel (and on structured
-  // meshes form a stream of owner/neighbour pairs at a fixed offset), while
-  // the window keeps the cells they read resident in L2 across the classes.
-  // Boundary faces by new owner.
-  std::vector<int32_t> fint(Fi), fbnd(B);
-  std::iota(fint.begin(), fint.end(), 0);
+  // Boundary faces by new owner (stable). The internal faces are ordered on
+  // the device (layout.cu).
+  std::vector<int32_t> fbnd(B);
   std::iota(fbnd.begin(), fbnd.end(), Fi);
-  constexpr int kFaceWindow = 4096;
-  // one 64-bit key per face: window (high bits), signature (< 3^7, 12 bits),
-  // owner within the window (12 bits); then the new neighbour and the face.
-  struct FaceKey {
-    uint64_t key;
-    int32_t nb, f;
-  };
-  std::vector<FaceKey> keys(Fi);
-  parallel_for(Fi, [&](int f) {
-    const uint64_t o = (uint64_t)newc(m.owner[f]);
-    const uint64_t sig =
-        (uint64_t)upwind_signature(m.face_normal + 3 * (size_t)f, m.streaming_dt[f]);
-    keys[f] = FaceKey{((o / kFaceWindow) << 24) | (sig << 12) | (o % kFaceWindow),
-                      newc(m.neighbour[f]), f};
+  std::stable_sort(fbnd.begin(), fbnd.end(), [&](int a, int b) {
+    return L.cell_new_of_old[m.owner[a]] < L.cell_new_of_old[m.owner[b]];
   });
-  // the window is the leading key: bucket by window, then sort the windows
-  // side by side
-  const int nwin = (C + kFaceWindow - 1) / kFaceWindow;
-  std::vector<int> woff(nwin + 1, 0);
-  for (const FaceKey& k : keys) woff[(k.key >> 24) + 1]++;
-  for (int w = 0; w < nwin; w++) woff[w + 1] += woff[w];
-  std::vector<FaceKey> sorted(Fi);
-  {
-    std::vector<int> pos(woff.begin(), woff.end() - 1);
-    for (const FaceKey& k : keys) sorted[pos[k.key >> 24]++] = k;
-  }
-  parallel_for(
-      nwin,
-      [&](int w) {
-        std::sort(sorted.begin() + woff[w], sorted.begin() + woff[w + 1],
-                  [](const FaceKey& a, const FaceKey& b) {
-                    if (a.key != b.key) return a.key < b.key;
-                    if (a.nb != b.nb) return a.nb < b.nb;
-                    return a.f < b.f;
-                  });
-      },
-      2);
-  for (int k = 0; k < Fi; k++) fint[k] = sorted[k].f;
-  std::stable_sort(fbnd.begin(), fbnd.end(),
-                   [&](int a, int b) { return newc(m.owner[a]) < newc(m.owner[b]); });
-  L.face_old_of_new.resize(F);
-  L.face_new_of_old.resize(F);
-  for (int k = 0; k < Fi; k++) L.face_old_of_new[k] = fint[k];
-  for (int k = 0; k < B; k++) L.face_old_of_new[Fi + k] = fbnd[k];
-  for (int k = 0; k < F; k++) L.face_new_of_old[L.face_old_of_new[k]] = k;
   L.bc_old_of_new.resize(B);
   L.bc_new_of_old.resize(B);
   for (int b = 0; b < B; b++) {
     L.bc_old_of_new[b] = fbnd[b] - Fi;
     L.bc_new_of_old[fbnd[b] - Fi] = b;
   }
-  // any old cell index (interior or ghost) -> new
-  auto newcell = [&](int old) { return old < C ? L.cell_new_of_old[old] : C + L.bc_new_of_old[old - C]; };
   L.quirk_b = B > 0 ? L.bc_new_of_old[0] : -1;
-
-  L.centroid.resize(3 * (size_t)T);
-  for (long long o = 0; o < T; o++) {
-    const long long n = newcell((int)o);
-    for (int c = 0; c < 3; c++) L.centroid[3 * n + c] = m.cell_centroid[3 * o + c];
-  }
-
-  // --- face records ----------------------------------------------------------
-  L.face0.assign(4 * (size_t)F, 0.0);
-  L.face1.assign(4 * (size_t)F, 0.0);
-  L.face2.assign(4 * (size_t)F, 0.0);
-  L.face_ids.assign(2 * (size_t)F, 0);
-  const double visc3 = cfg.visc * 3, pg = 1.0 / cfg.gamma;
-  parallel_for(F, [&](int k) {
-    const int f = L.face_old_of_new[k];
-    const int o = m.owner[f], nbo = m.neighbour[f];
-    const double* n = m.face_normal + 3 * (size_t)f;
-    const double* xf = m.face_centroid + 3 * (size_t)f;
-    const double* c1 = m.cell_centroid + 3 * (size_t)o;
-    const double* c2 = m.cell_centroid + 3 * (size_t)nbo;
-    double* a = &L.face0[4 * (size_t)k];
-    a[0] = n[0];
-    a[1] = n[1];
-    a[2] = n[2];
-    a[3] = m.face_area[f];
-    double* b = &L.face1[4 * (size_t)k];
-    b[0] = m.streaming_dt[f];
-    b[1] = c1[0] - xf[0];  // cell_1 - interface_node, LBFS.cu:343
-    b[2] = c1[1] - xf[1];
-    b[3] = c1[2] - xf[2];
-    double* c = &L.face2[4 * (size_t)k];
-    c[0] = c2[0] - xf[0];  // cell_2 - interface_node, LBFS.cu:344
-    c[1] = c2[1] - xf[1];
-    c[2] = c2[2] - xf[2];
-    // relaxation factor 3 nu / (dt_s gamma) (calculate_flux_at_interface, LBFS.cu:1042-1223)
-    c[3] = visc3 / m.streaming_dt[f] * pg;
-    L.face_ids[2 * (size_t)k] = newc(o);
-    L.face_ids[2 * (size_t)k + 1] = newcell(nbo);
-  });
 
   // --- boundary records --------------------------------------------------------
   L.bc0.assign(4 * (size_t)B, 0.0);
@@ -452,54 +430,6 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
       return PLFBS_ERR_MESH;
     }
   }
-
-  // --- gradient stencil (ELL, precombined weights) ---------------------------
-  L.K = K;
-  L.st_nbr.assign((size_t)K * C, -1);
-  L.st_wx.assign((size_t)K * C, 0.0);
-  L.st_wy.assign((size_t)K * C, 0.0);
-  L.st_wz.assign((size_t)K * C, 0.0);
-  parallel_for(C, [&](int io) {
-    const int in = newc(io);
-    const double* Li = &lhs[9 * (size_t)io];
-    int slot = 0;
-    for (int e = m.stencil_offsets[io]; e < m.stencil_offsets[io + 1]; e++, slot++) {
-      const double* r = &rhs[3 * (size_t)e];
-      const size_t s = (size_t)slot * C + in;
-      L.st_nbr[s] = newcell(m.stencil_cells[e]);
-      L.st_wx[s] = Li[0] * r[0] + Li[1] * r[1] + Li[2] * r[2];
-      L.st_wy[s] = Li[3] * r[0] + Li[4] * r[1] + Li[5] * r[2];
-      L.st_wz[s] = Li[6] * r[0] + Li[7] * r[1] + Li[8] * r[2];
-    }
-  });
-
-  // --- face -> cell gather ------------------------------------------------------
-  std::vector<int32_t> nf(C, 0);
-  for (int k = 0; k < F; k++) {
-    const int f = L.face_old_of_new[k];
-    nf[newc(m.owner[f])]++;
-    if (f < Fi) nf[newc(m.neighbour[f])]++;
-  }
-  int K2 = 0;
-  for (int i = 0; i < C; i++) K2 = std::max(K2, nf[i]);
-  L.K2 = K2;
-  L.gather.assign((size_t)K2 * C, -1);
-  std::fill(nf.begin(), nf.end(), 0);
-  for (int k = 0; k < F; k++) {
-    const int f = L.face_old_of_new[k];
-    const int o = newc(m.owner[f]);
-    L.gather[(size_t)(nf[o]++) * C + o] = (k << 1);
-    if (f < Fi) {
-      const int nn = newc(m.neighbour[f]);
-      L.gather[(size_t)(nf[nn]++) * C + nn] = (k << 1) | 1;
-    }
-  }
-  if ((long long)F * 2 >= (1LL << 31)) {
-    err = "too many faces for the 31-bit gather encoding";
-    return PLFBS_ERR_MESH;
-  }
-  L.inv_volume.resize(C);
-  for (int io = 0; io < C; io++) L.inv_volume[newc(io)] = 1.0 / m.cell_volume[io];
   return PLFBS_OK;
 }
 
@@ -507,16 +437,13 @@ int build_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
 
 namespace plfbs {
 
-void build_layout32(const Layout& L, double rho0, double uref, Layout32& o) {
-  const size_t F = L.F, B = L.B;
+void boundary_records32(const Layout& L, double rho0, double uref, BoundaryRecords32& o) {
+  const size_t B = L.B;
   auto cast = [](const std::vector<double>& v) {
     std::vector<float> r(v.size());
     for (size_t i = 0; i < v.size(); i++) r[i] = (float)v[i];
     return r;
   };
-  o.face0 = cast(L.face0);
-  o.face1 = cast(L.face1);
-  o.face2 = cast(L.face2);  // (t2, relaxation factor)
   // boundary values as deviations: velocity / U, rho - rho0
   auto dev = [&](const std::vector<double>& v) {
     std::vector<float> r(v.size());
@@ -530,10 +457,6 @@ void build_layout32(const Layout& L, double rho0, double uref, Layout32& o) {
   o.bc1 = dev(L.bc1);
   o.bc2 = cast(L.bc2);
   o.bc3 = cast(L.bc3);  // the type code (< 2^24) is exact in float
-  o.st_wx = cast(L.st_wx);
-  o.st_wy = cast(L.st_wy);
-  o.st_wz = cast(L.st_wz);
-  o.inv_volume = cast(L.inv_volume);
 }
 
 }  // namespace plfbs

@@ -23,6 +23,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr"]
+# layout.cu evaluates the host's least-squares formulas bit for bit: no FMA contraction
+FILE_FLAGS = {"layout.cu": ["-fmad=false"]}
 
 
 def sources():
@@ -49,7 +51,8 @@ def build(force=False, verbose=False, ptxas_info=False):
     objs = []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
-        cmd = [NVCC, *ARCH, *FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj]
+        cmd = [NVCC, *ARCH, *FLAGS, *FILE_FLAGS.get(os.path.basename(src), []), "-I", INCLUDE,
+               "-I", CSRC, "-c", src, "-o", obj]
         if ptxas_info and src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"]
         if verbose:

@@ -30,12 +30,25 @@ EXPORTS = ("plfbs_create", "plfbs_set_state", "plfbs_run", "plfbs_get_state",
            "plfbs_last_error", "plfbs_destroy", "plfbs_version",
            "plfbs_residual_norms_noalloc", "plfbs_release_cached", "plfbs_warm_start",
            "plfbs_checkpoint_bytes", "plfbs_save_checkpoint", "plfbs_load_checkpoint",
-           "plfbs_wall_forces")
+           "plfbs_wall_forces", "plfbs_get_layout", "plfbs_polymesh_geometry")
 
 
 class MeshView(C.Structure):
     _fields_ = [("n_cells", C.c_int32), ("n_faces", C.c_int32), ("n_internal", C.c_int32),
                 ("owner", _ip), ("neighbour", _ip), ("face_area", _dp), ("face_normal", _dp),
+                ("face_centroid", _dp), ("streaming_dt", _dp), ("cell_volume", _dp),
+                ("cell_centroid", _dp), ("stencil_offsets", _ip), ("stencil_cells", _ip),
+                ("stencil_faces", _ip)]
+
+
+class PolyMeshView(C.Structure):
+    _fields_ = [("n_points", C.c_int32), ("n_faces", C.c_int32), ("n_internal", C.c_int32),
+                ("n_cells", C.c_int32), ("points", C.POINTER(C.c_float)),
+                ("face_offsets", _ip), ("face_points", _ip), ("owner", _ip), ("neighbour", _ip)]
+
+
+class MeshOut(C.Structure):
+    _fields_ = [("owner", _ip), ("neighbour", _ip), ("face_area", _dp), ("face_normal", _dp),
                 ("face_centroid", _dp), ("streaming_dt", _dp), ("cell_volume", _dp),
                 ("cell_centroid", _dp), ("stencil_offsets", _ip), ("stencil_cells", _ip),
                 ("stencil_faces", _ip)]
@@ -99,6 +112,9 @@ def lib():
         L.plfbs_warm_start.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_int64, _dp, C.c_int32]
         L.plfbs_checkpoint_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
         L.plfbs_wall_forces.argtypes = [C.c_void_p, _ip, C.c_int32, _dp, _dp]
+        L.plfbs_get_layout.argtypes = [C.c_void_p, _ip, _ip, _ip, _ip, _dp, _ip]
+        L.plfbs_polymesh_geometry.argtypes = [C.POINTER(PolyMeshView), C.c_double, C.c_double,
+                                              C.c_double, C.c_int32, C.POINTER(MeshOut)]
         L.plfbs_save_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
         L.plfbs_load_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
         L.plfbs_release_cached.restype = C.c_int
@@ -155,6 +171,40 @@ def ls_weights(ma, mode):
     if rc:
         raise PlfbsError(rc, lib().plfbs_last_error(None).decode())
     return lhs, rhs
+
+
+def polymesh_geometry(pm, visc, gamma, fneq_min, device=0):
+    """The solver's mesh arrays (a cases.MeshArrays) of a cases.PolyMesh,
+    computed on the GPU by plfbs_polymesh_geometry."""
+    from . import cases
+    F, Fi, Cn = pm.n_faces, pm.n_internal, pm.n_cells
+    B = F - Fi
+    nv = np.asarray(pm.nverts, np.int32)
+    offsets = np.zeros(F + 1, np.int32)
+    np.cumsum(nv, out=offsets[1:])
+    faces = np.asarray(pm.faces)
+    fp = np.ascontiguousarray(faces[np.arange(faces.shape[1])[None, :] < nv[:, None]], np.int32)
+    pts = np.ascontiguousarray(pm.points, np.float32)
+    owner = np.ascontiguousarray(pm.owner, np.int32)
+    nb = np.ascontiguousarray(pm.neighbour, np.int32)
+    v = PolyMeshView()
+    v.n_points, v.n_faces, v.n_internal, v.n_cells = pts.shape[0], F, Fi, Cn
+    v.points = pts.ctypes.data_as(C.POINTER(C.c_float))
+    v.face_offsets, v.face_points, v.owner, v.neighbour = _i(offsets), _i(fp), _i(owner), _i(nb)
+    T, nnz = Cn + B, 2 * Fi + B
+    a = dict(owner=np.zeros(F, np.int32), neighbour=np.zeros(F, np.int32),
+             face_area=np.zeros(F), face_normal=np.zeros((F, 3)), face_centroid=np.zeros((F, 3)),
+             streaming_dt=np.zeros(F), cell_volume=np.zeros(T), cell_centroid=np.zeros((T, 3)),
+             stencil_offsets=np.zeros(Cn + 1, np.int32), stencil_cells=np.zeros(nnz, np.int32),
+             stencil_faces=np.zeros(nnz, np.int32))
+    o = MeshOut()
+    for k, arr in a.items():
+        setattr(o, k, _i(arr) if arr.dtype == np.int32 else _d(arr))
+    rc = lib().plfbs_polymesh_geometry(C.byref(v), float(visc), float(gamma), float(fneq_min),
+                                       int(device), C.byref(o))
+    if rc:
+        raise PlfbsError(rc, lib().plfbs_last_error(None).decode())
+    return cases.MeshArrays(n_cells=Cn, n_faces=F, n_internal=Fi, bc_types=pm.bc_types(), **a)
 
 
 class Solver:
@@ -285,6 +335,20 @@ class Solver:
             nx = np.ascontiguousarray(node_x, np.float64).reshape(self.N, 3)
         self._check(lib().plfbs_warm_start(self.h, *[_d(c) for c in cols], self.T,
                                            _d(nx) if nx is not None else None, self.N))
+
+    def layout(self):
+        """The device-built layout (device numbering): dict of cell_order [C],
+        face_order [F], stencil_nbr [K, C], stencil_w [3, K, C], gather [K2, C]."""
+        sz = np.zeros(2, np.int32)
+        self._check(lib().plfbs_get_layout(self.h, _i(sz), None, None, None, None, None))
+        K, K2 = int(sz[0]), int(sz[1])
+        out = dict(cell_order=np.zeros(self.C, np.int32), face_order=np.zeros(self.F, np.int32),
+                   stencil_nbr=np.zeros((K, self.C), np.int32),
+                   stencil_w=np.zeros((3, K, self.C)), gather=np.zeros((K2, self.C), np.int32))
+        self._check(lib().plfbs_get_layout(self.h, _i(sz), _i(out["cell_order"]),
+                                           _i(out["face_order"]), _i(out["stencil_nbr"]),
+                                           _d(out["stencil_w"]), _i(out["gather"])))
+        return out
 
     def wall_forces(self, wall_bc):
         """(Cd, Cl) over the boundary faces `wall_bc` (caller numbering)."""

@@ -82,6 +82,37 @@ typedef struct {
   const int32_t* stencil_faces;   /* [nnz] gradient_faces[i][*] */
 } plfbs_mesh_view;
 
+/* A raw OpenFOAM polyMesh (what unstructured_mesh reads from points, faces,
+ * owner and neighbour, unstructured_mesh.cpp:300-305 and the face loops after
+ * it): internal faces first, then the boundary faces patch by patch. */
+typedef struct {
+  int32_t n_points;
+  int32_t n_faces;
+  int32_t n_internal;           /* faces with a neighbour */
+  int32_t n_cells;
+  const float* points;          /* [3 n_points] x, y, z (read as float, unstructured_mesh.h:50) */
+  const int32_t* face_offsets;  /* [n_faces + 1] into face_points; every face has >= 3 vertices */
+  const int32_t* face_points;   /* [face_offsets[n_faces]] vertex indices */
+  const int32_t* owner;         /* [n_faces] */
+  const int32_t* neighbour;     /* [n_internal] */
+} plfbs_polymesh_view;
+
+/* Caller-allocated outputs of plfbs_polymesh_geometry, sized as the arrays of
+ * the mesh view above; B = n_faces - n_internal, nnz = 2 n_internal + B. */
+typedef struct {
+  int32_t* owner;             /* [F] */
+  int32_t* neighbour;         /* [F] (boundary: C + f - F_i) */
+  double* face_area;          /* [F] */
+  double* face_normal;        /* [3F] */
+  double* face_centroid;      /* [3F] */
+  double* streaming_dt;       /* [F] */
+  double* cell_volume;        /* [C+B] (ghosts 0) */
+  double* cell_centroid;      /* [3(C+B)] */
+  int32_t* stencil_offsets;   /* [C+1] */
+  int32_t* stencil_cells;     /* [nnz] */
+  int32_t* stencil_faces;     /* [nnz] */
+} plfbs_mesh_arrays;
+
 /* Boundary conditions per boundary face (Boundary_Conditions, marshalled as in
  * Solver_gpu.cu:653-655). Supported on the GPU path: rho_type 1 (Dirichlet) or
  * 2 (Neumann); vel_type 1 (Dirichlet), 2 (Neumann) or 9 (parabolic inlet). */
@@ -131,6 +162,20 @@ typedef struct {
 } plfbs_stats;
 
 typedef struct plfbs_ctx plfbs_ctx;
+
+/* The pre-processed mesh of a polyMesh, computed on `device`:
+ * unstructured_mesh::generate_internal_mesh (unstructured_mesh.cpp:1133-1233)
+ * with calc_face_delta_t (:979-983) and the ghost cells of
+ * populate_ghost_cell_from_foam_face (:1346-1375). Faces are fanned from
+ * vertex 0: area, area-weighted centroid and unit normal from the triangles'
+ * cross products; cell volumes from the tetrahedra (a . (b-a) x (c-a)) / 6,
+ * owner + and neighbour -; cell centroids as the area-weighted mean of their
+ * faces' centroids; streaming dt = min(sqrt(A)/2, 3 visc / (gamma fneq_min))
+ * (no cap when fneq_min is 0); the stencil lists each cell's faces in face
+ * order. Every sum runs in the reference's order, so the arrays equal the
+ * reference's bit for bit. Fills `out` (host memory) for plfbs_create. */
+int plfbs_polymesh_geometry(const plfbs_polymesh_view* mesh, double visc, double gamma,
+                            double fneq_min, int32_t device, plfbs_mesh_arrays* out);
 
 /* Replaces the setup half of Solver_gpu.cu:150-662: validates the views,
  * builds the least-squares weights (gradients.cpp:214-313), renumbers for
@@ -210,6 +255,17 @@ int plfbs_run_stages(plfbs_ctx* ctx, int64_t n_stages);
 int plfbs_get_gradients(plfbs_ctx* ctx, double* grad, int32_t n_cells);
 int plfbs_get_face_flux(plfbs_ctx* ctx, double* flux, int32_t n_faces);
 int plfbs_get_residual(plfbs_ctx* ctx, double* res, int32_t n_cells);
+
+/* The layout the device built, for tests, in device numbering: sizes[2] =
+ * (K stencil slots, K2 gather slots per cell); cell_order [C] and face_order
+ * [F] give the caller's cell / face of each device cell / face; stencil_nbr
+ * [K*C] and stencil_w [3][K*C] (x, y, z weights, widened from FP32 in the
+ * FP32 form) hold slot k of device cell i at k*C + i, neighbour -1 in empty
+ * slots (device numbering, ghosts C + device boundary index); gather [K2*C]
+ * holds (device face << 1) | (cell is the neighbour), -1 empty. Every array
+ * pointer may be NULL; call with only `sizes` first to size the others. */
+int plfbs_get_layout(plfbs_ctx* ctx, int32_t* sizes, int32_t* cell_order, int32_t* face_order,
+                     int32_t* stencil_nbr, double* stencil_w, int32_t* gather);
 
 /* Host-only: the least-squares weights as gradients::pre_fill_LHS_and_RHS_matrix
  * computes them (gradients.cpp:214-313, determinant as written at :282-284):

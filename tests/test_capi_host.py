@@ -157,3 +157,30 @@ def test_exact_inverse_option(plfbs_lib, mode):
             L += w * np.outer(d, d)
         if mode == 0:
             np.testing.assert_allclose(lhs_x[i] @ L, np.eye(3), atol=1e-12)
+
+
+def test_polymesh_geometry_rejects_bad_indices(plfbs_lib):
+    """The polyMesh's indices are checked on the host before any device work."""
+    import copy
+    pm = golden_cases.build("cavity")["pm"]
+    bad = copy.deepcopy(pm)
+    bad.faces = bad.faces.copy()
+    bad.faces[5, 2] = bad.points.shape[0]  # vertex out of range
+    with pytest.raises(capi.PlfbsError) as e:
+        capi.polymesh_geometry(bad, 0.01, 1.0, 0.0)
+    assert e.value.code == capi.ERR_MESH and "vertex" in str(e.value)
+    bad = copy.deepcopy(pm)
+    bad.nverts = bad.nverts.copy()
+    bad.nverts[3] = 2  # a face needs three vertices
+    with pytest.raises(capi.PlfbsError) as e:
+        capi.polymesh_geometry(bad, 0.01, 1.0, 0.0)
+    assert e.value.code == capi.ERR_MESH
+    bad = copy.deepcopy(pm)
+    bad.neighbour = bad.neighbour.copy()
+    bad.neighbour[0] = bad.owner[0]
+    with pytest.raises(capi.PlfbsError) as e:
+        capi.polymesh_geometry(bad, 0.01, 1.0, 0.0)
+    assert e.value.code == capi.ERR_MESH
+    with pytest.raises(capi.PlfbsError) as e:
+        capi.polymesh_geometry(pm, 0.01, 0.0, 0.0)
+    assert e.value.code == capi.ERR_ARG
