@@ -1,6 +1,7 @@
 // The extern "C" entry points of include/plfbs.h: context lifetime, device
 // memory, the CUDA-graph time step and the host loop around it.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -38,6 +39,8 @@ struct plfbs_ctx {
   int wall_cap = 0;
   uint64_t fingerprint = 0;  // of the caller's mesh, checked when a checkpoint is loaded
   int32_t* face_order = nullptr;  // device [F]: caller face of each device face
+  plfbs::FluxMaps flux_maps{};    // tensor maps of the TMA-staged flux kernel (FP64)
+  bool flux_maps_ok = false;
   std::string err;
 };
 
@@ -197,6 +200,42 @@ int download4(plfbs_ctx* ctx, const void* src, size_t n, std::vector<double>& ou
                        ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
   }
+  return PLFBS_OK;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// A 2D FP64 tensor map of `rows` rows of `cols` doubles (row stride cols * 8
+// bytes, a multiple of 16), boxes of one row: what tile::gather4 copies.
+bool encode_rows(CUtensorMap* map, const void* base, int cols, long long rows) {
+  auto enc = tensor_map_encoder();
+  if (!enc || rows <= 0 || (cols * 8) % 16 != 0) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)cols * 8};
+  const cuuint32_t box[2] = {(cuuint32_t)cols, 1};
+  const cuuint32_t elem[2] = {1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(base), dims, strides, box,
+             elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int check_fault(plfbs_ctx* ctx) {
+  if (ctx->stats_host->fault)
+    return set_err(ctx, PLFBS_ERR_CUDA,
+                   "a kernel's bounded wait ran out (flux staging); the state is invalid");
   return PLFBS_OK;
 }
 
@@ -527,6 +566,7 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   const long long T = (long long)L.C + L.B;
   a.C = L.C;
   a.F = L.F;
+  a.Fi = L.Fi;
   a.B = L.B;
   a.K = L.K;
   a.quirk_b = L.quirk_b;
@@ -557,6 +597,10 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   a.t1 = p;
   if ((rc = dev_alloc(ctx, &p, (size_t)L.C * 3 * e4))) return fail(rc);
   a.grad = p;
+  a.flux_maps = nullptr;
+  if (!fp32)
+    ctx->flux_maps_ok = encode_rows(&ctx->flux_maps.state, a.state, 4, L.C) &&
+                        encode_rows(&ctx->flux_maps.grad, a.grad, 12, L.C);
   if ((rc = dev_alloc(ctx, &p, (size_t)L.F * e4))) return fail(rc);
   a.flux = p;
   if ((rc = build_device_layout(ctx, *mesh))) return fail(rc);
@@ -987,9 +1031,24 @@ int plfbs_run(plfbs_ctx* ctx, int64_t max_steps, plfbs_stats* stats, double* his
     stats->kernel_ms = ms_total;
     stats->steps_run = s->steps - start;
   }
+  TRY(check_fault(ctx));
   if (ctx->stats_host->diverged)
     return set_err(ctx, PLFBS_ERR_DIVERGED, "residual is NaN or rho exceeded 1000");
   return PLFBS_OK;
+}
+
+int plfbs_set_flux_kernel(plfbs_ctx* ctx, int32_t kind) {
+  TRY(check_ctx(ctx));
+  if (kind != 0 && kind != 1) return set_err(ctx, PLFBS_ERR_ARG, "flux kernel kind is 0 or 1");
+  if (ctx->stages_done != 0)
+    return set_err(ctx, PLFBS_ERR_STATE, "flux kernel change in the middle of a step");
+  if (kind == 1 && !ctx->flux_maps_ok)
+    return set_err(ctx, PLFBS_ERR_ARG,
+                   "the TMA-staged flux kernel needs an FP64 context and tensor-map support");
+  if (kind == 1) plfbs::prepare_flux_tma();
+  CK(cudaGetLastError());
+  ctx->args.flux_maps = kind == 1 ? &ctx->flux_maps : nullptr;
+  return capture_step(ctx);
 }
 
 int plfbs_get_state(plfbs_ctx* ctx, double* rho, double* u, double* v, double* w,
@@ -1069,7 +1128,8 @@ int plfbs_run_stages(plfbs_ctx* ctx, int64_t n_stages) {
     ctx->stages_done = (ctx->stages_done + 1) % 4;
   }
   CK(cudaStreamSynchronize(ctx->stream));
-  return PLFBS_OK;
+  TRY(read_stats(ctx));
+  return check_fault(ctx);
 }
 
 int plfbs_get_gradients(plfbs_ctx* ctx, double* grad, int32_t n_cells) {
@@ -1209,7 +1269,8 @@ int plfbs_profile_steps(plfbs_ctx* ctx, int64_t n_steps, double* ms) {
   }
   for (auto& e : ev) cudaEventDestroy(e);
   CK(cudaGetLastError());
-  return PLFBS_OK;
+  TRY(read_stats(ctx));
+  return check_fault(ctx);
 }
 
 int plfbs_memory_bytes(plfbs_ctx* ctx, int64_t* bytes) {

@@ -312,6 +312,70 @@ __device__ __forceinline__ void lattice_pair(const double si[4], const double sn
 // The face flux is (momentum, mass) = ((sum e e^T f) n, (sum e f) . n) A.
 // A boundary face (neighbour > n_cells in the reference) takes both sides from
 // the boundary value and all gradients from the ghost (LBFS.cu:356-401).
+// The face's moments and flux from its reconstructed values (si owner side,
+// sn neighbour side, sc their mean, each (rho, u, v, w)) and gradients g1, g2
+// (12 doubles each; transformed in place), n the unit normal and dt the
+// streaming dt.
+__device__ __forceinline__ void face_flux_out(const KernelArgs& a, const int f, const double n[3],
+                                              const double dt, const double si[4],
+                                              const double sn[4], const double sc[4],
+                                              double g1[12], double g2[12]) {
+  const double pg = a.pg, c45 = 4.5 * pg, c15 = 1.5 * pg;
+  const double w0 = 2.0 / 9.0, w1 = 1.0 / 9.0, w7 = 1.0 / 72.0;
+  // the seven branch decisions up front: n is not needed again until the end
+  unsigned sides;
+  {
+    const double d1 = 0.001 * dt;
+    sides = pair_side<1, 0, 0>(n, d1) | pair_side<0, 1, 0>(n, d1) << 2 |
+            pair_side<0, 0, 1>(n, d1) << 4 | pair_side<1, 1, 1>(n, d1) << 6 |
+            pair_side<1, 1, -1>(n, d1) << 8 | pair_side<1, -1, 1>(n, d1) << 10 |
+            pair_side<-1, 1, 1>(n, d1) << 12;
+  }
+  // centre node (k = 0): e = 0
+  const double u2c = fma(sc[3], sc[3], fma(sc[2], sc[2], sc[1] * sc[1]));
+  double rhoI = w0 * sc[0] * fma(-c15, u2c, 1.0);
+  double m[3], P[6], D;  // first written by the pairs below (see lattice_pair)
+  lattice_pair<1, 0, 0>(si, sn, sc, g1, g2, sides & 3, dt, c45, c15, w1, rhoI, m, P, D);
+  lattice_pair<0, 1, 0>(si, sn, sc, g1, g2, sides >> 2 & 3, dt, c45, c15, w1, rhoI, m, P, D);
+  lattice_pair<0, 0, 1>(si, sn, sc, g1, g2, sides >> 4 & 3, dt, c45, c15, w1, rhoI, m, P, D);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {  // (gx, gy, gz) -> (gx + gy, gx - gy, gz), see gdot
+    const double s1 = g1[3 * k] + g1[3 * k + 1], r1 = g1[3 * k] - g1[3 * k + 1];
+    const double s2 = g2[3 * k] + g2[3 * k + 1], r2 = g2[3 * k] - g2[3 * k + 1];
+    g1[3 * k] = s1;
+    g1[3 * k + 1] = r1;
+    g2[3 * k] = s2;
+    g2[3 * k + 1] = r2;
+  }
+  lattice_pair<1, 1, 1>(si, sn, sc, g1, g2, sides >> 6 & 3, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<1, 1, -1>(si, sn, sc, g1, g2, sides >> 8 & 3, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<1, -1, 1>(si, sn, sc, g1, g2, sides >> 10 & 3, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<-1, 1, 1>(si, sn, sc, g1, g2, sides >> 12 & 3, dt, c45, c15, w7, rhoI, m, P, D);
+  rhoI += D;
+  P[0] += D;
+  P[1] += D;
+  P[2] += D;
+
+  // n, A and the relaxation factor 3 nu / (dt_s gamma) are read again here
+  // (an L1 hit) rather than held in registers through the pairs.
+  const d4 g0 = ld4(launder(a.face0), f);
+  const double nf[3] = {g0.x, g0.y, g0.z};
+  const double area = g0.w;
+  const double tau = __ldg(static_cast<const double*>(launder(a.face2)) + 4LL * f + 3);
+  const double mn = m[0] * nf[0] + m[1] * nf[1] + m[2] * nf[2];
+  const double Pn[3] = {P[0] * nf[0] + P[3] * nf[1] + P[4] * nf[2],
+                        P[3] * nf[0] + P[1] * nf[1] + P[5] * nf[2],
+                        P[4] * nf[0] + P[5] * nf[1] + P[2] * nf[2]};
+  const double p3 = rhoI * (1.0 / 3.0);
+  const double mnr = mn / rhoI * pg;
+  d4 out;
+  out.x = ((1.0 - tau) * fma(m[0], mnr, p3 * nf[0]) + tau * Pn[0]) * area;
+  out.y = ((1.0 - tau) * fma(m[1], mnr, p3 * nf[1]) + tau * Pn[1]) * area;
+  out.z = ((1.0 - tau) * fma(m[2], mnr, p3 * nf[2]) + tau * Pn[2]) * area;
+  out.w = mn * area;
+  st4(a.flux, f, out);
+}
+
 __device__ __forceinline__ int2 face_ids(const KernelArgs& a, long long f) {
   return __ldg(reinterpret_cast<const int2*>(a.face_ids) + f);
 }
@@ -369,80 +433,182 @@ __device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, cons
     }
   }
 
-  const double pg = a.pg, c45 = 4.5 * pg, c15 = 1.5 * pg;
-  const double w0 = 2.0 / 9.0, w1 = 1.0 / 9.0, w7 = 1.0 / 72.0;
-  // the seven branch decisions up front: n is not needed again until the end
-  unsigned sides;
-  {
-    const double d1 = 0.001 * dt;
-    sides = pair_side<1, 0, 0>(n, d1) | pair_side<0, 1, 0>(n, d1) << 2 |
-            pair_side<0, 0, 1>(n, d1) << 4 | pair_side<1, 1, 1>(n, d1) << 6 |
-            pair_side<1, 1, -1>(n, d1) << 8 | pair_side<1, -1, 1>(n, d1) << 10 |
-            pair_side<-1, 1, 1>(n, d1) << 12;
-  }
-  // centre node (k = 0): e = 0
-  const double u2c = fma(sc[3], sc[3], fma(sc[2], sc[2], sc[1] * sc[1]));
-  double rhoI = w0 * sc[0] * fma(-c15, u2c, 1.0);
-  double m[3], P[6], D;  // first written by the pairs below (see lattice_pair)
-  lattice_pair<1, 0, 0>(si, sn, sc, g1, g2, sides & 3, dt, c45, c15, w1, rhoI, m, P, D);
-  lattice_pair<0, 1, 0>(si, sn, sc, g1, g2, sides >> 2 & 3, dt, c45, c15, w1, rhoI, m, P, D);
-  lattice_pair<0, 0, 1>(si, sn, sc, g1, g2, sides >> 4 & 3, dt, c45, c15, w1, rhoI, m, P, D);
-#pragma unroll
-  for (int k = 0; k < 4; k++) {  // (gx, gy, gz) -> (gx + gy, gx - gy, gz), see gdot
-    const double s1 = g1[3 * k] + g1[3 * k + 1], r1 = g1[3 * k] - g1[3 * k + 1];
-    const double s2 = g2[3 * k] + g2[3 * k + 1], r2 = g2[3 * k] - g2[3 * k + 1];
-    g1[3 * k] = s1;
-    g1[3 * k + 1] = r1;
-    g2[3 * k] = s2;
-    g2[3 * k + 1] = r2;
-  }
-  lattice_pair<1, 1, 1>(si, sn, sc, g1, g2, sides >> 6 & 3, dt, c45, c15, w7, rhoI, m, P, D);
-  lattice_pair<1, 1, -1>(si, sn, sc, g1, g2, sides >> 8 & 3, dt, c45, c15, w7, rhoI, m, P, D);
-  lattice_pair<1, -1, 1>(si, sn, sc, g1, g2, sides >> 10 & 3, dt, c45, c15, w7, rhoI, m, P, D);
-  lattice_pair<-1, 1, 1>(si, sn, sc, g1, g2, sides >> 12 & 3, dt, c45, c15, w7, rhoI, m, P, D);
-  rhoI += D;
-  P[0] += D;
-  P[1] += D;
-  P[2] += D;
-
-  // n, A and the relaxation factor 3 nu / (dt_s gamma) are read again here
-  // (an L1 hit) rather than held in registers through the pairs.
-  const d4 g0 = ld4(launder(a.face0), f);
-  const double nf[3] = {g0.x, g0.y, g0.z};
-  const double area = g0.w;
-  const double tau = __ldg(static_cast<const double*>(launder(a.face2)) + 4LL * f + 3);
-  const double mn = m[0] * nf[0] + m[1] * nf[1] + m[2] * nf[2];
-  const double Pn[3] = {P[0] * nf[0] + P[3] * nf[1] + P[4] * nf[2],
-                        P[3] * nf[0] + P[1] * nf[1] + P[5] * nf[2],
-                        P[4] * nf[0] + P[5] * nf[1] + P[2] * nf[2]};
-  const double p3 = rhoI * (1.0 / 3.0);
-  const double mnr = mn / rhoI * pg;
-  d4 out;
-  out.x = ((1.0 - tau) * fma(m[0], mnr, p3 * nf[0]) + tau * Pn[0]) * area;
-  out.y = ((1.0 - tau) * fma(m[1], mnr, p3 * nf[1]) + tau * Pn[1]) * area;
-  out.z = ((1.0 - tau) * fma(m[2], mnr, p3 * nf[2]) + tau * Pn[2]) * area;
-  out.w = mn * area;
-  st4(a.flux, f, out);
+  face_flux_out(a, f, n, dt, si, sn, sc, g1, g2);
 }
 
-// Persistent over the faces (grid stride): the owner/neighbour ids of a
-// thread's next face are loaded before its current face is computed, so the
-// next face's cell gathers do not wait behind a load of its face record.
-// Four blocks per SM (128 registers, a few doubles spilled to L1) measured
-// faster than three without spills (73 vs 75 us): latency hiding wins.
-__global__ void __launch_bounds__(kFluxBlock, 4) k_flux(const KernelArgs a) {
+// Persistent over the faces [f_begin, f_end) (grid stride): the
+// owner/neighbour ids of a thread's next face are loaded before its current
+// face is computed, so the next face's cell gathers do not wait behind a load
+// of its face record. Four blocks per SM (128 registers, a few doubles spilled
+// to L1) measured faster than three without spills (73 vs 75 us) and than
+// five or six with more spills (102, 191 us): latency hiding wins until the
+// spills take over.
+__global__ void __launch_bounds__(kFluxBlock, 4) k_flux(const KernelArgs a, int f_begin,
+                                                        int f_end) {
   if (halted(a)) return;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= a.F) return;
+  long long f = f_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= f_end) return;
   int2 ids = face_ids(a, f);
   for (;;) {
     const long long fn = f + stride;
-    const int2 next = fn < a.F ? face_ids(a, fn) : make_int2(0, 0);
+    const int2 next = fn < f_end ? face_ids(a, fn) : make_int2(0, 0);
     flux_face(a, (int)f, ids);
-    if (fn >= a.F) break;
+    if (fn >= f_end) break;
     f = fn;
     ids = next;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// flux, TMA-staged (internal faces): a producer warp gathers each tile's cell
+// rows into shared memory with tile::gather4 bulk tensor copies while four
+// consumer warps compute the previous tile. The consumers never wait on a
+// global gather; the arithmetic per face is face_flux_out's.
+// ---------------------------------------------------------------------------
+constexpr int kTmaFaces = 128;  // faces per tile, one per consumer thread
+constexpr int kTmaStages = 2;
+constexpr int kTmaThreads = kTmaFaces + 32;
+// stage layout (bytes): owner state rows, neighbour state rows, owner
+// gradient rows, neighbour gradient rows
+constexpr int kTmaSo = 0, kTmaSn = kTmaFaces * 32, kTmaGo = 2 * kTmaFaces * 32,
+              kTmaGn = kTmaGo + kTmaFaces * 96, kTmaStageBytes = kTmaGn + kTmaFaces * 96;
+// + room to align the stages to 128 bytes by hand (bulk tensor copies need it)
+constexpr int kTmaSmem = kTmaStages * kTmaStageBytes + 2 * kTmaStages * 8 + 128;
+constexpr int kSpinLimit = 1 << 22;  // try_wait rounds before a wait gives up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, int bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)),
+               "r"(bytes)
+               : "memory");
+}
+// Waits for the phase of the given parity; false after kSpinLimit tries.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+  for (int i = 0; i < kSpinLimit; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// Rows r[0..3] (column 0) of a 2D tensor map into consecutive boxes at dst.
+__device__ __forceinline__ void gather4(void* dst, const CUtensorMap* map, const int r[4],
+                                        uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void report_fault(const KernelArgs& a) {
+  atomicExch(&a.stats->fault, 1);
+  atomicExch(&a.stats->halt, 1);
+}
+
+__global__ void __launch_bounds__(kTmaThreads, 3)
+    k_flux_tma(const KernelArgs a, const __grid_constant__ FluxMaps maps) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  if (halted(a)) return;
+  unsigned char* smem = smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kTmaStages * kTmaStageBytes);
+  uint64_t* empty = full + kTmaStages;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kTmaStages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kTmaFaces / 32);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const int ntiles = (a.Fi + kTmaFaces - 1) / kTmaFaces;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == kTmaFaces / 32) {
+    // producer: four faces per lane, one gather4 per row kind
+    int k = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {
+      const int s = k % kTmaStages;
+      if (k >= kTmaStages && !mbar_wait(&empty[s], (k / kTmaStages - 1) & 1)) {
+        report_fault(a);
+        return;
+      }
+      int own[4], nbr[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int f = t * kTmaFaces + 4 * lane + j;
+        const int2 id = f < a.Fi ? face_ids(a, f) : make_int2(0, 0);  // past the end: cell 0
+        own[j] = id.x;
+        nbr[j] = id.y;
+      }
+      if (lane == 0) mbar_expect_tx(&full[s], kTmaStageBytes);
+      __syncwarp();
+      unsigned char* st = smem + s * kTmaStageBytes;
+      gather4(st + kTmaSo + 128 * lane, &maps.state, own, &full[s]);
+      gather4(st + kTmaSn + 128 * lane, &maps.state, nbr, &full[s]);
+      gather4(st + kTmaGo + 384 * lane, &maps.grad, own, &full[s]);
+      gather4(st + kTmaGn + 384 * lane, &maps.grad, nbr, &full[s]);
+    }
+    return;
+  }
+  // consumers: one face per thread per tile
+  const int c = threadIdx.x;
+  int k = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {
+    const int s = k % kTmaStages;
+    const int f = t * kTmaFaces + c;
+    const bool valid = f < a.Fi;
+    d4 f0{}, f1{}, f2{};
+    if (valid) {  // face records: contiguous, issued before the wait
+      f0 = ld4(a.face0, f);
+      f1 = ld4(a.face1, f);
+      f2 = ld4(a.face2, f);
+    }
+    if (!mbar_wait(&full[s], (k / kTmaStages) & 1)) {
+      report_fault(a);
+      mbar_wait(&full[s], (k / kTmaStages) & 1);  // let copies in flight land
+      return;
+    }
+    const unsigned char* st = smem + s * kTmaStageBytes;
+    const double* so = reinterpret_cast<const double*>(st + kTmaSo) + 4 * c;
+    const double* sn_ = reinterpret_cast<const double*>(st + kTmaSn) + 4 * c;
+    const double* go = reinterpret_cast<const double*>(st + kTmaGo) + 12 * c;
+    const double* gn = reinterpret_cast<const double*>(st + kTmaGn) + 12 * c;
+    // state rows are (u, v, w, rho)
+    const double qov[4] = {so[3], so[0], so[1], so[2]}, qnv[4] = {sn_[3], sn_[0], sn_[1], sn_[2]};
+    double g1[12], g2[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) {
+      g1[i] = go[i];
+      g2[i] = gn[i];
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+    if (!valid) continue;
+    const double n[3] = {f0.x, f0.y, f0.z};
+    const double dt = f1.x;
+    const double t1[3] = {f1.y, f1.z, f1.w}, t2[3] = {f2.x, f2.y, f2.z};
+    double si[4], sn[4], sc[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      si[q] = qov[q] - (t1[0] * g1[3 * q] + t1[1] * g1[3 * q + 1] + t1[2] * g1[3 * q + 2]);
+      sn[q] = qnv[q] - (t2[0] * g2[3 * q] + t2[1] * g2[3 * q + 1] + t2[2] * g2[3 * q + 2]);
+      sc[q] = (si[q] + sn[q]) * 0.5;
+    }
+    face_flux_out(a, f, n, dt, si, sn, sc, g1, g2);
   }
 }
 
@@ -813,10 +979,44 @@ void launch_gradient(const KernelArgs& a, int precision, cudaStream_t s) {
   if (precision == PLFBS_FP32_DEVIATION) return launch_gradient32(a, s);
   k_gradient<<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
 }
+int prepare_flux_tma() {
+  static std::atomic<int> tma_resident[kMaxDevices];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) dev = 0;
+  int r = tma_resident[dev].load(std::memory_order_relaxed);
+  if (r <= 0) {
+    int per_sm = 0, sms = 0;
+    cudaFuncSetAttribute(k_flux_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flux_tma, kTmaThreads, kTmaSmem) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        per_sm <= 0 || sms <= 0) {
+      per_sm = 1;
+      sms = 148;
+    }
+    r = per_sm * sms;
+    tma_resident[dev].store(r, std::memory_order_relaxed);
+  }
+  return r;
+}
+
 void launch_flux(const KernelArgs& a, int precision, cudaStream_t s) {
   if (precision == PLFBS_FP32_DEVIATION) return launch_flux32(a, s);
   static std::atomic<int> resident[kMaxDevices];
-  k_flux<<<persistent_blocks(k_flux, kFluxBlock, a.F, resident), kFluxBlock, 0, s>>>(a);
+  if (!a.flux_maps || a.Fi == 0) {
+    k_flux<<<persistent_blocks(k_flux, kFluxBlock, a.F, resident), kFluxBlock, 0, s>>>(a, 0, a.F);
+    return;
+  }
+  // internal faces through the TMA-staged kernel, boundary faces (the last
+  // F - Fi of the face order) through the per-thread one
+  const int r = prepare_flux_tma();
+  const int tiles = (a.Fi + kTmaFaces - 1) / kTmaFaces;
+  k_flux_tma<<<tiles < r ? tiles : r, kTmaThreads, kTmaSmem, s>>>(a, *a.flux_maps);
+  if (a.F > a.Fi) {
+    static std::atomic<int> bnd_resident[kMaxDevices];
+    k_flux<<<persistent_blocks(k_flux, kFluxBlock, a.F - a.Fi, bnd_resident), kFluxBlock, 0, s>>>(
+        a, a.Fi, a.F);
+  }
 }
 template <int RK>
 static void launch_update_rk(const KernelArgs& a, int nb, cudaStream_t s) {

@@ -2,6 +2,7 @@
 // (capi.cpp) and the kernels (kernels.cu). Not part of the public ABI.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -180,16 +181,23 @@ struct DevStats {
   int halt;                    // 1 once converged or diverged: kernels return at entry
   int converged;
   int diverged;
-  int pad0;
+  int fault;                   // a kernel's bounded wait ran out (the step is invalid)
   long long steps;             // completed time steps
   long long converged_step;
   double last[6];              // t, max_error, rho, u, v, w rms of the last step
   alignas(128) double history[kHistoryCap][6];
 };
 
+// Tensor maps of the FP64 state and gradient rows for the TMA-staged flux
+// kernel (k_flux_tma): 2D, one cell per row, boxes one row high.
+struct FluxMaps {
+  CUtensorMap state;  // [C rows][4 doubles]
+  CUtensorMap grad;   // [C rows][12 doubles]
+};
+
 struct KernelArgs {
   // sizes
-  int C, F, B, K, K2, quirk_b, N, nblk_update;
+  int C, F, Fi, B, K, K2, quirk_b, N, nblk_update;
   int ibm_xc, ibm_yc;
   // scalars
   double dt;            // RK time step
@@ -225,6 +233,9 @@ struct KernelArgs {
   const int32_t* face_ids;                     // int2 [F]
   float* fforce_x; float* fforce_y; float* fforce_z;  // [C] body force / U, or null
   float rho0f, inv_uref_f;
+  // host side: tensor maps of the TMA-staged FP64 flux kernel, or null for
+  // the per-thread gathers (read by launch_flux, not by kernels)
+  const FluxMaps* flux_maps;
 };
 
 // Launchers (kernels.cu; the FP32 deviation form in kernels_fp32.cu). All
@@ -232,6 +243,9 @@ struct KernelArgs {
 void launch_ibm(const KernelArgs& a, int precision, cudaStream_t stream);
 void launch_gradient(const KernelArgs& a, int precision, cudaStream_t stream);
 void launch_flux(const KernelArgs& a, int precision, cudaStream_t stream);
+// Sets the TMA-staged flux kernel's shared-memory size on the current device
+// (once) and returns its resident block count; call before capturing it.
+int prepare_flux_tma();
 void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t stream);
 void launch_seed(const KernelArgs& a, int precision, bool conserved, cudaStream_t stream);
 void launch_wall_forces(const KernelArgs& a, int precision, const int* walls, int n,

@@ -30,7 +30,8 @@ EXPORTS = ("plfbs_create", "plfbs_set_state", "plfbs_run", "plfbs_get_state",
            "plfbs_last_error", "plfbs_destroy", "plfbs_version",
            "plfbs_residual_norms_noalloc", "plfbs_release_cached", "plfbs_warm_start",
            "plfbs_checkpoint_bytes", "plfbs_save_checkpoint", "plfbs_load_checkpoint",
-           "plfbs_wall_forces", "plfbs_get_layout", "plfbs_polymesh_geometry")
+           "plfbs_wall_forces", "plfbs_get_layout", "plfbs_polymesh_geometry",
+           "plfbs_set_flux_kernel")
 
 
 class MeshView(C.Structure):
@@ -113,6 +114,7 @@ def lib():
         L.plfbs_checkpoint_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
         L.plfbs_wall_forces.argtypes = [C.c_void_p, _ip, C.c_int32, _dp, _dp]
         L.plfbs_get_layout.argtypes = [C.c_void_p, _ip, _ip, _ip, _ip, _dp, _ip]
+        L.plfbs_set_flux_kernel.argtypes = [C.c_void_p, C.c_int32]
         L.plfbs_polymesh_geometry.argtypes = [C.POINTER(PolyMeshView), C.c_double, C.c_double,
                                               C.c_double, C.c_int32, C.POINTER(MeshOut)]
         L.plfbs_save_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
@@ -335,6 +337,10 @@ class Solver:
             nx = np.ascontiguousarray(node_x, np.float64).reshape(self.N, 3)
         self._check(lib().plfbs_warm_start(self.h, *[_d(c) for c in cols], self.T,
                                            _d(nx) if nx is not None else None, self.N))
+
+    def set_flux_kernel(self, kind):
+        """0: per-thread gathers (default); 1: TMA-staged internal faces (FP64)."""
+        self._check(lib().plfbs_set_flux_kernel(self.h, int(kind)))
 
     def layout(self):
         """The device-built layout (device numbering): dict of cell_order [C],

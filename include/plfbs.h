@@ -278,6 +278,13 @@ int plfbs_ls_weights(const plfbs_mesh_view* mesh, int32_t gradient_mode, double*
  * ms[4] = {ibm, gradient, flux, update}. For profiling; the state advances. */
 int plfbs_profile_steps(plfbs_ctx* ctx, int64_t n_steps, double* ms);
 
+/* Which FP64 flux kernel the step uses: 0 = one thread per face gathering its
+ * cells' state and gradients itself (the default); 1 = internal faces staged
+ * through shared memory by a producer warp's tile::gather4 bulk tensor copies
+ * (TMA), consumer warps computing from shared memory, boundary faces as in 0.
+ * Both compute the same flux bit for bit. PLFBS_ERR_ARG for FP32 contexts. */
+int plfbs_set_flux_kernel(plfbs_ctx* ctx, int32_t kind);
+
 /* Device bytes held by the context. */
 int plfbs_memory_bytes(plfbs_ctx* ctx, int64_t* bytes);
 
