@@ -511,6 +511,12 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   *out = nullptr;
   if (cfg->precision != PLFBS_FP64 && cfg->precision != PLFBS_FP32_DEVIATION)
     return set_err(nullptr, PLFBS_ERR_ARG, "unknown precision mode");
+  if (cfg->flavour != PLFBS_FLAVOUR_GPU && cfg->flavour != PLFBS_FLAVOUR_CPU_SOLVER)
+    return set_err(nullptr, PLFBS_ERR_ARG, "unknown flavour");
+  if (cfg->flavour == PLFBS_FLAVOUR_CPU_SOLVER &&
+      (cfg->precision != PLFBS_FP64 || (ibm && ibm->n_nodes > 0)))
+    return set_err(nullptr, PLFBS_ERR_ARG,
+                   "the CPU-Solver flavour is FP64 without IBM nodes (the CPU Solver has none)");
   if (!(cfg->time_marching_step > 0) || !(cfg->gamma > 0) || !(cfg->ref_rho > 0) ||
       !(cfg->max_velocity > 0) || !std::isfinite(cfg->visc))
     return set_err(nullptr, PLFBS_ERR_ARG,
@@ -570,12 +576,16 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   a.B = L.B;
   a.K = L.K;
   a.quirk_b = L.quirk_b;
+  a.flavour = cfg->flavour;
   a.N = N;
   a.nblk_update = (L.C + plfbs::kBlock - 1) / plfbs::kBlock;
   a.dt = cfg->time_marching_step;
   a.pg = 1.0 / cfg->gamma;
   a.visc3 = cfg->visc * 3;
-  a.pressure_gradient = cfg->pressure_gradient;
+  // body force: +pressure_gradient on the GPU path (Solver_gpu.cu:700), the
+  // CPU Solver's force = -pressure_gradient (Solver.cpp:213)
+  a.pressure_gradient =
+      cfg->flavour == PLFBS_FLAVOUR_CPU_SOLVER ? -cfg->pressure_gradient : cfg->pressure_gradient;
   a.tolerance = cfg->tolerance;
   a.inv_ref_rho = 1.0 / cfg->ref_rho;
   // the FP32 form keeps momentum residuals divided by U
@@ -1042,9 +1052,10 @@ int plfbs_set_flux_kernel(plfbs_ctx* ctx, int32_t kind) {
   if (kind != 0 && kind != 1) return set_err(ctx, PLFBS_ERR_ARG, "flux kernel kind is 0 or 1");
   if (ctx->stages_done != 0)
     return set_err(ctx, PLFBS_ERR_STATE, "flux kernel change in the middle of a step");
-  if (kind == 1 && !ctx->flux_maps_ok)
+  if (kind == 1 && (!ctx->flux_maps_ok || ctx->cfg.flavour != PLFBS_FLAVOUR_GPU))
     return set_err(ctx, PLFBS_ERR_ARG,
-                   "the TMA-staged flux kernel needs an FP64 context and tensor-map support");
+                   "the TMA-staged flux kernel needs an FP64 GPU-flavour context and "
+                   "tensor-map support");
   if (kind == 1) plfbs::prepare_flux_tma();
   CK(cudaGetLastError());
   ctx->args.flux_maps = kind == 1 ? &ctx->flux_maps : nullptr;

@@ -77,12 +77,37 @@ __device__ __forceinline__ bool halted(const KernelArgs& a) {
   return h != 0;
 }
 
-// Ghost state from its owner (update_unstructured_bcs, LBFS.cu:1228-1301).
-// bc1 holds the Dirichlet target: the raw value, or for the parabolic inlet
-// (vel type 9) the profile 16 u (H/2+y)(H/2-y)(H/2+z)(H/2-z)/H^4 in x.
+// Ghost state from its owner. FL = 0 (GPU kernels, update_unstructured_bcs
+// in LBFS.cu:1228-1301): bc1 holds the Dirichlet target, the raw value or for
+// the parabolic inlet (vel type 9) the profile 16 u (H/2+y)(H/2-y)(H/2+z)(H/2-z)/H^4
+// in x. FL = 1 (CPU Solver, Solution::update_unstructured_bcs,
+// Solution.cpp:759-833): rho 1 mirror, 2 copy, 6 and 7 the value; velocity 1
+// mirror, 2 copy, 6 the value, 8 (u, -v, w) of the owner.
+template <int FL>
 __device__ __forceinline__ d4 ghost_state(const d4& q, const d4& tgt, int types) {
   const int rt = types & 0xff, vt = types >> 8;
   d4 g;
+  if (FL == 1) {
+    g.w = rt == 1 ? tgt.w - (q.w - tgt.w) : (rt == 2 ? q.w : tgt.w);
+    if (vt == 1) {
+      g.x = tgt.x - (q.x - tgt.x);
+      g.y = tgt.y - (q.y - tgt.y);
+      g.z = tgt.z - (q.z - tgt.z);
+    } else if (vt == 2) {
+      g.x = q.x;
+      g.y = q.y;
+      g.z = q.z;
+    } else if (vt == 8) {
+      g.x = q.x;
+      g.y = -q.y;
+      g.z = q.z;
+    } else {
+      g.x = tgt.x;
+      g.y = tgt.y;
+      g.z = tgt.z;
+    }
+    return g;
+  }
   g.w = (rt == 1) ? tgt.w - (q.w - tgt.w) : q.w;
   if (vt == 2) {
     g.x = q.x;
@@ -105,7 +130,7 @@ __device__ __forceinline__ d4 ghost_state(const d4& q, const d4& tgt, int types)
 // loaded first, then every slot's weights and neighbour state, so a cell waits
 // for two rounds of loads rather than two per slot; wider stencils fall back
 // to walking the slots.
-template <bool GHOSTS>
+template <bool GHOSTS, int FL>
 __device__ __forceinline__ void gradient_slot(const KernelArgs& a, int i, long long s, int j,
                                               const d4& qi, double g[12]) {
   d4 qj;
@@ -115,7 +140,7 @@ __device__ __forceinline__ void gradient_slot(const KernelArgs& a, int i, long l
     const int b = j - a.C;
     const d4 tgt = ld4(a.bc1, b);
     const int types = (int)__ldg(reinterpret_cast<const double*>(a.bc3) + 4LL * b + 3);
-    qj = ghost_state(qi, tgt, types);
+    qj = ghost_state<FL>(qi, tgt, types);
     st4(a.state, j, qj);  // the ghost's only reader in this kernel is its owner
   }
   const double w[3] = {__ldg(static_cast<const double*>(a.st_wx) + s),
@@ -130,6 +155,7 @@ __device__ __forceinline__ void gradient_slot(const KernelArgs& a, int i, long l
 
 constexpr int kStencilUnroll = 8;
 
+template <int FL>
 __global__ void __launch_bounds__(kBlock) k_gradient(const KernelArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (halted(a)) return;
@@ -145,13 +171,13 @@ __global__ void __launch_bounds__(kBlock) k_gradient(const KernelArgs a) {
       jj[k] = k < a.K ? __ldg(a.st_nbr + (long long)k * a.C + i) : -1;
 #pragma unroll
     for (int k = 0; k < kStencilUnroll; k++)
-      if (jj[k] >= 0) gradient_slot<true>(a, i, (long long)k * a.C + i, jj[k], qi, g);
+      if (jj[k] >= 0) gradient_slot<true, FL>(a, i, (long long)k * a.C + i, jj[k], qi, g);
   } else {
     for (int k = 0; k < a.K; k++) {
       const long long s = (long long)k * a.C + i;
       const int j = __ldg(a.st_nbr + s);
       if (j < 0) break;
-      gradient_slot<true>(a, i, s, j, qi, g);
+      gradient_slot<true, FL>(a, i, s, j, qi, g);
     }
   }
   st4(a.grad, 3LL * i + 0, d4{g[0], g[1], g[2], g[3]});
@@ -170,21 +196,39 @@ __device__ __forceinline__ void load_grad(const void* base, int c, double g[12])
   g[8] = a2.x; g[9] = a2.y; g[10] = a2.z; g[11] = a2.w;
 }
 
-// Ghost gradient (get_bc_gradients, LBFS.cu:1306-1416): Dirichlet
-// 2 (bc - q_owner) / |d| * d_hat from the raw boundary value; Neumann the
-// owner's gradient times (1 - |n|) componentwise.
+// Ghost gradient. FL = 0 (get_bc_gradients, LBFS.cu:1306-1416): Dirichlet
+// 2 (bc - q_owner) / |d| * d_hat from the raw boundary value (bc2 = (d_hat,
+// |d|)); Neumann the owner's gradient times (1 - |n|) componentwise (bc3).
+// FL = 1 (gradients::Get_LS_Gradients and get_ghost_grads,
+// gradients.cpp:370-506,592-648): Dirichlet (rho 1, velocity 1 and 8) along
+// the face normal (bc2 = (n, |d|)), Neumann times (1 - n) (bc3), types 6 zero,
+// rho 7 the owner's gradient.
+template <int FL>
 __device__ __forceinline__ void ghost_grad(const d4& q, const double go[12], const d4& bv,
                                            const d4& dd, const d4& nm, int types,
                                            double g[12]) {
   const int rt = types & 0xff, vt = types >> 8;
   const double dir[3] = {dd.x, dd.y, dd.z}, m[3] = {nm.x, nm.y, nm.z};
   const double dq[4] = {2 * (bv.w - q.w), 2 * (bv.x - q.x), 2 * (bv.y - q.y), 2 * (bv.z - q.z)};
+  if constexpr (FL == 1) {
 #pragma unroll
-  for (int f = 0; f < 4; f++) {
-    const bool dirichlet = (f == 0) ? (rt == 1) : (vt != 2);
+    for (int f = 0; f < 4; f++) {
+      const int t = f == 0 ? rt : vt;
 #pragma unroll
-    for (int c = 0; c < 3; c++)
-      g[3 * f + c] = dirichlet ? dq[f] / dd.w * dir[c] : go[3 * f + c] * m[c];
+      for (int c = 0; c < 3; c++)
+        g[3 * f + c] = (t == 1 || (f > 0 && t == 8)) ? dq[f] / dd.w * dir[c]
+                       : t == 2                      ? go[3 * f + c] * m[c]
+                       : t == 7                      ? go[3 * f + c]
+                                                     : 0.0;
+    }
+  } else {
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+      const bool dirichlet = (f == 0) ? (rt == 1) : (vt != 2);
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+        g[3 * f + c] = dirichlet ? dq[f] / dd.w * dir[c] : go[3 * f + c] * m[c];
+    }
   }
 }
 
@@ -212,10 +256,13 @@ __device__ __forceinline__ double gdot(const double* g) {
 }
 
 // Branch of a lattice pair from s = e . n (see lattice_pair), as two bits.
-template <int EX, int EY, int EZ>
+// FL = 1 (the CPU Solver, Solver.cpp:840-1274) has no dead band: s == 0 takes
+// both nodes from the owner side (3).
+template <int EX, int EY, int EZ, int FL>
 __device__ __forceinline__ unsigned pair_side(const double n[3], double d1) {
   const double s = (EX ? (EX > 0 ? n[0] : -n[0]) : 0.0) + (EY ? (EY > 0 ? n[1] : -n[1]) : 0.0) +
                    (EZ ? (EZ > 0 ? n[2] : -n[2]) : 0.0);
+  if (FL == 1) return s > 0.0 ? 1u : (s < 0.0 ? 2u : 3u);
   return s > d1 ? 1u : (s < -d1 ? 2u : 0u);
 }
 
@@ -228,7 +275,7 @@ __device__ __forceinline__ unsigned pair_side(const double n[3], double d1) {
 // rho_I, m = sum e f and P = sum e e^T f (xx, yy, zz, xy, xz, yz). A diagonal
 // pair adds the same f_k + f_k' to rho_I, P_xx, P_yy and P_zz: those pairs sum
 // it once into D, which the caller adds to the four.
-template <int EX, int EY, int EZ>
+template <int EX, int EY, int EZ, int FL>
 __device__ __forceinline__ void lattice_pair(const double si[4], const double sn[4],
                                              const double sc[4], const double g1[12],
                                              const double g2[12], int side, double dt,
@@ -250,6 +297,13 @@ __device__ __forceinline__ void lattice_pair(const double si[4], const double sn
     for (int f = 0; f < 4; f++) {
       qa[f] = fma(-gdot<EX, EY, EZ>(g2 + 3 * f), dt, sn[f]);
       qb[f] = fma(gdot<EX, EY, EZ>(g1 + 3 * f), dt, si[f]);
+    }
+  } else if (FL == 1) {  // side 3: both nodes from the owner side
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+      const double e = gdot<EX, EY, EZ>(g1 + 3 * f);
+      qa[f] = fma(-e, dt, si[f]);
+      qb[f] = fma(e, dt, si[f]);
     }
   } else {
     const double hdt = 0.5 * dt;  // e . (g1 + g2) / 2 dt
@@ -316,6 +370,7 @@ __device__ __forceinline__ void lattice_pair(const double si[4], const double sn
 // sn neighbour side, sc their mean, each (rho, u, v, w)) and gradients g1, g2
 // (12 doubles each; transformed in place), n the unit normal and dt the
 // streaming dt.
+template <int FL>
 __device__ __forceinline__ void face_flux_out(const KernelArgs& a, const int f, const double n[3],
                                               const double dt, const double si[4],
                                               const double sn[4], const double sc[4],
@@ -326,18 +381,18 @@ __device__ __forceinline__ void face_flux_out(const KernelArgs& a, const int f, 
   unsigned sides;
   {
     const double d1 = 0.001 * dt;
-    sides = pair_side<1, 0, 0>(n, d1) | pair_side<0, 1, 0>(n, d1) << 2 |
-            pair_side<0, 0, 1>(n, d1) << 4 | pair_side<1, 1, 1>(n, d1) << 6 |
-            pair_side<1, 1, -1>(n, d1) << 8 | pair_side<1, -1, 1>(n, d1) << 10 |
-            pair_side<-1, 1, 1>(n, d1) << 12;
+    sides = pair_side<1, 0, 0, FL>(n, d1) | pair_side<0, 1, 0, FL>(n, d1) << 2 |
+            pair_side<0, 0, 1, FL>(n, d1) << 4 | pair_side<1, 1, 1, FL>(n, d1) << 6 |
+            pair_side<1, 1, -1, FL>(n, d1) << 8 | pair_side<1, -1, 1, FL>(n, d1) << 10 |
+            pair_side<-1, 1, 1, FL>(n, d1) << 12;
   }
   // centre node (k = 0): e = 0
   const double u2c = fma(sc[3], sc[3], fma(sc[2], sc[2], sc[1] * sc[1]));
   double rhoI = w0 * sc[0] * fma(-c15, u2c, 1.0);
   double m[3], P[6], D;  // first written by the pairs below (see lattice_pair)
-  lattice_pair<1, 0, 0>(si, sn, sc, g1, g2, sides & 3, dt, c45, c15, w1, rhoI, m, P, D);
-  lattice_pair<0, 1, 0>(si, sn, sc, g1, g2, sides >> 2 & 3, dt, c45, c15, w1, rhoI, m, P, D);
-  lattice_pair<0, 0, 1>(si, sn, sc, g1, g2, sides >> 4 & 3, dt, c45, c15, w1, rhoI, m, P, D);
+  lattice_pair<1, 0, 0, FL>(si, sn, sc, g1, g2, sides & 3, dt, c45, c15, w1, rhoI, m, P, D);
+  lattice_pair<0, 1, 0, FL>(si, sn, sc, g1, g2, sides >> 2 & 3, dt, c45, c15, w1, rhoI, m, P, D);
+  lattice_pair<0, 0, 1, FL>(si, sn, sc, g1, g2, sides >> 4 & 3, dt, c45, c15, w1, rhoI, m, P, D);
 #pragma unroll
   for (int k = 0; k < 4; k++) {  // (gx, gy, gz) -> (gx + gy, gx - gy, gz), see gdot
     const double s1 = g1[3 * k] + g1[3 * k + 1], r1 = g1[3 * k] - g1[3 * k + 1];
@@ -347,10 +402,10 @@ __device__ __forceinline__ void face_flux_out(const KernelArgs& a, const int f, 
     g2[3 * k] = s2;
     g2[3 * k + 1] = r2;
   }
-  lattice_pair<1, 1, 1>(si, sn, sc, g1, g2, sides >> 6 & 3, dt, c45, c15, w7, rhoI, m, P, D);
-  lattice_pair<1, 1, -1>(si, sn, sc, g1, g2, sides >> 8 & 3, dt, c45, c15, w7, rhoI, m, P, D);
-  lattice_pair<1, -1, 1>(si, sn, sc, g1, g2, sides >> 10 & 3, dt, c45, c15, w7, rhoI, m, P, D);
-  lattice_pair<-1, 1, 1>(si, sn, sc, g1, g2, sides >> 12 & 3, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<1, 1, 1, FL>(si, sn, sc, g1, g2, sides >> 6 & 3, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<1, 1, -1, FL>(si, sn, sc, g1, g2, sides >> 8 & 3, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<1, -1, 1, FL>(si, sn, sc, g1, g2, sides >> 10 & 3, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<-1, 1, 1, FL>(si, sn, sc, g1, g2, sides >> 12 & 3, dt, c45, c15, w7, rhoI, m, P, D);
   rhoI += D;
   P[0] += D;
   P[1] += D;
@@ -380,6 +435,7 @@ __device__ __forceinline__ int2 face_ids(const KernelArgs& a, long long f) {
   return __ldg(reinterpret_cast<const int2*>(a.face_ids) + f);
 }
 
+template <int FL>
 __device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, const int2 ids) {
   const d4 f0 = ld4(a.face0, f), f1 = ld4(a.face1, f), f2 = ld4(a.face2, f);
   const int o = ids.x, nb = ids.y;
@@ -400,27 +456,34 @@ __device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, cons
     const int b = nb - a.C;
     const d4 bv = ld4(a.bc0, b), tgt = ld4(a.bc1, b), dd = ld4(a.bc2, b), nm = ld4(a.bc3, b);
     const int types = (int)nm.w;
-    ghost_grad(qo, g1, bv, dd, nm, types, g2);
+    ghost_grad<FL>(qo, g1, bv, dd, nm, types, g2);
     if (b == a.quirk_b) {
       // The reference tests neighbour > n_cells (LBFS.cu:356), so its first
       // ghost (index n_cells) goes through the interior branch with the ghost
       // state and gradient as the neighbour's.
-      qn = ghost_state(qo, tgt, types);
+      qn = ghost_state<FL>(qo, tgt, types);
     } else {
       interior = false;
       const int rt = types & 0xff, vt = types >> 8;
       const double bvv[4] = {bv.w, bv.x, bv.y, bv.z};
 #pragma unroll
       for (int k = 0; k < 4; k++) {
-        const bool dirichlet = (k == 0) ? (rt == 1) : (vt != 2);
-        sc[k] = dirichlet ? bvv[k]
-                          : qov[k] - (t1[0] * g2[3 * k] + t1[1] * g2[3 * k + 1] +
-                                      t1[2] * g2[3 * k + 2]);
+        // FL = 1 (populate_lattice_macros, Solver.cpp:862-904): rho 1 and
+        // velocity 1 the value, velocity 8 (u, 0, w) of the owner, otherwise
+        // extrapolated with the ghost gradient
+        const bool dirichlet = (k == 0) ? (rt == 1) : (FL == 1 ? vt == 1 : vt != 2);
+        const double ext =
+            qov[k] - (t1[0] * g2[3 * k] + t1[1] * g2[3 * k + 1] + t1[2] * g2[3 * k + 2]);
+        sc[k] = dirichlet ? bvv[k] : (FL == 1 && k > 0 && vt == 8) ? (k == 2 ? 0.0 : qov[k]) : ext;
         si[k] = sc[k];
         sn[k] = sc[k];
       }
+      // FL = 0: the ghost gradient on both sides (LBFS.cu:398-401); FL = 1
+      // keeps the owner's on the owner side
+      if (FL == 0) {
 #pragma unroll
-      for (int k = 0; k < 12; k++) g1[k] = g2[k];
+        for (int k = 0; k < 12; k++) g1[k] = g2[k];
+      }
     }
   }
   if (interior) {
@@ -433,7 +496,7 @@ __device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, cons
     }
   }
 
-  face_flux_out(a, f, n, dt, si, sn, sc, g1, g2);
+  face_flux_out<FL>(a, f, n, dt, si, sn, sc, g1, g2);
 }
 
 // Persistent over the faces [f_begin, f_end) (grid stride): the
@@ -443,6 +506,7 @@ __device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, cons
 // to L1) measured faster than three without spills (73 vs 75 us) and than
 // five or six with more spills (102, 191 us): latency hiding wins until the
 // spills take over.
+template <int FL>
 __global__ void __launch_bounds__(kFluxBlock, 4) k_flux(const KernelArgs a, int f_begin,
                                                         int f_end) {
   if (halted(a)) return;
@@ -453,7 +517,7 @@ __global__ void __launch_bounds__(kFluxBlock, 4) k_flux(const KernelArgs a, int 
   for (;;) {
     const long long fn = f + stride;
     const int2 next = fn < f_end ? face_ids(a, fn) : make_int2(0, 0);
-    flux_face(a, (int)f, ids);
+    flux_face<FL>(a, (int)f, ids);
     if (fn >= f_end) break;
     f = fn;
     ids = next;
@@ -608,7 +672,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
       sn[q] = qnv[q] - (t2[0] * g2[3 * q] + t2[1] * g2[3 * q + 1] + t2[2] * g2[3 * q + 2]);
       sc[q] = (si[q] + sn[q]) * 0.5;
     }
-    face_flux_out(a, f, n, dt, si, sn, sc, g1, g2);
+    face_flux_out<0>(a, f, n, dt, si, sn, sc, g1, g2);
   }
 }
 
@@ -977,7 +1041,10 @@ inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
 void launch_gradient(const KernelArgs& a, int precision, cudaStream_t s) {
   if (precision == PLFBS_FP32_DEVIATION) return launch_gradient32(a, s);
-  k_gradient<<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
+  if (a.flavour == PLFBS_FLAVOUR_CPU_SOLVER)
+    k_gradient<1><<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
+  else
+    k_gradient<0><<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
 }
 int prepare_flux_tma() {
   static std::atomic<int> tma_resident[kMaxDevices];
@@ -1003,8 +1070,15 @@ int prepare_flux_tma() {
 void launch_flux(const KernelArgs& a, int precision, cudaStream_t s) {
   if (precision == PLFBS_FP32_DEVIATION) return launch_flux32(a, s);
   static std::atomic<int> resident[kMaxDevices];
+  if (a.flavour == PLFBS_FLAVOUR_CPU_SOLVER) {
+    static std::atomic<int> cpu_resident[kMaxDevices];
+    k_flux<1><<<persistent_blocks(k_flux<1>, kFluxBlock, a.F, cpu_resident), kFluxBlock, 0, s>>>(
+        a, 0, a.F);
+    return;
+  }
   if (!a.flux_maps || a.Fi == 0) {
-    k_flux<<<persistent_blocks(k_flux, kFluxBlock, a.F, resident), kFluxBlock, 0, s>>>(a, 0, a.F);
+    k_flux<0><<<persistent_blocks(k_flux<0>, kFluxBlock, a.F, resident), kFluxBlock, 0, s>>>(
+        a, 0, a.F);
     return;
   }
   // internal faces through the TMA-staged kernel, boundary faces (the last
@@ -1014,8 +1088,8 @@ void launch_flux(const KernelArgs& a, int precision, cudaStream_t s) {
   k_flux_tma<<<tiles < r ? tiles : r, kTmaThreads, kTmaSmem, s>>>(a, *a.flux_maps);
   if (a.F > a.Fi) {
     static std::atomic<int> bnd_resident[kMaxDevices];
-    k_flux<<<persistent_blocks(k_flux, kFluxBlock, a.F - a.Fi, bnd_resident), kFluxBlock, 0, s>>>(
-        a, a.Fi, a.F);
+    k_flux<0><<<persistent_blocks(k_flux<0>, kFluxBlock, a.F - a.Fi, bnd_resident), kFluxBlock,
+                0, s>>>(a, a.Fi, a.F);
   }
 }
 template <int RK>

@@ -198,6 +198,7 @@ struct FluxMaps {
 struct KernelArgs {
   // sizes
   int C, F, Fi, B, K, K2, quirk_b, N, nblk_update;
+  int flavour;  // PLFBS_FLAVOUR_*: whose reconstruction and boundary tables
   int ibm_xc, ibm_yc;
   // scalars
   double dt;            // RK time step

@@ -349,16 +349,21 @@ int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfb
     return PLFBS_ERR_MESH;
   }
   L.K = K;
+  const bool cpu = cfg.flavour == PLFBS_FLAVOUR_CPU_SOLVER;
   for (int b = 0; b < B; b++) {
     const int rt = bcv.rho_type[b], vt = bcv.vel_type[b];
-    if (rt != 1 && rt != 2) {
-      err = msg("boundary rho_type not defined on the GPU path (LBFS.cu:1252-1260 "
-                "handles 1 dirichlet and 2 neumann)", b, rt);
+    if (cpu ? (rt != 1 && rt != 2 && rt != 6 && rt != 7) : (rt != 1 && rt != 2)) {
+      err = msg(cpu ? "boundary rho_type not taken by the CPU-Solver flavour (1, 2, 6, 7)"
+                    : "boundary rho_type not defined on the GPU path (LBFS.cu:1252-1260 "
+                      "handles 1 dirichlet and 2 neumann)",
+                b, rt);
       return PLFBS_ERR_BC;
     }
-    if (vt != 1 && vt != 2 && vt != 9) {
-      err = msg("boundary vel_type not defined on the GPU path (LBFS.cu:1262-1294 "
-                "handles 1 dirichlet, 2 neumann, 9 parabolic)", b, vt);
+    if (cpu ? (vt != 1 && vt != 2 && vt != 6 && vt != 8) : (vt != 1 && vt != 2 && vt != 9)) {
+      err = msg(cpu ? "boundary vel_type not taken by the CPU-Solver flavour (1, 2, 6, 8)"
+                    : "boundary vel_type not defined on the GPU path (LBFS.cu:1262-1294 "
+                      "handles 1 dirichlet, 2 neumann, 9 parabolic)",
+                b, vt);
       return PLFBS_ERR_BC;
     }
     for (int c = 0; c < 4; c++)
@@ -409,21 +414,24 @@ int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfb
     const double* n = m.face_normal + 3 * (size_t)f;
     for (int c = 0; c < 4; c++) L.bc0[4 * (size_t)bn + c] = val[c];
     for (int c = 0; c < 4; c++) L.bc1[4 * (size_t)bn + c] = val[c];
-    if (bcv.vel_type[bo] == 9) {  // parabolic inlet target, LBFS.cu:1286
+    if (!cpu && bcv.vel_type[bo] == 9) {  // parabolic inlet target, LBFS.cu:1286
       L.bc1[4 * (size_t)bn] =
           16 * val[0] * (H2 + cg[1]) * (H2 - cg[1]) * (H2 + cg[2]) * (H2 - cg[2]) / H4;
     }
     const double dx = cg[0] - cn[0], dy = cg[1] - cn[1], dz = cg[2] - cn[2];
     const double dmag = std::sqrt(std::pow(dx, 2.0) + std::pow(dy, 2.0) + std::pow(dz, 2.0));
+    // Dirichlet ghost-gradient direction and Neumann factors: the unit
+    // owner->ghost vector and 1 - |n| (LBFS.cu:1306-1416), or for the CPU
+    // Solver the face normal and 1 - n (gradients.cpp:383-386,612-645)
     double* d = &L.bc2[4 * (size_t)bn];
-    d[0] = dx / dmag;
-    d[1] = dy / dmag;
-    d[2] = dz / dmag;
+    d[0] = cpu ? n[0] : dx / dmag;
+    d[1] = cpu ? n[1] : dy / dmag;
+    d[2] = cpu ? n[2] : dz / dmag;
     d[3] = dmag;
     double* t = &L.bc3[4 * (size_t)bn];
-    t[0] = 1 - std::fabs(n[0]);
-    t[1] = 1 - std::fabs(n[1]);
-    t[2] = 1 - std::fabs(n[2]);
+    t[0] = cpu ? 1 - n[0] : 1 - std::fabs(n[0]);
+    t[1] = cpu ? 1 - n[1] : 1 - std::fabs(n[1]);
+    t[2] = cpu ? 1 - n[2] : 1 - std::fabs(n[2]);
     t[3] = (double)(bcv.rho_type[bo] | (bcv.vel_type[bo] << 8));
     if (!(dmag > 0)) {
       err = msg("ghost centroid coincides with its owner's", bo, own);

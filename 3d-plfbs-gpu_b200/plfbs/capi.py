@@ -18,6 +18,7 @@ OK, ERR_ARG, ERR_MESH, ERR_BC, ERR_CUDA, ERR_DIVERGED, ERR_NO_DEVICE, ERR_STATE 
     0, -1, -2, -3, -4, -5, -6, -7)
 GRAD_LS, GRAD_HYBRID, GRAD_GREEN_GAUSS, GRAD_EXACT_INVERSE = 0, 1, 2, 0x100
 FP64, FP32_DEVIATION = 0, 1
+FLAVOUR_GPU, FLAVOUR_CPU_SOLVER = 0, 1
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -70,7 +71,7 @@ class Config(C.Structure):
                 ("tolerance", C.c_double), ("pressure_gradient", C.c_double),
                 ("channel_height", C.c_double), ("origin", C.c_double * 3),
                 ("lengths", C.c_double * 3), ("gradient_mode", C.c_int32),
-                ("precision", C.c_int32), ("renumber", C.c_int32), ("reserved", C.c_int32)]
+                ("precision", C.c_int32), ("renumber", C.c_int32), ("flavour", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -214,7 +215,7 @@ class Solver:
 
     ``cfg`` keys: visc, gamma, dt (time_marching_step), domain_dt, max_velocity,
     ref_rho, tolerance, pressure_gradient, channel_height, origin, lengths,
-    gradient_mode, precision, renumber. ``ibm`` (optional): node_ref [N,3],
+    gradient_mode, precision, renumber, flavour. ``ibm`` (optional): node_ref [N,3],
     node_x [N,3], stiffness, radius, depth, object_nodes.
     """
 
@@ -247,6 +248,7 @@ class Solver:
         cf.gradient_mode = cfg.get("gradient_mode", GRAD_LS)
         cf.precision = cfg.get("precision", FP64)
         cf.renumber = cfg.get("renumber", 0)
+        cf.flavour = cfg.get("flavour", FLAVOUR_GPU)
         iv = IBMView()
         self.N = 0
         if ibm is not None and len(ibm.get("node_ref", [])) > 0:

@@ -503,8 +503,8 @@ class BC:
     u: float
     v: float
     w: float
-    vel_type: str  # dirichlet | neumann | parabolic
-    rho_type: str  # dirichlet | neumann
+    vel_type: str  # a name of BC_TYPES
+    rho_type: str  # a name of BC_TYPES
 
 
 @dataclass
@@ -618,8 +618,14 @@ def write_xml(path, c: Case):
         f.write("\n".join(g) + "\n")
 
 
-VEL_TYPES = {"dirichlet": 1, "neumann": 2, "parabolic": 9}
-RHO_TYPES = {"dirichlet": 1, "neumann": 2}
+# The reference's boundary-type names and codes, the same table for velocity
+# and density (preprocessor.cpp:241-262). The GPU path defines 1, 2 and 9
+# (LBFS.cu:1252-1294); the CPU Solver 1, 2, 3, 6, 7 and 8 (Solution.cpp:759-833,
+# gradients.cpp:370-506).
+BC_TYPES = {"dirichlet": 1, "neumann": 2, "periodic": 3, "parabolic-N": 4, "parabolic-W": 5,
+            "inlet": 6, "wall": 7, "symmetry-x": 8, "parabolic": 9}
+VEL_TYPES = BC_TYPES
+RHO_TYPES = BC_TYPES
 
 
 def bc_arrays(ma: MeshArrays, case: Case):

@@ -54,6 +54,24 @@ enum {
   PLFBS_GRAD_EXACT_INVERSE = 0x100
 };
 
+/* Which of the reference's two solvers the step reproduces.
+ * PLFBS_FLAVOUR_GPU: its CUDA kernels (LBFS.cu), the path Solver_gpu.cu runs:
+ *   boundary types 1, 2 and 9, the +-0.001 dt dead band with face averages,
+ *   the ghost gradient on both sides of a boundary face, Neumann 1 - |n|,
+ *   body force +pressure_gradient, IBM.
+ * PLFBS_FLAVOUR_CPU_SOLVER: its CPU Solver (Solver.cpp:88-590,840-1274 with
+ *   gradients.cpp:319-506,592-648 and Solution.cpp:759-833): strict-sign
+ *   upwinding (a lattice node on a face-parallel direction from the owner
+ *   side), owner gradients on the owner side of a boundary face, Dirichlet
+ *   ghost gradients along the face normal, Neumann 1 - n, rho types 1, 2, 6
+ *   ("inlet", the value) and 7 ("wall", the value with the owner's gradient),
+ *   velocity types 1, 2, 6 ("inlet") and 8 ("symmetry-x", (u, -v, w)), body
+ *   force -pressure_gradient; FP64 only, no IBM (the CPU Solver has none).
+ *   Periodic boundaries (3) are not taken: the reference's partner search reads
+ *   an uninitialised cell index (Boundary_Conditions.cpp:426-444); nor rho type
+ *   8, whose ghost gradient the reference never writes. */
+enum { PLFBS_FLAVOUR_GPU = 0, PLFBS_FLAVOUR_CPU_SOLVER = 1 };
+
 /* Arithmetic of the time step. */
 enum {
   PLFBS_FP64 = 0,            /* the reference's FP64 semantics */
@@ -148,7 +166,7 @@ typedef struct {
   int32_t gradient_mode;      /* PLFBS_GRAD_*, optionally | PLFBS_GRAD_EXACT_INVERSE */
   int32_t precision;          /* PLFBS_FP64 or PLFBS_FP32_DEVIATION */
   int32_t renumber;           /* 1: reorder cells (RCM) and faces for locality */
-  int32_t reserved;
+  int32_t flavour;            /* PLFBS_FLAVOUR_*: whose reconstruction and boundary tables */
 } plfbs_config;
 
 typedef struct {

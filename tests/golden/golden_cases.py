@@ -12,6 +12,14 @@ exercises a different part of the reference's GPU path:
   graded    6x6x5 geometrically graded hexes, hybrid LS/Green-Gauss weights,
             gamma = 1.3, streaming dt capped by fneq_min, offset origin
   converge  the cavity with a loose tolerance: stops after its first step
+
+and of the reference CPU Solver (Solver.cpp), no IBM, from a seeded field:
+
+  cpu_cavity   6x5x4 cavity, Dirichlet walls and lid, Neumann density
+  cpu_channel  10x6x6 channel, gamma = 1.2, a body force: velocity "inlet" (6),
+               Dirichlet-density outlet, "symmetry-x" (8) sides in y, no-slip
+               walls in z with density "wall" (7)
+  cpu_tets     4x4x4 hexes with jittered nodes split into 384 tetrahedra, walls
 """
 
 from __future__ import annotations
@@ -28,6 +36,7 @@ sys.path.insert(0, os.path.join(REPO, "3d-plfbs-gpu_b200"))
 from plfbs import cases  # noqa: E402
 
 NAMES = ("cavity", "channel", "graded", "converge")
+CPU_NAMES = ("cpu_cavity", "cpu_channel", "cpu_tets")
 
 
 def _random_state(ma, seed, amp=0.02):
@@ -103,3 +112,37 @@ def oracle_cfg(d):
                 gradient_mode={"LS": 0, "hybrid": 1}.get(c.gradient_calc, 2),
                 node_ref=nodes, node_x=nodes, stiffness=c.obj_stiffness, radius=c.obj_radius,
                 depth=c.obj_depth, object_nodes=nodes.shape[0])
+
+
+def build_cpu(name):
+    """Returns dict(pm, case, nodes, state0, ma) for a CPU-Solver case."""
+    if name == "cpu_cavity":
+        pm = cases.uniform_box(6, 5, 4, patch_types=["wall", "wall", "wall", "lid", "wall", "wall"])
+        c = cases.Case(mesh_dir="", X=6, Y=5, Z=4, dt=0.1, mach=0.1, reynolds=100.0,
+                       ref_length=4.0, tolerance=0.0, steps=25, gpu_solver=0,
+                       bcs=[cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann"),
+                            cases.BC("lid", 1, 1, 0, 0, "dirichlet", "neumann")])
+        seed = 21
+    elif name == "cpu_channel":
+        pm = cases.uniform_box(10, 6, 6, patch_types=["inlet", "outlet", "slip", "slip", "wall",
+                                                      "wall"])
+        c = cases.Case(mesh_dir="", X=10, Y=6, Z=6, dt=0.1, mach=0.05, reynolds=50.0,
+                       ref_length=6.0, tolerance=0.0, steps=20, gpu_solver=0, gamma=1.2,
+                       pressure_gradient=2e-5,
+                       bcs=[cases.BC("inlet", 1, 1, 0, 0, "inlet", "neumann"),
+                            cases.BC("outlet", 1, 0, 0, 0, "neumann", "dirichlet"),
+                            cases.BC("slip", 1, 0, 0, 0, "symmetry-x", "neumann"),
+                            cases.BC("wall", 1, 0, 0, 0, "dirichlet", "wall")])
+        seed = 22
+    elif name == "cpu_tets":
+        pm = cases.jittered_tet_box(4, jitter=0.1, seed=23,
+                                    patch_types=["wall", "wall", "wall", "lid", "wall", "wall"])
+        c = cases.Case(mesh_dir="", X=4, Y=4, Z=4, dt=0.05, mach=0.1, reynolds=100.0,
+                       ref_length=4.0, tolerance=0.0, steps=10, gpu_solver=0,
+                       bcs=[cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann"),
+                            cases.BC("lid", 1, 1, 0, 0, "dirichlet", "neumann")])
+        seed = 24
+    else:
+        raise KeyError(name)
+    ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
+    return dict(pm=pm, case=c, nodes=np.zeros((0, 3)), state0=_random_state(ma, seed), ma=ma)

@@ -10,6 +10,11 @@ gradients, face fluxes, residuals and state after the first RK stage, the body
 force and Lagrangian nodes after the first IBM update, and the state, RK
 accumulator, residual history and nodes after the last step, and (for a run
 that converges) the wall drag and lift coefficients of cylinder_post_processing.
+
+The CPU-Solver cases (golden_cases.CPU_NAMES) run oracle/_ref/plfbs_ref_cpu,
+the same program with <gpu_solver>0</gpu_solver> whose final state
+ref_cpu_dump.cpp writes losslessly; their fixtures cpu_<case>.npz hold the
+initial and final states.
 """
 
 from __future__ import annotations
@@ -34,9 +39,21 @@ KEEP = ("sizes", "owner", "neighbour", "stencil", "face_area", "streaming_dt", "
         "final_state", "final_t1", "history", "steps_done", "final_nodes", "wall_forces")
 
 
+CPU_BIN = os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle", "_ref", "plfbs_ref_cpu")
+
+
 def main():
     tmp = tempfile.mkdtemp(prefix="plfbs_golden_")
     try:
+        for name in golden_cases.CPU_NAMES:
+            d = golden_cases.build_cpu(name)
+            dumps = refrun.run_reference(os.path.join(tmp, name), d["pm"], d["case"],
+                                         init_state=d["state0"], binary=CPU_BIN)
+            out = dict(state_init=d["state0"], final_state=dumps["cpu_final_state"],
+                       steps=np.array([d["case"].steps], np.int32))
+            path = os.path.join(HERE, name + ".npz")
+            np.savez_compressed(path, **out)
+            print("%-11s %7d bytes  steps=%d" % (name, os.path.getsize(path), d["case"].steps))
         for name in golden_cases.NAMES:
             d = golden_cases.build(name)
             dumps = refrun.run_reference(os.path.join(tmp, name), d["pm"], d["case"],

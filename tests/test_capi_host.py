@@ -184,3 +184,50 @@ def test_polymesh_geometry_rejects_bad_indices(plfbs_lib):
     with pytest.raises(capi.PlfbsError) as e:
         capi.polymesh_geometry(pm, 0.01, 0.0, 0.0)
     assert e.value.code == capi.ERR_ARG
+
+
+def test_flavour_boundary_tables(plfbs_lib):
+    """Each flavour takes its own reference solver's boundary types; checked
+    on the host, so a case that passes reaches the device check."""
+    d = golden_cases.build_cpu("cpu_channel")
+    ma = d["ma"]
+    rt, vt, val = cases.bc_arrays(ma, d["case"])
+    assert set(vt) == {1, 2, 6, 8} and set(rt) == {1, 2, 7}
+    cfg = dict(golden_cases.oracle_cfg(d))
+    with pytest.raises(capi.PlfbsError) as e:  # GPU kernels: types 1, 2, 9 only
+        capi.Solver(ma, rt, vt, val, cfg)
+    assert e.value.code == capi.ERR_BC
+    cpu = dict(cfg, flavour=capi.FLAVOUR_CPU_SOLVER)
+    try:  # valid: fails only for want of a device
+        capi.Solver(ma, rt, vt, val, cpu).close()
+    except capi.PlfbsError as e:
+        assert e.code == capi.ERR_NO_DEVICE
+    bad = vt.copy()
+    bad[0] = 9  # parabolic: GPU path only
+    with pytest.raises(capi.PlfbsError) as e:
+        capi.Solver(ma, rt, bad, val, cpu)
+    assert e.value.code == capi.ERR_BC
+    bad = rt.copy()
+    bad[0] = 8  # the reference never writes this ghost's density gradient
+    with pytest.raises(capi.PlfbsError) as e:
+        capi.Solver(ma, bad, vt, val, cpu)
+    assert e.value.code == capi.ERR_BC
+    with pytest.raises(capi.PlfbsError) as e:
+        capi.Solver(ma, rt, vt, val, dict(cpu, precision=capi.FP32_DEVIATION))
+    assert e.value.code == capi.ERR_ARG
+    nodes = np.zeros((2, 3)) + 3.0
+    with pytest.raises(capi.PlfbsError) as e:
+        capi.Solver(ma, rt, vt, val, cpu, ibm=dict(node_ref=nodes, object_nodes=2))
+    assert e.value.code == capi.ERR_ARG
+    with pytest.raises(capi.PlfbsError) as e:
+        capi.Solver(ma, rt, vt, val, dict(cfg, flavour=2))
+    assert e.value.code == capi.ERR_ARG
+
+
+@pytest.mark.parametrize("name", golden_cases.CPU_NAMES)
+def test_cpu_solver_fixtures(name):
+    d = golden_cases.build_cpu(name)
+    g = load_golden(name)
+    np.testing.assert_array_equal(d["state0"], g["state_init"])
+    assert g["final_state"].shape == (d["ma"].total_cells, 4)
+    assert np.isfinite(g["final_state"]).all()
