@@ -422,7 +422,7 @@ int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfb
     const double dmag = std::sqrt(std::pow(dx, 2.0) + std::pow(dy, 2.0) + std::pow(dz, 2.0));
     // Dirichlet ghost-gradient direction and Neumann factors: the unit
     // owner->ghost vector and 1 - |n| (LBFS.cu:1306-1416), or for the CPU
-    // Solver the face normal and 1 - n (gradients.cpp:383-386,612-645)
+    // Solver the face normal and 1 - n (gradients.cpp:412-414,612-645)
     double* d = &L.bc2[4 * (size_t)bn];
     d[0] = cpu ? n[0] : dx / dmag;
     d[1] = cpu ? n[1] : dy / dmag;
