@@ -200,7 +200,7 @@ __device__ __forceinline__ void load_grad(const void* base, int c, double g[12])
 // 2 (bc - q_owner) / |d| * d_hat from the raw boundary value (bc2 = (d_hat,
 // |d|)); Neumann the owner's gradient times (1 - |n|) componentwise (bc3).
 // FL = 1 (gradients::Get_LS_Gradients and get_ghost_grads,
-// gradients.cpp:370-506,592-648): Dirichlet (rho 1, velocity 1 and 8) along
+// gradients.cpp:395-506,592-648): Dirichlet (rho 1, velocity 1 and 8) along
 // the face normal (bc2 = (n, |d|)), Neumann times (1 - n) (bc3), types 6 zero,
 // rho 7 the owner's gradient.
 template <int FL>

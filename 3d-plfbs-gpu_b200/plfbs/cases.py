@@ -621,7 +621,7 @@ def write_xml(path, c: Case):
 # The reference's boundary-type names and codes, the same table for velocity
 # and density (preprocessor.cpp:241-262). The GPU path defines 1, 2 and 9
 # (LBFS.cu:1252-1294); the CPU Solver 1, 2, 3, 6, 7 and 8 (Solution.cpp:759-833,
-# gradients.cpp:370-506).
+# gradients.cpp:395-506).
 BC_TYPES = {"dirichlet": 1, "neumann": 2, "periodic": 3, "parabolic-N": 4, "parabolic-W": 5,
             "inlet": 6, "wall": 7, "symmetry-x": 8, "parabolic": 9}
 VEL_TYPES = BC_TYPES
