@@ -87,6 +87,29 @@ cudaMemPool_t device_pool(int device) {
   return g_pools[device];
 }
 
+// Pinned host copies of the run status, recycled across contexts: freeing
+// pinned memory can stall for a long time on a busy host, so plfbs_destroy
+// returns the buffer here and only plfbs_release_cached frees them.
+std::vector<DevStats*> g_pinned_stats;
+
+DevStats* take_pinned_stats() {
+  {
+    std::lock_guard<std::mutex> g(g_pool_mutex);
+    if (!g_pinned_stats.empty()) {
+      DevStats* p = g_pinned_stats.back();
+      g_pinned_stats.pop_back();
+      return p;
+    }
+  }
+  void* p = nullptr;
+  return cudaMallocHost(&p, sizeof(DevStats)) == cudaSuccess ? static_cast<DevStats*>(p) : nullptr;
+}
+
+void give_pinned_stats(DevStats* p) {
+  std::lock_guard<std::mutex> g(g_pool_mutex);
+  g_pinned_stats.push_back(p);
+}
+
 int pool_alloc(plfbs_ctx* ctx, void** dst, size_t n) {
   cudaMemPool_t pool = device_pool(ctx->device);
   if (!pool) return set_err(ctx, PLFBS_ERR_CUDA, "device memory pool creation failed");
@@ -565,7 +588,7 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
     return fail(set_err(ctx, PLFBS_ERR_CUDA, "stream/event creation failed"));
-  if (cudaMallocHost(&ctx->stats_host, sizeof(DevStats)) != cudaSuccess)
+  if (!(ctx->stats_host = take_pinned_stats()))
     return fail(set_err(ctx, PLFBS_ERR_CUDA, "cudaMallocHost failed"));
 
   KernelArgs& a = ctx->args;
@@ -686,7 +709,7 @@ void plfbs_destroy(plfbs_ctx* ctx) {
   if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
   for (void* p : ctx->allocs) cudaFreeAsync(p, ctx->stream);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  if (ctx->stats_host) cudaFreeHost(ctx->stats_host);
+  if (ctx->stats_host) give_pinned_stats(ctx->stats_host);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -754,6 +777,12 @@ int plfbs_release_cached(int32_t device) {
       return set_err(nullptr, PLFBS_ERR_ARG, "device index out of range");
     pool = g_pools[device];
   }
+  std::vector<DevStats*> pinned;
+  {
+    std::lock_guard<std::mutex> g(g_pool_mutex);
+    pinned.swap(g_pinned_stats);
+  }
+  for (DevStats* p : pinned) cudaFreeHost(p);
   if (!pool) return PLFBS_OK;
   cudaError_t e = cudaMemPoolTrimTo(pool, 0);
   if (e != cudaSuccess)
