@@ -30,32 +30,15 @@
 
 #include "Solver_gpu.h"
 #include "plfbs.h"
+#include "plfbs_shim_common.hpp"
 #include "residuals.h"
 #include "tecplot_output.h"
 
 gpu_solver::gpu_solver() {}
 gpu_solver::~gpu_solver() {}
 
-namespace {
-
-struct Owned {
-  std::vector<int32_t> owner, neighbour, st_off, st_cells, st_faces, rho_type, vel_type;
-  std::vector<double> area, normal, fcen, sdt, vol, ccen, bcval, xref, x;
-};
-
-int gradient_mode(const std::string& s) {
-  // gradients.cpp:259-265
-  if (s == "hybrid") return PLFBS_GRAD_HYBRID;
-  if (s == "LS") return PLFBS_GRAD_LS;
-  return PLFBS_GRAD_GREEN_GAUSS;
-}
-
-void report(plfbs_ctx* ctx, const char* what, int rc) {
-  std::cout << "plfbs: " << what << " failed (" << rc << "): " << plfbs_last_error(ctx)
-            << std::endl;
-}
-
-}  // namespace
+using plfbs_shim::Owned;
+using plfbs_shim::report;
 
 void gpu_solver::General_Purpose_Solver_mk_i(
     unstructured_mesh& Mesh, Solution& soln, Boundary_Conditions& bcs, external_forces& source,
@@ -64,60 +47,11 @@ void gpu_solver::General_Purpose_Solver_mk_i(
     std::vector<lagrangian_object>& object_vec) {
   (void)source;
   (void)quad_bcs_orig;
-  const int C = Mesh.get_n_cells(), F = Mesh.get_n_faces(), Fi = Mesh.get_n_neighbours();
+  const int C = Mesh.get_n_cells();
   const int B = Mesh.get_num_bc(), T = Mesh.get_total_cells();
   Owned o;
-  // --- mesh (Solver_gpu.cu:629-651, with the stencil as CSR) -------------------
-  o.owner.resize(F);
-  o.neighbour.resize(F);
-  o.area.resize(F);
-  o.sdt.resize(F);
-  o.normal.resize(3 * (size_t)F);
-  o.fcen.resize(3 * (size_t)F);
-  for (int f = 0; f < F; f++) {
-    o.owner[f] = Mesh.get_mesh_owner(f);
-    o.neighbour[f] = Mesh.get_mesh_neighbour(f);
-    o.area[f] = Mesh.get_face_area(f);
-    o.sdt[f] = Mesh.get_delta_t_face(f);
-    o.normal[3 * f] = Mesh.get_face_i(f);
-    o.normal[3 * f + 1] = Mesh.get_face_j(f);
-    o.normal[3 * f + 2] = Mesh.get_face_k(f);
-    o.fcen[3 * f] = Mesh.get_face_x(f);
-    o.fcen[3 * f + 1] = Mesh.get_face_y(f);
-    o.fcen[3 * f + 2] = Mesh.get_face_z(f);
-  }
-  o.vol.resize(T);
-  o.ccen.resize(3 * (size_t)T);
-  for (int i = 0; i < T; i++) {
-    o.vol[i] = Mesh.get_cell_volume(i);
-    o.ccen[3 * i] = Mesh.get_centroid_x(i);
-    o.ccen[3 * i + 1] = Mesh.get_centroid_y(i);
-    o.ccen[3 * i + 2] = Mesh.get_centroid_z(i);
-  }
-  o.st_off.assign(1, 0);
-  for (int i = 0; i < C; i++) {
-    for (size_t j = 0; j < Mesh.gradient_cells[i].size(); j++) {
-      o.st_cells.push_back(Mesh.gradient_cells[i][j]);
-      o.st_faces.push_back(Mesh.gradient_faces[i][j]);
-    }
-    o.st_off.push_back((int32_t)o.st_cells.size());
-  }
-  plfbs_mesh_view mv = {C, F, Fi, o.owner.data(), o.neighbour.data(), o.area.data(),
-                        o.normal.data(), o.fcen.data(), o.sdt.data(), o.vol.data(),
-                        o.ccen.data(), o.st_off.data(), o.st_cells.data(), o.st_faces.data()};
-  // --- boundary conditions (Solver_gpu.cu:653-655) -----------------------------
-  o.rho_type.resize(B);
-  o.vel_type.resize(B);
-  o.bcval.resize(4 * (size_t)B);
-  for (int b = 0; b < B; b++) {
-    o.rho_type[b] = bcs.get_rho_type(b);
-    o.vel_type[b] = bcs.get_vel_type(b);
-    o.bcval[4 * b] = bcs.get_u(b);
-    o.bcval[4 * b + 1] = bcs.get_v(b);
-    o.bcval[4 * b + 2] = bcs.get_w(b);
-    o.bcval[4 * b + 3] = bcs.get_rho(b);
-  }
-  plfbs_bc_view bv = {o.rho_type.data(), o.vel_type.data(), o.bcval.data()};
+  const plfbs_mesh_view mv = plfbs_shim::mesh_view(Mesh, o);
+  const plfbs_bc_view bv = plfbs_shim::bc_view(bcs, B, o);
   // --- Lagrangian objects (Solver_gpu.cu:1469-1499) ---------------------------
   int N = 0;
   for (auto& obj : object_vec) N += obj.num_nodes;
@@ -142,25 +76,7 @@ void gpu_solver::General_Purpose_Solver_mk_i(
     iv.depth = object_vec[0].depth;
     iv.object_nodes = object_vec[0].num_nodes;
   }
-  plfbs_config cfg = {};
-  cfg.visc = globals.visc;
-  cfg.gamma = globals.pre_conditioned_gamma;
-  cfg.time_marching_step = globals.time_marching_step;
-  cfg.domain_dt = domain.dt;
-  cfg.max_velocity = globals.max_velocity;
-  cfg.ref_rho = globals.ref_rho;
-  cfg.tolerance = globals.tolerance;
-  cfg.pressure_gradient = init_conds.pressure_gradient;
-  cfg.channel_height = domain.Y;
-  cfg.origin[0] = domain.origin_x;
-  cfg.origin[1] = domain.origin_y;
-  cfg.origin[2] = domain.origin_z;
-  cfg.lengths[0] = domain.X;
-  cfg.lengths[1] = domain.Y;
-  cfg.lengths[2] = domain.Z;
-  cfg.gradient_mode = gradient_mode(globals.gradient_calc_type);
-  cfg.precision = PLFBS_FP64;
-  cfg.renumber = 1;
+  const plfbs_config cfg = plfbs_shim::config(globals, domain, init_conds, PLFBS_FLAVOUR_GPU);
 
   plfbs_ctx* ctx = nullptr;
   int rc = plfbs_create(&cfg, &mv, &bv, &iv, 0, &ctx);
