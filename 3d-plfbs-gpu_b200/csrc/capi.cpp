@@ -40,6 +40,8 @@ struct plfbs_ctx {
   uint64_t fingerprint = 0;  // of the caller's mesh, checked when a checkpoint is loaded
   int32_t* face_order = nullptr;  // device [F]: caller face of each device face
   plfbs::FluxMaps flux_maps{};    // tensor maps of the TMA-staged flux kernel (FP64)
+  int compact_faces = 0;          // unique face records in the compact layout (0: none)
+  int compact_cells = 0;          // unique cell weight sets in the compact layout (0: none)
   bool flux_maps_ok = false;
   std::string err;
 };
@@ -399,6 +401,80 @@ int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
   return PLFBS_OK;
 }
 
+// The compact FP64 layout: face records and cells' weight sets that are
+// bitwise equal are stored once (layout.cu, dedupe), each item keeping an
+// index. Used where a table holds at most 1/8 of the items (structured
+// regions of a mesh repeat their geometry); otherwise the kernels read the
+// per-item arrays. The per-item arrays stay for the other readers.
+int build_compact_layout(plfbs_ctx* ctx) {
+  Layout& L = ctx->L;
+  KernelArgs& a = ctx->args;
+  ctx->compact_faces = ctx->compact_cells = 0;
+  if (ctx->cfg.precision != PLFBS_FP64) return PLFBS_OK;
+  ScratchList S(ctx);
+  plfbs::RecordSource src[2];
+  src[0] = {0, L.F, 0, static_cast<const double*>(a.face0), static_cast<const double*>(a.face1),
+            static_cast<const double*>(a.face2)};
+  src[1] = {1, L.C, L.K, static_cast<const double*>(a.st_wx), static_cast<const double*>(a.st_wy),
+            static_cast<const double*>(a.st_wz)};
+  plfbs::DedupeScratch d[2];
+  int nwin[2];
+  for (int k = 0; k < 2; k++) {
+    const size_t n = (size_t)src[k].n;
+    int P = 1;
+    while ((size_t)P < 2 * n && P < (1 << 30)) P <<= 1;
+    nwin[k] = (int)((n + plfbs::kFaceWindow - 1) / plfbs::kFaceWindow);
+    d[k].P = P;
+    TRY(S.alloc(&d[k].slot_hash, 8 * (size_t)P, true));
+    TRY(S.alloc(&d[k].slot_rep, 4 * (size_t)P, false));
+    CK(cudaMemsetAsync(d[k].slot_rep, 0x7f, 4 * (size_t)P, ctx->stream));
+    TRY(S.alloc(&d[k].item_slot, 4 * n, false));
+    TRY(S.alloc(&d[k].rep_of, 4 * n, false));
+    TRY(S.alloc(&d[k].is_rep, 4 * n, false));
+    TRY(S.alloc(&d[k].off, 4 * n, false));
+    TRY(S.alloc(&d[k].wsum, 4 * (size_t)nwin[k], false));
+    TRY(S.alloc(&d[k].wbase, 4 * (size_t)(nwin[k] + 1), false));
+    TRY(S.alloc(&d[k].info, 16, true));
+    plfbs::launch_dedupe_scan(src[k], d[k], ctx->stream);
+  }
+  CK(cudaGetLastError());
+  int32_t unique[2], overflow[2];
+  for (int k = 0; k < 2; k++) {
+    CK(cudaMemcpyAsync(&unique[k], d[k].wbase + nwin[k], 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&overflow[k], d[k].info, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  void* p = nullptr;
+  for (int k = 0; k < 2; k++) {
+    const int n = src[k].n, U = unique[k];
+    if (overflow[k] || U <= 0 || U > n / 8) continue;
+    TRY(pool_alloc(ctx, &p, 4 * (size_t)n));
+    int32_t* index = static_cast<int32_t*>(p);
+    if (k == 0) {
+      void* t[3];
+      for (void*& x : t) TRY(pool_alloc(ctx, &x, 32 * (size_t)U));
+      plfbs::launch_dedupe_emit(src[k], d[k], index, static_cast<double*>(t[0]),
+                                static_cast<double*>(t[1]), static_cast<double*>(t[2]),
+                                ctx->stream);
+      a.face_rec = index;
+      a.frec0 = t[0];
+      a.frec1 = t[1];
+      a.frec2 = t[2];
+      ctx->compact_faces = U;
+    } else {
+      TRY(pool_alloc(ctx, &p, 24 * (size_t)U * L.K));
+      plfbs::launch_dedupe_emit(src[k], d[k], index, static_cast<double*>(p), nullptr, nullptr,
+                                ctx->stream);
+      a.cell_wset = index;
+      a.wtab = static_cast<const double*>(p);
+      ctx->compact_cells = U;
+    }
+  }
+  CK(cudaGetLastError());
+  a.compact = (ctx->compact_faces || ctx->compact_cells) ? 1 : 0;
+  return PLFBS_OK;
+}
+
 int check_ctx(plfbs_ctx* ctx) {
   if (!ctx) return set_err(nullptr, PLFBS_ERR_ARG, "null context");
   cudaError_t e = cudaSetDevice(ctx->device);
@@ -637,6 +713,7 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   if ((rc = dev_alloc(ctx, &p, (size_t)L.F * e4))) return fail(rc);
   a.flux = p;
   if ((rc = build_device_layout(ctx, *mesh))) return fail(rc);
+  if ((rc = build_compact_layout(ctx))) return fail(rc);
   if (fp32) {
     plfbs::BoundaryRecords32 b32;
     plfbs::boundary_records32(L, cfg->ref_rho, cfg->max_velocity, b32);
@@ -1076,6 +1153,17 @@ int plfbs_run(plfbs_ctx* ctx, int64_t max_steps, plfbs_stats* stats, double* his
   return PLFBS_OK;
 }
 
+int plfbs_set_layout_compression(plfbs_ctx* ctx, int32_t on) {
+  TRY(check_ctx(ctx));
+  if (on != 0 && on != 1) return set_err(ctx, PLFBS_ERR_ARG, "compression is 0 or 1");
+  if (ctx->stages_done != 0)
+    return set_err(ctx, PLFBS_ERR_STATE, "layout change in the middle of a step");
+  if (on && !ctx->compact_faces && !ctx->compact_cells)
+    return set_err(ctx, PLFBS_ERR_ARG, "this mesh's records do not repeat enough for the compact layout");
+  ctx->args.compact = on;
+  return capture_step(ctx);
+}
+
 int plfbs_set_flux_kernel(plfbs_ctx* ctx, int32_t kind) {
   TRY(check_ctx(ctx));
   if (kind != 0 && kind != 1) return set_err(ctx, PLFBS_ERR_ARG, "flux kernel kind is 0 or 1");
@@ -1229,6 +1317,8 @@ int plfbs_get_layout(plfbs_ctx* ctx, int32_t* sizes, int32_t* cell_order, int32_
   if (!sizes) return set_err(ctx, PLFBS_ERR_ARG, "layout: null sizes");
   sizes[0] = L.K;
   sizes[1] = L.K2;
+  sizes[2] = ctx->args.compact ? ctx->compact_faces : 0;
+  sizes[3] = ctx->args.compact ? ctx->compact_cells : 0;
   const size_t C = L.C, KC = (size_t)L.K * C;
   if (cell_order) std::memcpy(cell_order, L.cell_old_of_new.data(), 4 * C);
   if (face_order)

@@ -130,9 +130,9 @@ __device__ __forceinline__ d4 ghost_state(const d4& q, const d4& tgt, int types)
 // loaded first, then every slot's weights and neighbour state, so a cell waits
 // for two rounds of loads rather than two per slot; wider stencils fall back
 // to walking the slots.
-template <bool GHOSTS, int FL>
+template <bool GHOSTS, int FL, bool CW>
 __device__ __forceinline__ void gradient_slot(const KernelArgs& a, int i, long long s, int j,
-                                              const d4& qi, double g[12]) {
+                                              const d4& qi, double g[12], const double* wrow) {
   d4 qj;
   if (!GHOSTS || j < a.C) {
     qj = ld4(a.state, j);
@@ -143,9 +143,10 @@ __device__ __forceinline__ void gradient_slot(const KernelArgs& a, int i, long l
     qj = ghost_state<FL>(qi, tgt, types);
     st4(a.state, j, qj);  // the ghost's only reader in this kernel is its owner
   }
-  const double w[3] = {__ldg(static_cast<const double*>(a.st_wx) + s),
-                       __ldg(static_cast<const double*>(a.st_wy) + s),
-                       __ldg(static_cast<const double*>(a.st_wz) + s)};
+  // CW: the cell's weight set from the compact table (wrow = its slot's triple)
+  const double w[3] = {CW ? __ldg(wrow) : __ldg(static_cast<const double*>(a.st_wx) + s),
+                       CW ? __ldg(wrow + 1) : __ldg(static_cast<const double*>(a.st_wy) + s),
+                       CW ? __ldg(wrow + 2) : __ldg(static_cast<const double*>(a.st_wz) + s)};
   const double d[4] = {qj.w - qi.w, qj.x - qi.x, qj.y - qi.y, qj.z - qi.z};
 #pragma unroll
   for (int f = 0; f < 4; f++)
@@ -155,12 +156,13 @@ __device__ __forceinline__ void gradient_slot(const KernelArgs& a, int i, long l
 
 constexpr int kStencilUnroll = 8;
 
-template <int FL>
+template <int FL, bool CW>
 __global__ void __launch_bounds__(kBlock) k_gradient(const KernelArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (halted(a)) return;
   if (i >= a.C) return;
   const d4 qi = ld4(a.state, i);
+  const double* wset = CW ? a.wtab + (size_t)__ldg(a.cell_wset + i) * a.K * 3 : nullptr;
   double g[12];
 #pragma unroll
   for (int k = 0; k < 12; k++) g[k] = 0.0;
@@ -171,13 +173,15 @@ __global__ void __launch_bounds__(kBlock) k_gradient(const KernelArgs a) {
       jj[k] = k < a.K ? __ldg(a.st_nbr + (long long)k * a.C + i) : -1;
 #pragma unroll
     for (int k = 0; k < kStencilUnroll; k++)
-      if (jj[k] >= 0) gradient_slot<true, FL>(a, i, (long long)k * a.C + i, jj[k], qi, g);
+      if (jj[k] >= 0)
+        gradient_slot<true, FL, CW>(a, i, (long long)k * a.C + i, jj[k], qi, g,
+                                    CW ? wset + 3 * k : nullptr);
   } else {
     for (int k = 0; k < a.K; k++) {
       const long long s = (long long)k * a.C + i;
       const int j = __ldg(a.st_nbr + s);
       if (j < 0) break;
-      gradient_slot<true, FL>(a, i, s, j, qi, g);
+      gradient_slot<true, FL, CW>(a, i, s, j, qi, g, CW ? wset + 3 * k : nullptr);
     }
   }
   st4(a.grad, 3LL * i + 0, d4{g[0], g[1], g[2], g[3]});
@@ -370,8 +374,9 @@ __device__ __forceinline__ void lattice_pair(const double si[4], const double sn
 // sn neighbour side, sc their mean, each (rho, u, v, w)) and gradients g1, g2
 // (12 doubles each; transformed in place), n the unit normal and dt the
 // streaming dt.
-template <int FL>
-__device__ __forceinline__ void face_flux_out(const KernelArgs& a, const int f, const double n[3],
+template <int FL, bool CR>
+__device__ __forceinline__ void face_flux_out(const KernelArgs& a, const int f, const int r,
+                                              const double n[3],
                                               const double dt, const double si[4],
                                               const double sn[4], const double sc[4],
                                               double g1[12], double g2[12]) {
@@ -413,10 +418,10 @@ __device__ __forceinline__ void face_flux_out(const KernelArgs& a, const int f, 
 
   // n, A and the relaxation factor 3 nu / (dt_s gamma) are read again here
   // (an L1 hit) rather than held in registers through the pairs.
-  const d4 g0 = ld4(launder(a.face0), f);
+  const d4 g0 = ld4(launder(CR ? a.frec0 : a.face0), r);
   const double nf[3] = {g0.x, g0.y, g0.z};
   const double area = g0.w;
-  const double tau = __ldg(static_cast<const double*>(launder(a.face2)) + 4LL * f + 3);
+  const double tau = __ldg(static_cast<const double*>(launder(CR ? a.frec2 : a.face2)) + 4LL * r + 3);
   const double mn = m[0] * nf[0] + m[1] * nf[1] + m[2] * nf[2];
   const double Pn[3] = {P[0] * nf[0] + P[3] * nf[1] + P[4] * nf[2],
                         P[3] * nf[0] + P[1] * nf[1] + P[5] * nf[2],
@@ -435,9 +440,13 @@ __device__ __forceinline__ int2 face_ids(const KernelArgs& a, long long f) {
   return __ldg(reinterpret_cast<const int2*>(a.face_ids) + f);
 }
 
-template <int FL>
-__device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, const int2 ids) {
-  const d4 f0 = ld4(a.face0, f), f1 = ld4(a.face1, f), f2 = ld4(a.face2, f);
+// CR: the face's records from the compact tables (rec = its index there).
+template <int FL, bool CR>
+__device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, const int2 ids,
+                                          const int rec) {
+  const d4 f0 = CR ? ld4(a.frec0, rec) : ld4(a.face0, f);
+  const d4 f1 = CR ? ld4(a.frec1, rec) : ld4(a.face1, f);
+  const d4 f2 = CR ? ld4(a.frec2, rec) : ld4(a.face2, f);
   const int o = ids.x, nb = ids.y;
   const double n[3] = {f0.x, f0.y, f0.z};
   const double dt = f1.x;
@@ -496,7 +505,7 @@ __device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, cons
     }
   }
 
-  face_flux_out<FL>(a, f, n, dt, si, sn, sc, g1, g2);
+  face_flux_out<FL, CR>(a, f, CR ? rec : f, n, dt, si, sn, sc, g1, g2);
 }
 
 // Persistent over the faces [f_begin, f_end) (grid stride): the
@@ -506,7 +515,7 @@ __device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, cons
 // to L1) measured faster than three without spills (73 vs 75 us) and than
 // five or six with more spills (102, 191 us): latency hiding wins until the
 // spills take over.
-template <int FL>
+template <int FL, bool CR>
 __global__ void __launch_bounds__(kFluxBlock, 4) k_flux(const KernelArgs a, int f_begin,
                                                         int f_end) {
   if (halted(a)) return;
@@ -514,13 +523,16 @@ __global__ void __launch_bounds__(kFluxBlock, 4) k_flux(const KernelArgs a, int 
   long long f = f_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= f_end) return;
   int2 ids = face_ids(a, f);
+  int rec = CR ? __ldg(a.face_rec + f) : 0;
   for (;;) {
     const long long fn = f + stride;
     const int2 next = fn < f_end ? face_ids(a, fn) : make_int2(0, 0);
-    flux_face<FL>(a, (int)f, ids);
+    const int next_rec = (CR && fn < f_end) ? __ldg(a.face_rec + fn) : 0;
+    flux_face<FL, CR>(a, (int)f, ids, rec);
     if (fn >= f_end) break;
     f = fn;
     ids = next;
+    rec = next_rec;
   }
 }
 
@@ -672,7 +684,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
       sn[q] = qnv[q] - (t2[0] * g2[3 * q] + t2[1] * g2[3 * q + 1] + t2[2] * g2[3 * q + 2]);
       sc[q] = (si[q] + sn[q]) * 0.5;
     }
-    face_flux_out<0>(a, f, n, dt, si, sn, sc, g1, g2);
+    face_flux_out<0, false>(a, f, f, n, dt, si, sn, sc, g1, g2);
   }
 }
 
@@ -1041,10 +1053,19 @@ inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
 void launch_gradient(const KernelArgs& a, int precision, cudaStream_t s) {
   if (precision == PLFBS_FP32_DEVIATION) return launch_gradient32(a, s);
-  if (a.flavour == PLFBS_FLAVOUR_CPU_SOLVER)
-    k_gradient<1><<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
-  else
-    k_gradient<0><<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
+  const int nb = blocks_for(a.C, kBlock);
+  const bool cw = a.compact && a.wtab;
+  if (a.flavour == PLFBS_FLAVOUR_CPU_SOLVER) {
+    if (cw)
+      k_gradient<1, true><<<nb, kBlock, 0, s>>>(a);
+    else
+      k_gradient<1, false><<<nb, kBlock, 0, s>>>(a);
+  } else {
+    if (cw)
+      k_gradient<0, true><<<nb, kBlock, 0, s>>>(a);
+    else
+      k_gradient<0, false><<<nb, kBlock, 0, s>>>(a);
+  }
 }
 int prepare_flux_tma() {
   static std::atomic<int> tma_resident[kMaxDevices];
@@ -1070,15 +1091,25 @@ int prepare_flux_tma() {
 void launch_flux(const KernelArgs& a, int precision, cudaStream_t s) {
   if (precision == PLFBS_FP32_DEVIATION) return launch_flux32(a, s);
   static std::atomic<int> resident[kMaxDevices];
+  const bool cr = a.compact && a.face_rec;
   if (a.flavour == PLFBS_FLAVOUR_CPU_SOLVER) {
-    static std::atomic<int> cpu_resident[kMaxDevices];
-    k_flux<1><<<persistent_blocks(k_flux<1>, kFluxBlock, a.F, cpu_resident), kFluxBlock, 0, s>>>(
-        a, 0, a.F);
+    static std::atomic<int> cpu_resident[kMaxDevices], cpu_cr_resident[kMaxDevices];
+    if (cr)
+      k_flux<1, true><<<persistent_blocks(k_flux<1, true>, kFluxBlock, a.F, cpu_cr_resident),
+                        kFluxBlock, 0, s>>>(a, 0, a.F);
+    else
+      k_flux<1, false><<<persistent_blocks(k_flux<1, false>, kFluxBlock, a.F, cpu_resident),
+                         kFluxBlock, 0, s>>>(a, 0, a.F);
     return;
   }
   if (!a.flux_maps || a.Fi == 0) {
-    k_flux<0><<<persistent_blocks(k_flux<0>, kFluxBlock, a.F, resident), kFluxBlock, 0, s>>>(
-        a, 0, a.F);
+    static std::atomic<int> cr_resident[kMaxDevices];
+    if (cr)
+      k_flux<0, true><<<persistent_blocks(k_flux<0, true>, kFluxBlock, a.F, cr_resident),
+                        kFluxBlock, 0, s>>>(a, 0, a.F);
+    else
+      k_flux<0, false><<<persistent_blocks(k_flux<0, false>, kFluxBlock, a.F, resident),
+                         kFluxBlock, 0, s>>>(a, 0, a.F);
     return;
   }
   // internal faces through the TMA-staged kernel, boundary faces (the last
@@ -1088,8 +1119,8 @@ void launch_flux(const KernelArgs& a, int precision, cudaStream_t s) {
   k_flux_tma<<<tiles < r ? tiles : r, kTmaThreads, kTmaSmem, s>>>(a, *a.flux_maps);
   if (a.F > a.Fi) {
     static std::atomic<int> bnd_resident[kMaxDevices];
-    k_flux<0><<<persistent_blocks(k_flux<0>, kFluxBlock, a.F - a.Fi, bnd_resident), kFluxBlock,
-                0, s>>>(a, a.Fi, a.F);
+    k_flux<0, false><<<persistent_blocks(k_flux<0, false>, kFluxBlock, a.F - a.Fi, bnd_resident),
+                       kFluxBlock, 0, s>>>(a, a.Fi, a.F);
   }
 }
 template <int RK>

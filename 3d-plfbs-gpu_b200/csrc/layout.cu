@@ -532,6 +532,107 @@ __global__ void k_ghost_geometry(const DevPolyMesh pm, const GeometryOut o) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Exact deduplication of per-item records (face records, cells' weight sets):
+// items whose records are bitwise equal share one table entry. Claim: each
+// item's hash takes an open-addressed slot, the lowest item index with that
+// hash becomes the slot's representative. Resolve: an item equal to its
+// representative bit for bit maps to it, otherwise (a hash collision) to
+// itself. Representatives are numbered in item order by the window scans.
+// ---------------------------------------------------------------------------
+constexpr int kMaxProbe = 1 << 12;
+
+__device__ __forceinline__ double rec_get(const RecordSource& r, int i, int j) {
+  if (r.kind == 0) {  // three double4 arrays [n]
+    const double* p = j < 4 ? r.p0 : (j < 8 ? r.p1 : r.p2);
+    return p[4 * (size_t)i + (j & 3)];
+  }
+  const int k = j / 3, c = j - 3 * k;  // three slot-major arrays [K][n]
+  const double* p = c == 0 ? r.p0 : (c == 1 ? r.p1 : r.p2);
+  return p[(size_t)k * r.n + i];
+}
+__device__ __forceinline__ int rec_width(const RecordSource& r) { return r.kind == 0 ? 12 : 3 * r.K; }
+
+// Lanes of a warp with equal hashes claim once: the lowest of them (the
+// smallest item index) does the atomics and hands the slot to the others, so
+// the thousands of equal records of a structured mesh do not serialise on one
+// slot.
+__global__ void k_dedupe_claim(const RecordSource r, int P, unsigned long long* slot_hash,
+                               int32_t* slot_rep, int32_t* item_slot, int32_t* overflow) {
+  const int stride = gridDim.x * blockDim.x;
+  const int W = rec_width(r);
+  for (int base = blockIdx.x * blockDim.x; base < r.n; base += stride) {
+    const int i = base + (int)threadIdx.x;
+    const bool valid = i < r.n;
+    uint64_t h = 0;
+    if (valid) {
+      h = 0x9e3779b97f4a7c15ull;
+      for (int j = 0; j < W; j++)
+        h = mix64(h ^ ((uint64_t)__double_as_longlong(rec_get(r, i, j)) +
+                       0x632be59bd9b4e019ull * j));
+      h |= 1;  // 0 marks an empty slot (and idle lanes)
+    }
+    const unsigned group = __match_any_sync(0xffffffffu, (unsigned long long)h);
+    const int leader = __ffs(group) - 1;
+    int slot = -1;
+    if (valid && (int)(threadIdx.x & 31) == leader) {
+      int pos = (int)(h & (uint64_t)(P - 1));
+      for (int probe = 0; probe < kMaxProbe; probe++) {
+        const unsigned long long prev = atomicCAS(slot_hash + pos, 0ull, (unsigned long long)h);
+        if (prev == 0ull || prev == h) {
+          atomicMin(slot_rep + pos, i);
+          slot = pos;
+          break;
+        }
+        pos = (pos + 1) & (P - 1);
+      }
+      if (slot < 0) atomicExch(overflow, 1);
+    }
+    slot = __shfl_sync(0xffffffffu, slot, leader);
+    if (valid) item_slot[i] = slot;
+  }
+}
+
+__global__ void k_dedupe_resolve(const RecordSource r, const int32_t* slot_rep,
+                                 const int32_t* item_slot, int32_t* rep_of, int32_t* is_rep) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
+    const int s = item_slot[i];
+    int rep = s < 0 ? i : slot_rep[s];
+    if (rep != i) {
+      const int W = rec_width(r);
+      for (int j = 0; j < W; j++)
+        if (__double_as_longlong(rec_get(r, i, j)) != __double_as_longlong(rec_get(r, rep, j))) {
+          rep = i;
+          break;
+        }
+    }
+    rep_of[i] = rep;
+    is_rep[i] = rep == i;
+  }
+}
+
+// Item -> table index, and the representatives' records into the table
+// (kind 0: three double4 arrays [U]; kind 1: [U][K][3] doubles).
+__global__ void k_dedupe_emit(const RecordSource r, const int32_t* rep_of, const int32_t* off,
+                              const int32_t* wbase, int32_t* index, double* t0, double* t1,
+                              double* t2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
+    const int rep = rep_of[i];
+    const int id = wbase[rep / kFaceWindow] + off[rep];
+    index[i] = id;
+    if (rep != i) continue;
+    if (r.kind == 0) {
+      for (int j = 0; j < 4; j++) {
+        t0[4 * (size_t)id + j] = r.p0[4 * (size_t)i + j];
+        t1[4 * (size_t)id + j] = r.p1[4 * (size_t)i + j];
+        t2[4 * (size_t)id + j] = r.p2[4 * (size_t)i + j];
+      }
+    } else {
+      for (int j = 0; j < 3 * r.K; j++) t0[(size_t)id * 3 * r.K + j] = rec_get(r, i, j);
+    }
+  }
+}
+
 int grid_for(long long n) {
   const long long g = (n + kLayoutBlock - 1) / kLayoutBlock;
   return (int)(g < 148 * 16 ? (g > 0 ? g : 1) : 148 * 16);
@@ -589,6 +690,24 @@ void launch_layout_records(const DevMesh& m, const LayoutScratch& s, int precisi
         m, mode, st_nbr, static_cast<double*>(st_wx), static_cast<double*>(st_wy),
         static_cast<double*>(st_wz), static_cast<double*>(inv_volume), s.info);
   }
+}
+
+void launch_dedupe_scan(const RecordSource& r, const DedupeScratch& d, cudaStream_t st) {
+  const int nwin = (r.n + kFaceWindow - 1) / kFaceWindow;
+  k_dedupe_claim<<<grid_for(r.n), kLayoutBlock, 0, st>>>(r, d.P, d.slot_hash, d.slot_rep,
+                                                         d.item_slot, d.info);
+  k_dedupe_resolve<<<grid_for(r.n), kLayoutBlock, 0, st>>>(r, d.slot_rep, d.item_slot, d.rep_of,
+                                                           d.is_rep);
+  DevMesh m{};
+  m.C = r.n;
+  k_window_scan<<<nwin, kWinBlock, 0, st>>>(m, d.is_rep, d.is_rep, d.off, d.wsum, d.info + 2);
+  k_window_base<<<1, kWinBlock, 0, st>>>(d.wsum, nwin, d.wbase);
+}
+
+void launch_dedupe_emit(const RecordSource& r, const DedupeScratch& d, int32_t* index, double* t0,
+                        double* t1, double* t2, cudaStream_t st) {
+  k_dedupe_emit<<<grid_for(r.n), kLayoutBlock, 0, st>>>(r, d.rep_of, d.off, d.wbase, index, t0,
+                                                        t1, t2);
 }
 
 void launch_layout_gather(const DevMesh& m, const LayoutScratch& s, const int32_t* face_ids,

@@ -32,7 +32,7 @@ EXPORTS = ("plfbs_create", "plfbs_set_state", "plfbs_run", "plfbs_get_state",
            "plfbs_residual_norms_noalloc", "plfbs_release_cached", "plfbs_warm_start",
            "plfbs_checkpoint_bytes", "plfbs_save_checkpoint", "plfbs_load_checkpoint",
            "plfbs_wall_forces", "plfbs_get_layout", "plfbs_polymesh_geometry",
-           "plfbs_set_flux_kernel")
+           "plfbs_set_flux_kernel", "plfbs_set_layout_compression")
 
 
 class MeshView(C.Structure):
@@ -116,6 +116,7 @@ def lib():
         L.plfbs_wall_forces.argtypes = [C.c_void_p, _ip, C.c_int32, _dp, _dp]
         L.plfbs_get_layout.argtypes = [C.c_void_p, _ip, _ip, _ip, _ip, _dp, _ip]
         L.plfbs_set_flux_kernel.argtypes = [C.c_void_p, C.c_int32]
+        L.plfbs_set_layout_compression.argtypes = [C.c_void_p, C.c_int32]
         L.plfbs_polymesh_geometry.argtypes = [C.POINTER(PolyMeshView), C.c_double, C.c_double,
                                               C.c_double, C.c_int32, C.POINTER(MeshOut)]
         L.plfbs_save_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
@@ -344,10 +345,16 @@ class Solver:
         """0: per-thread gathers (default); 1: TMA-staged internal faces (FP64)."""
         self._check(lib().plfbs_set_flux_kernel(self.h, int(kind)))
 
+    def set_layout_compression(self, on):
+        """1: the kernels read the deduplicated record tables (FP64, default where
+        available); 0: the per-face / per-cell arrays."""
+        self._check(lib().plfbs_set_layout_compression(self.h, int(bool(on))))
+
     def layout(self):
         """The device-built layout (device numbering): dict of cell_order [C],
-        face_order [F], stencil_nbr [K, C], stencil_w [3, K, C], gather [K2, C]."""
-        sz = np.zeros(2, np.int32)
+        face_order [F], stencil_nbr [K, C], stencil_w [3, K, C], gather [K2, C],
+        compact = (unique face records, unique cell weight sets) in use."""
+        sz = np.zeros(4, np.int32)
         self._check(lib().plfbs_get_layout(self.h, _i(sz), None, None, None, None, None))
         K, K2 = int(sz[0]), int(sz[1])
         out = dict(cell_order=np.zeros(self.C, np.int32), face_order=np.zeros(self.F, np.int32),
@@ -356,6 +363,7 @@ class Solver:
         self._check(lib().plfbs_get_layout(self.h, _i(sz), _i(out["cell_order"]),
                                            _i(out["face_order"]), _i(out["stencil_nbr"]),
                                            _d(out["stencil_w"]), _i(out["gather"])))
+        out["compact"] = (int(sz[2]), int(sz[3]))
         return out
 
     def wall_forces(self, wall_bc):
