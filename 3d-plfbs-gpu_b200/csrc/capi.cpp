@@ -401,7 +401,7 @@ int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
   return PLFBS_OK;
 }
 
-// The compact FP64 layout: face records and cells' weight sets that are
+// The compact layout: face records and cells' weight sets that are
 // bitwise equal are stored once (layout.cu, dedupe), each item keeping an
 // index. Used where a table holds at most 1/8 of the items (structured
 // regions of a mesh repeat their geometry); otherwise the kernels read the
@@ -410,13 +410,12 @@ int build_compact_layout(plfbs_ctx* ctx) {
   Layout& L = ctx->L;
   KernelArgs& a = ctx->args;
   ctx->compact_faces = ctx->compact_cells = 0;
-  if (ctx->cfg.precision != PLFBS_FP64) return PLFBS_OK;
+  const int fp32 = ctx->cfg.precision == PLFBS_FP32_DEVIATION;
+  const size_t es = fp32 ? 4 : 8;
   ScratchList S(ctx);
   plfbs::RecordSource src[2];
-  src[0] = {0, L.F, 0, static_cast<const double*>(a.face0), static_cast<const double*>(a.face1),
-            static_cast<const double*>(a.face2)};
-  src[1] = {1, L.C, L.K, static_cast<const double*>(a.st_wx), static_cast<const double*>(a.st_wy),
-            static_cast<const double*>(a.st_wz)};
+  src[0] = {0, L.F, 0, fp32, a.face0, a.face1, a.face2};
+  src[1] = {1, L.C, L.K, fp32, a.st_wx, a.st_wy, a.st_wz};
   plfbs::DedupeScratch d[2];
   int nwin[2];
   for (int k = 0; k < 2; k++) {
@@ -452,21 +451,18 @@ int build_compact_layout(plfbs_ctx* ctx) {
     int32_t* index = static_cast<int32_t*>(p);
     if (k == 0) {
       void* t[3];
-      for (void*& x : t) TRY(pool_alloc(ctx, &x, 32 * (size_t)U));
-      plfbs::launch_dedupe_emit(src[k], d[k], index, static_cast<double*>(t[0]),
-                                static_cast<double*>(t[1]), static_cast<double*>(t[2]),
-                                ctx->stream);
+      for (void*& x : t) TRY(pool_alloc(ctx, &x, 4 * es * (size_t)U));
+      plfbs::launch_dedupe_emit(src[k], d[k], index, t[0], t[1], t[2], ctx->stream);
       a.face_rec = index;
       a.frec0 = t[0];
       a.frec1 = t[1];
       a.frec2 = t[2];
       ctx->compact_faces = U;
     } else {
-      TRY(pool_alloc(ctx, &p, 24 * (size_t)U * L.K));
-      plfbs::launch_dedupe_emit(src[k], d[k], index, static_cast<double*>(p), nullptr, nullptr,
-                                ctx->stream);
+      TRY(pool_alloc(ctx, &p, 3 * es * (size_t)U * L.K));
+      plfbs::launch_dedupe_emit(src[k], d[k], index, p, nullptr, nullptr, ctx->stream);
       a.cell_wset = index;
-      a.wtab = static_cast<const double*>(p);
+      a.wtab = p;
       ctx->compact_cells = U;
     }
   }

@@ -162,7 +162,8 @@ __global__ void __launch_bounds__(kBlock) k_gradient(const KernelArgs a) {
   if (halted(a)) return;
   if (i >= a.C) return;
   const d4 qi = ld4(a.state, i);
-  const double* wset = CW ? a.wtab + (size_t)__ldg(a.cell_wset + i) * a.K * 3 : nullptr;
+  const double* wset =
+      CW ? static_cast<const double*>(a.wtab) + (size_t)__ldg(a.cell_wset + i) * a.K * 3 : nullptr;
   double g[12];
 #pragma unroll
   for (int k = 0; k < 12; k++) g[k] = 0.0;

@@ -68,8 +68,9 @@ __device__ __forceinline__ f4 ghost_state32(const f4& q, const f4& tgt, int type
 
 // Gradient layout: 3 x float4 per cell: (rx ry rz ux)(uy uz vx vy)(vz wx wy wz).
 // Stencil slots as in k_gradient: neighbour ids first, then the slots.
+template <bool CW>
 __device__ __forceinline__ void gradient_slot32(const KernelArgs& a, long long s, int j,
-                                                const f4& qi, float g[12]) {
+                                                const f4& qi, float g[12], const float* wrow) {
   f4 qj;
   if (j < a.C) {
     qj = ldf(a.state, j);
@@ -80,9 +81,10 @@ __device__ __forceinline__ void gradient_slot32(const KernelArgs& a, long long s
     qj = ghost_state32(qi, tgt, types);
     stf(a.state, j, qj);
   }
-  const float w[3] = {__ldg(static_cast<const float*>(a.st_wx) + s),
-                      __ldg(static_cast<const float*>(a.st_wy) + s),
-                      __ldg(static_cast<const float*>(a.st_wz) + s)};
+  // CW: the cell's weight set from the compact table (wrow = its slot's triple)
+  const float w[3] = {CW ? __ldg(wrow) : __ldg(static_cast<const float*>(a.st_wx) + s),
+                      CW ? __ldg(wrow + 1) : __ldg(static_cast<const float*>(a.st_wy) + s),
+                      CW ? __ldg(wrow + 2) : __ldg(static_cast<const float*>(a.st_wz) + s)};
   const float d[4] = {qj.w - qi.w, qj.x - qi.x, qj.y - qi.y, qj.z - qi.z};
 #pragma unroll
   for (int f = 0; f < 4; f++)
@@ -90,11 +92,14 @@ __device__ __forceinline__ void gradient_slot32(const KernelArgs& a, long long s
     for (int c = 0; c < 3; c++) g[3 * f + c] = fmaf(w[c], d[f], g[3 * f + c]);
 }
 
+template <bool CW>
 __global__ void __launch_bounds__(kBlock) k_gradient32(const KernelArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (halted(a)) return;
   if (i >= a.C) return;
   const f4 qi = ldf(a.state, i);
+  const float* wset =
+      CW ? static_cast<const float*>(a.wtab) + (size_t)__ldg(a.cell_wset + i) * a.K * 3 : nullptr;
   float g[12];
 #pragma unroll
   for (int k = 0; k < 12; k++) g[k] = 0.0f;
@@ -105,13 +110,14 @@ __global__ void __launch_bounds__(kBlock) k_gradient32(const KernelArgs a) {
     for (int k = 0; k < kUnroll; k++) jj[k] = k < a.K ? __ldg(a.st_nbr + (long long)k * a.C + i) : -1;
 #pragma unroll
     for (int k = 0; k < kUnroll; k++)
-      if (jj[k] >= 0) gradient_slot32(a, (long long)k * a.C + i, jj[k], qi, g);
+      if (jj[k] >= 0)
+        gradient_slot32<CW>(a, (long long)k * a.C + i, jj[k], qi, g, CW ? wset + 3 * k : nullptr);
   } else {
     for (int k = 0; k < a.K; k++) {
       const long long s = (long long)k * a.C + i;
       const int j = __ldg(a.st_nbr + s);
       if (j < 0) break;
-      gradient_slot32(a, s, j, qi, g);
+      gradient_slot32<CW>(a, s, j, qi, g, CW ? wset + 3 * k : nullptr);
     }
   }
   stf(a.grad, 3LL * i + 0, f4{g[0], g[1], g[2], g[3]});
@@ -227,8 +233,13 @@ __device__ __forceinline__ void lattice_pair32(const float si[4], const float sn
 
 // Face flux in deviation form (see the file comment); the same branches and
 // boundary handling as k_flux in kernels.cu.
-__device__ __forceinline__ void flux_face32(const KernelArgs& a, const int f, const int2 ids) {
-  const f4 f0 = ldf(a.face0, f), f1 = ldf(a.face1, f), f2 = ldf(a.face2, f);
+// CR: the face's records from the compact tables (rec = its index there).
+template <bool CR>
+__device__ __forceinline__ void flux_face32(const KernelArgs& a, const int f, const int2 ids,
+                                            const int rec) {
+  const f4 f0 = CR ? ldf(a.frec0, rec) : ldf(a.face0, f);
+  const f4 f1 = CR ? ldf(a.frec1, rec) : ldf(a.face1, f);
+  const f4 f2 = CR ? ldf(a.frec2, rec) : ldf(a.face2, f);
   const int o = ids.x, nb = ids.y;
   const float n[3] = {f0.x, f0.y, f0.z};
   const float area = f0.w, dt = f1.x;
@@ -333,20 +344,24 @@ __device__ __forceinline__ void flux_face32(const KernelArgs& a, const int f, co
 
 // Persistent over the faces, next face's ids prefetched (as k_flux); six blocks
 // per SM (85 registers) measured fastest.
+template <bool CR>
 __global__ void __launch_bounds__(kFluxBlock, 6) k_flux32(const KernelArgs a) {
   if (halted(a)) return;
   const long long stride = (long long)gridDim.x * blockDim.x;
   long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= a.F) return;
   int2 ids = __ldg(reinterpret_cast<const int2*>(a.face_ids) + f);
+  int rec = CR ? __ldg(a.face_rec + f) : 0;
   for (;;) {
     const long long fn = f + stride;
     const int2 next =
         fn < a.F ? __ldg(reinterpret_cast<const int2*>(a.face_ids) + fn) : make_int2(0, 0);
-    flux_face32(a, (int)f, ids);
+    const int next_rec = (CR && fn < a.F) ? __ldg(a.face_rec + fn) : 0;
+    flux_face32<CR>(a, (int)f, ids, rec);
     if (fn >= a.F) break;
     f = fn;
     ids = next;
+    rec = next_rec;
   }
 }
 
@@ -617,11 +632,19 @@ void launch_update32_rk(const KernelArgs& a, int nb, cudaStream_t s) {
 }  // namespace
 
 void launch_gradient32(const KernelArgs& a, cudaStream_t s) {
-  k_gradient32<<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
+  if (a.compact && a.wtab)
+    k_gradient32<true><<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
+  else
+    k_gradient32<false><<<blocks_for(a.C, kBlock), kBlock, 0, s>>>(a);
 }
 void launch_flux32(const KernelArgs& a, cudaStream_t s) {
-  static std::atomic<int> resident[kMaxDevices];
-  k_flux32<<<persistent_blocks(k_flux32, kFluxBlock, a.F, resident), kFluxBlock, 0, s>>>(a);
+  static std::atomic<int> resident[kMaxDevices], cr_resident[kMaxDevices];
+  if (a.compact && a.face_rec)
+    k_flux32<true><<<persistent_blocks(k_flux32<true>, kFluxBlock, a.F, cr_resident), kFluxBlock,
+                     0, s>>>(a);
+  else
+    k_flux32<false><<<persistent_blocks(k_flux32<false>, kFluxBlock, a.F, resident), kFluxBlock,
+                      0, s>>>(a);
 }
 void launch_update32(const KernelArgs& a, int rk, cudaStream_t s) {
   const int nb = blocks_for(a.C, kBlock);

@@ -542,14 +542,19 @@ __global__ void k_ghost_geometry(const DevPolyMesh pm, const GeometryOut o) {
 // ---------------------------------------------------------------------------
 constexpr int kMaxProbe = 1 << 12;
 
-__device__ __forceinline__ double rec_get(const RecordSource& r, int i, int j) {
-  if (r.kind == 0) {  // three double4 arrays [n]
-    const double* p = j < 4 ? r.p0 : (j < 8 ? r.p1 : r.p2);
-    return p[4 * (size_t)i + (j & 3)];
+// Element j of item i's record, as its bits (FP64 or FP32).
+__device__ __forceinline__ uint64_t rec_bits(const RecordSource& r, int i, int j) {
+  const void* p;
+  size_t e;
+  if (r.kind == 0) {  // three 4-vector arrays [n]
+    p = j < 4 ? r.p0 : (j < 8 ? r.p1 : r.p2);
+    e = 4 * (size_t)i + (j & 3);
+  } else {  // three slot-major arrays [K][n]
+    const int k = j / 3, c = j - 3 * k;
+    p = c == 0 ? r.p0 : (c == 1 ? r.p1 : r.p2);
+    e = (size_t)k * r.n + i;
   }
-  const int k = j / 3, c = j - 3 * k;  // three slot-major arrays [K][n]
-  const double* p = c == 0 ? r.p0 : (c == 1 ? r.p1 : r.p2);
-  return p[(size_t)k * r.n + i];
+  return r.fp32 ? (uint64_t)static_cast<const uint32_t*>(p)[e] : static_cast<const uint64_t*>(p)[e];
 }
 __device__ __forceinline__ int rec_width(const RecordSource& r) { return r.kind == 0 ? 12 : 3 * r.K; }
 
@@ -568,8 +573,7 @@ __global__ void k_dedupe_claim(const RecordSource r, int P, unsigned long long* 
     if (valid) {
       h = 0x9e3779b97f4a7c15ull;
       for (int j = 0; j < W; j++)
-        h = mix64(h ^ ((uint64_t)__double_as_longlong(rec_get(r, i, j)) +
-                       0x632be59bd9b4e019ull * j));
+        h = mix64(h ^ (rec_bits(r, i, j) + 0x632be59bd9b4e019ull * j));
       h |= 1;  // 0 marks an empty slot (and idle lanes)
     }
     const unsigned group = __match_any_sync(0xffffffffu, (unsigned long long)h);
@@ -601,7 +605,7 @@ __global__ void k_dedupe_resolve(const RecordSource r, const int32_t* slot_rep,
     if (rep != i) {
       const int W = rec_width(r);
       for (int j = 0; j < W; j++)
-        if (__double_as_longlong(rec_get(r, i, j)) != __double_as_longlong(rec_get(r, rep, j))) {
+        if (rec_bits(r, i, j) != rec_bits(r, rep, j)) {
           rep = i;
           break;
         }
@@ -611,24 +615,29 @@ __global__ void k_dedupe_resolve(const RecordSource r, const int32_t* slot_rep,
   }
 }
 
+__device__ __forceinline__ void put_bits(void* t, size_t e, uint64_t v, int fp32) {
+  if (fp32)
+    static_cast<uint32_t*>(t)[e] = (uint32_t)v;
+  else
+    static_cast<uint64_t*>(t)[e] = v;
+}
+
 // Item -> table index, and the representatives' records into the table
-// (kind 0: three double4 arrays [U]; kind 1: [U][K][3] doubles).
+// (kind 0: three 4-vector arrays [U]; kind 1: [U][K][3]), bit for bit.
 __global__ void k_dedupe_emit(const RecordSource r, const int32_t* rep_of, const int32_t* off,
-                              const int32_t* wbase, int32_t* index, double* t0, double* t1,
-                              double* t2) {
+                              const int32_t* wbase, int32_t* index, void* t0, void* t1, void* t2) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
     const int rep = rep_of[i];
     const int id = wbase[rep / kFaceWindow] + off[rep];
     index[i] = id;
     if (rep != i) continue;
     if (r.kind == 0) {
-      for (int j = 0; j < 4; j++) {
-        t0[4 * (size_t)id + j] = r.p0[4 * (size_t)i + j];
-        t1[4 * (size_t)id + j] = r.p1[4 * (size_t)i + j];
-        t2[4 * (size_t)id + j] = r.p2[4 * (size_t)i + j];
-      }
+      for (int j = 0; j < 12; j++)
+        put_bits(j < 4 ? t0 : (j < 8 ? t1 : t2), 4 * (size_t)id + (j & 3), rec_bits(r, i, j),
+                 r.fp32);
     } else {
-      for (int j = 0; j < 3 * r.K; j++) t0[(size_t)id * 3 * r.K + j] = rec_get(r, i, j);
+      for (int j = 0; j < 3 * r.K; j++)
+        put_bits(t0, (size_t)id * 3 * r.K + j, rec_bits(r, i, j), r.fp32);
     }
   }
 }
@@ -704,8 +713,8 @@ void launch_dedupe_scan(const RecordSource& r, const DedupeScratch& d, cudaStrea
   k_window_base<<<1, kWinBlock, 0, st>>>(d.wsum, nwin, d.wbase);
 }
 
-void launch_dedupe_emit(const RecordSource& r, const DedupeScratch& d, int32_t* index, double* t0,
-                        double* t1, double* t2, cudaStream_t st) {
+void launch_dedupe_emit(const RecordSource& r, const DedupeScratch& d, int32_t* index, void* t0,
+                        void* t1, void* t2, cudaStream_t st) {
   k_dedupe_emit<<<grid_for(r.n), kLayoutBlock, 0, st>>>(r, d.rep_of, d.off, d.wbase, index, t0,
                                                         t1, t2);
 }

@@ -143,14 +143,15 @@ void launch_polymesh_geometry(const DevPolyMesh& pm, double ref_dt, const Geomet
 // Host checks of a polyMesh's indices (setup.cpp).
 int validate_polymesh(const plfbs_polymesh_view& pm, std::string& err);
 
-// Exact deduplication of per-item records for the compact FP64 layout
-// (layout.cu): kind 0, face records (three double4 arrays [n]); kind 1, a
-// cell's K precombined weight triples (three slot-major arrays [K][n]).
+// Exact deduplication of per-item records for the compact layout
+// (layout.cu): kind 0, face records (three 4-vector arrays [n]); kind 1, a
+// cell's K precombined weight triples (three slot-major arrays [K][n]);
+// elements FP64, or FP32 with fp32 = 1 (the deviation form's layout).
 struct RecordSource {
-  int kind, n, K;
-  const double* p0;
-  const double* p1;
-  const double* p2;
+  int kind, n, K, fp32;
+  const void* p0;
+  const void* p1;
+  const void* p2;
 };
 struct DedupeScratch {
   int P;                          // hash slots, a power of two >= 2n
@@ -167,8 +168,8 @@ struct DedupeScratch {
 // Claim, resolve and number the unique records (wbase[windows] = their count).
 void launch_dedupe_scan(const RecordSource& r, const DedupeScratch& d, cudaStream_t stream);
 // Per-item table index and the unique records into the table.
-void launch_dedupe_emit(const RecordSource& r, const DedupeScratch& d, int32_t* index, double* t0,
-                        double* t1, double* t2, cudaStream_t stream);
+void launch_dedupe_emit(const RecordSource& r, const DedupeScratch& d, int32_t* index, void* t0,
+                        void* t1, void* t2, cudaStream_t stream);
 
 // FP32 boundary records for the deviation form (PLFBS_FP32_DEVIATION):
 // rounded once from the FP64 records, values as deviations (rho - rho0,
@@ -264,12 +265,12 @@ struct KernelArgs {
   // host side: tensor maps of the TMA-staged FP64 flux kernel, or null for
   // the per-thread gathers (read by launch_flux, not by kernels)
   const FluxMaps* flux_maps;
-  // compact FP64 layout: bitwise-equal face records and cell weight sets
+  // compact layout: bitwise-equal face records and cell weight sets
   // stored once (null where the mesh's records do not repeat)
   const int32_t* face_rec;                        // [F] index into frec0/1/2
-  const void* frec0; const void* frec1; const void* frec2;  // double4 [unique records]
+  const void* frec0; const void* frec1; const void* frec2;  // double4 (FP32: float4) [unique]
   const int32_t* cell_wset;                       // [C] index into wtab
-  const double* wtab;                             // [unique sets][K][3]
+  const void* wtab;                               // [unique sets][K][3] double (FP32: float)
   int compact;                                    // 1: the kernels read the tables
 };
 

@@ -304,13 +304,14 @@ int plfbs_profile_steps(plfbs_ctx* ctx, int64_t n_steps, double* ms);
  * Both compute the same flux bit for bit. PLFBS_ERR_ARG for FP32 contexts. */
 int plfbs_set_flux_kernel(plfbs_ctx* ctx, int32_t kind);
 
-/* FP64 contexts store bitwise-equal face records (normal, area, streaming dt,
+/* Contexts store bitwise-equal face records (normal, area, streaming dt,
  * centroid offsets, relaxation factor) and cells' gradient-weight sets once,
  * each face or cell keeping an index, when a table holds at most 1/8 of the
  * items (structured regions of a mesh repeat their geometry): the kernels
- * read 4 bytes per face and per cell instead of 96 and 24 K. On by default
- * where available; 0 reads the per-item arrays (the same bits, so the same
- * results). PLFBS_ERR_ARG when the mesh has no compact layout. */
+ * read 4 bytes per face and per cell instead of 96 and 24 K (FP32: 48 and
+ * 12 K). On by default where available; 0 reads the per-item arrays (the
+ * same bits, so the same results). PLFBS_ERR_ARG when the mesh has no compact
+ * layout. */
 int plfbs_set_layout_compression(plfbs_ctx* ctx, int32_t on);
 
 /* Device bytes held by the context. */

@@ -1,4 +1,4 @@
-"""The compact FP64 layout (bitwise-equal face records and cell weight sets
+"""The compact layout (bitwise-equal face records and cell weight sets
 stored once, plfbs_set_layout_compression) against the per-item arrays: the
 kernels read the same bits, so a stage's fluxes and whole runs agree bit for
 bit (to rounding where several IBM nodes spread into one cell, whose FP64
@@ -44,16 +44,20 @@ def _compare(make, q0, steps, exact):
         np.testing.assert_allclose(out[1][1], out[0][1], rtol=1e-11, atol=1e-14)
 
 
-@pytest.mark.parametrize("flavour", [capi.FLAVOUR_GPU, capi.FLAVOUR_CPU_SOLVER])
+@pytest.mark.parametrize("flavour,precision", [(capi.FLAVOUR_GPU, capi.FP64),
+                                               (capi.FLAVOUR_CPU_SOLVER, capi.FP64),
+                                               (capi.FLAVOUR_GPU, capi.FP32_DEVIATION)])
 @pytest.mark.parametrize("renumber", [0, 1])
-def test_compact_box_is_bitwise_equal(plfbs_lib, renumber, flavour):
+def test_compact_box_is_bitwise_equal(plfbs_lib, renumber, flavour, precision):
     ma, c = _box()
     rt, vt, val = cases.bc_arrays(ma, c)
     cfg = dict(visc=c.visc, dt=c.dt, max_velocity=c.mach, channel_height=c.Y,
                lengths=(c.X, c.Y, c.Z), renumber=renumber, flavour=flavour,
-               pressure_gradient=1e-5)
+               pressure_gradient=1e-5, precision=precision)
     ibm = None
-    if flavour == capi.FLAVOUR_GPU:
+    # IBM on the FP64 GPU flavour only: its FP64 atomics reorder to rounding
+    # (compared to 1e-11); the FP32 and CPU-flavour runs compare bit for bit
+    if flavour == capi.FLAVOUR_GPU and precision == capi.FP64:
         nodes = cases.fibonacci_sphere(150, 4.0, (12.0, 10.0, 10.0))
         ibm = dict(node_ref=nodes, stiffness=0.5, radius=4.0, depth=8.0, object_nodes=len(nodes))
     rng = np.random.default_rng(9)
