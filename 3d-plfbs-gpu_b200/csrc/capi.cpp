@@ -458,6 +458,12 @@ int build_compact_layout(plfbs_ctx* ctx) {
       a.frec1 = t[1];
       a.frec2 = t[2];
       ctx->compact_faces = U;
+      if (!fp32) {
+        TRY(pool_alloc(ctx, &p, 4 * (size_t)U));
+        plfbs::launch_record_sides(t[0], t[1], U, ctx->cfg.flavour, static_cast<int32_t*>(p),
+                                   ctx->stream);
+        a.frec_sides = static_cast<const int32_t*>(p);
+      }
     } else {
       TRY(pool_alloc(ctx, &p, 3 * es * (size_t)U * L.K));
       plfbs::launch_dedupe_emit(src[k], d[k], index, p, nullptr, nullptr, ctx->stream);

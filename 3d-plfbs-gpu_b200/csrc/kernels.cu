@@ -383,9 +383,12 @@ __device__ __forceinline__ void face_flux_out(const KernelArgs& a, const int f, 
                                               double g1[12], double g2[12]) {
   const double pg = a.pg, c45 = 4.5 * pg, c15 = 1.5 * pg;
   const double w0 = 2.0 / 9.0, w1 = 1.0 / 9.0, w7 = 1.0 / 72.0;
-  // the seven branch decisions up front: n is not needed again until the end
+  // the seven branch decisions up front: n is not needed again until the end;
+  // with the compact layout they come precomputed per record (record_sides)
   unsigned sides;
-  {
+  if (CR) {  // FP64 compact layouts always carry the record sides
+    sides = (unsigned)__ldg(a.frec_sides + r);
+  } else {
     const double d1 = 0.001 * dt;
     sides = pair_side<1, 0, 0, FL>(n, d1) | pair_side<0, 1, 0, FL>(n, d1) << 2 |
             pair_side<0, 0, 1, FL>(n, d1) << 4 | pair_side<1, 1, 1, FL>(n, d1) << 6 |
@@ -1050,7 +1053,33 @@ __global__ void __launch_bounds__(kWallBlock) k_wall_forces(const KernelArgs a, 
 
 inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
+// The seven branch decisions of each unique face record of the compact
+// layout, as face_flux_out computes them.
+template <int FL>
+__global__ void k_record_sides(const void* frec0, const void* frec1, int n, int32_t* out) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const d4 f0 = ld4(frec0, r), f1 = ld4(frec1, r);
+    const double nv[3] = {f0.x, f0.y, f0.z};
+    const double d1 = 0.001 * f1.x;
+    out[r] = (int32_t)(pair_side<1, 0, 0, FL>(nv, d1) | pair_side<0, 1, 0, FL>(nv, d1) << 2 |
+                       pair_side<0, 0, 1, FL>(nv, d1) << 4 | pair_side<1, 1, 1, FL>(nv, d1) << 6 |
+                       pair_side<1, 1, -1, FL>(nv, d1) << 8 |
+                       pair_side<1, -1, 1, FL>(nv, d1) << 10 |
+                       pair_side<-1, 1, 1, FL>(nv, d1) << 12);
+  }
+}
+
 }  // namespace
+
+void launch_record_sides(const void* frec0, const void* frec1, int n, int flavour, int32_t* out,
+                         cudaStream_t s) {
+  if (n <= 0) return;
+  const int nb = (int)blocks_for(n, kBlock);
+  if (flavour == PLFBS_FLAVOUR_CPU_SOLVER)
+    k_record_sides<1><<<nb, kBlock, 0, s>>>(frec0, frec1, n, out);
+  else
+    k_record_sides<0><<<nb, kBlock, 0, s>>>(frec0, frec1, n, out);
+}
 
 void launch_gradient(const KernelArgs& a, int precision, cudaStream_t s) {
   if (precision == PLFBS_FP32_DEVIATION) return launch_gradient32(a, s);

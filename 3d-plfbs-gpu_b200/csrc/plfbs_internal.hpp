@@ -271,6 +271,7 @@ struct KernelArgs {
   const void* frec0; const void* frec1; const void* frec2;  // double4 (FP32: float4) [unique]
   const int32_t* cell_wset;                       // [C] index into wtab
   const void* wtab;                               // [unique sets][K][3] double (FP32: float)
+  const int32_t* frec_sides;                      // [unique records] branch bits (FP64)
   int compact;                                    // 1: the kernels read the tables
 };
 
@@ -287,6 +288,10 @@ void launch_seed(const KernelArgs& a, int precision, bool conserved, cudaStream_
 void launch_wall_forces(const KernelArgs& a, int precision, const int* walls, int n,
                         double visc_gamma, double gamma, double* out, cudaStream_t stream);
 void launch_ibm32(const KernelArgs& a, cudaStream_t stream);
+// Branch bits (the flux kernel's seven lattice-pair sides) of n unique FP64
+// face records of the compact layout.
+void launch_record_sides(const void* frec0, const void* frec1, int n, int flavour, int32_t* out,
+                         cudaStream_t stream);
 void launch_gradient32(const KernelArgs& a, cudaStream_t stream);
 void launch_flux32(const KernelArgs& a, cudaStream_t stream);
 void launch_update32(const KernelArgs& a, int rk, cudaStream_t stream);
