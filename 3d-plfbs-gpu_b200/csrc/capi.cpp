@@ -514,8 +514,10 @@ int check_device(int device) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0)
     return set_err(nullptr, PLFBS_ERR_NO_DEVICE, "no CUDA device with that index");
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10)
+  // one attribute (cudaGetDeviceProperties fills every field and can be slow)
+  int major = 0;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess ||
+      major != 10)
     return set_err(nullptr, PLFBS_ERR_NO_DEVICE,
                    "this library is built for sm_100a (B200); device major != 10");
   return PLFBS_OK;
@@ -649,8 +651,9 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     delete ctx;
     return set_err(nullptr, PLFBS_ERR_NO_DEVICE, "no CUDA device with that index");
   }
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+  int major = 0;  // one attribute (cudaGetDeviceProperties fills every field and can be slow)
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess ||
+      major != 10) {
     delete ctx;
     return set_err(nullptr, PLFBS_ERR_NO_DEVICE,
                    "this library is built for sm_100a (B200); device major != 10");

@@ -1068,14 +1068,17 @@ int plfbs_gnn_create(const plfbs_gnn_shape* shape, const int32_t* src, const int
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
     return gerr(nullptr, PLFBS_ERR_NO_DEVICE, "no CUDA device with that index");
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10)
+  // two attributes (cudaGetDeviceProperties fills every field and can be slow)
+  int major = 0, sms = 0;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess ||
+      major != 10 ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
     return gerr(nullptr, PLFBS_ERR_NO_DEVICE, "this library is built for sm_100a (B200)");
   plfbs_gnn* g = new (std::nothrow) plfbs_gnn();
   if (!g) return gerr(nullptr, PLFBS_ERR_ARG, "out of host memory");
   g->s = s;
   g->device = device;
-  g->sms = prop.multiProcessorCount;
+  g->sms = sms;
   auto fail = [&](int rc) {
     g_gnn_err = g->err;
     plfbs_gnn_destroy(g);

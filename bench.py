@@ -42,6 +42,7 @@ sys.path.insert(0, os.path.join(REPO, "3d-plfbs-gpu_b200"))
 from plfbs import cases  # noqa: E402
 
 METRIC = "Mcell-updates/s"
+E2E_REPS = 3  # end-to-end repetitions (the median is reported)
 WORKLOAD = "sphere_channel_128x64x64_ibm3217_fp64"
 NX, NY, NZ = 128, 64, 64
 DIAM, CENTRE, NNODES = 16.0, (32.0, 32.0, 32.0), 3217
@@ -516,26 +517,33 @@ def main():
             "unit": "GB/s", "frac": kern[dom]["frac"], "peak_kind": peak_kind,
             "traffic": load_traffic(dom, workload)}
 
-    # end to end through the C ABI from host buffers
+    # end to end through the C ABI from host buffers; the median of E2E_REPS
+    # repetitions (host-side timings on a shared machine vary from run to run)
     e2e = None
     if not args.no_e2e:
         barrier()
         solver.close()
-        t0 = time.perf_counter()
-        s2 = capi.Solver(ma, rt, vt, val, solver_cfg(c, prec), ibm=ibm_cfg(nodes),
-                         device=local_rank)
-        t1 = time.perf_counter()
-        s2.set_state(state0)
-        t2 = time.perf_counter()
-        st2, hist2 = s2.run(args.steps, history=True)
-        t3 = time.perf_counter()
-        out = s2.get_state()
-        t4 = time.perf_counter()
-        s2.close()
-        t5 = time.perf_counter()
-        wall = max_over_ranks(t5 - t0)
-        phases = {"create_s": t1 - t0, "set_state_s": t2 - t1, "run_s": t3 - t2,
-                  "get_state_s": t4 - t3, "destroy_s": t5 - t4}
+        reps = []
+        for _ in range(E2E_REPS):
+            barrier()
+            t0 = time.perf_counter()
+            s2 = capi.Solver(ma, rt, vt, val, solver_cfg(c, prec), ibm=ibm_cfg(nodes),
+                             device=local_rank)
+            t1 = time.perf_counter()
+            s2.set_state(state0)
+            t2 = time.perf_counter()
+            st2, hist2 = s2.run(args.steps, history=True)
+            t3 = time.perf_counter()
+            out = s2.get_state()
+            t4 = time.perf_counter()
+            s2.close()
+            t5 = time.perf_counter()
+            reps.append((max_over_ranks(t5 - t0),
+                         {"create_s": t1 - t0, "set_state_s": t2 - t1, "run_s": t3 - t2,
+                          "get_state_s": t4 - t3, "destroy_s": t5 - t4}))
+            assert np.isfinite(out).all() and st2["steps_run"] == args.steps
+        reps.sort(key=lambda r: r[0])
+        wall, phases = reps[len(reps) // 2]
         T = ma.total_cells
         mesh_bytes = (ma.n_faces * (4 + 4 + 8 + 24 + 24 + 8) + T * (8 + 24) +
                       (ma.n_cells + 1 + 2 * len(ma.stencil_cells)) * 4 + ma.n_bc * (4 + 4 + 32) +
@@ -546,8 +554,8 @@ def main():
                "unit": METRIC,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "wall_s": wall, "includes": "create+set_state+run+history+get_state+destroy",
+               "repetitions": E2E_REPS, "of": "median", "walls_s": [r[0] for r in reps],
                "phases": phases}
-        assert np.isfinite(out).all() and st2["steps_run"] == args.steps
     else:
         solver.close()
 
