@@ -13,44 +13,37 @@
 #include <string>
 #include <vector>
 
-#include "plfbs.h"
-#include "plfbs_internal.hpp"
+#include "capi_internal.hpp"
 
 using plfbs::DevStats;
 using plfbs::KernelArgs;
 using plfbs::Layout;
 
-struct plfbs_ctx {
-  int device = 0;
-  plfbs_config cfg{};
-  Layout L;
-  int N = 0;
-  cudaStream_t stream = nullptr;
-  cudaGraphExec_t step_exec = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  KernelArgs args{};
-  std::vector<void*> allocs;
-  int64_t bytes = 0;
-  DevStats* stats_host = nullptr;  // pinned copy of the stats header
-  long long stages_done = 0;       // stages run through plfbs_run_stages in the current step
-  bool debug = false;
-  bool have_state = false;
-  int* wall_buf = nullptr;   // device wall list of plfbs_wall_forces (grown on demand)
-  int wall_cap = 0;
-  uint64_t fingerprint = 0;  // of the caller's mesh, checked when a checkpoint is loaded
-  int32_t* face_order = nullptr;  // device [F]: caller face of each device face
-  plfbs::FluxMaps flux_maps{};    // tensor maps of the TMA-staged flux kernel (FP64)
-  int compact_faces = 0;          // unique face records in the compact layout (0: none)
-  int compact_cells = 0;          // unique cell weight sets in the compact layout (0: none)
-  bool flux_maps_ok = false;
-  std::string err;
-};
 
 namespace {
 
 std::string g_err;  // errors without a context
 
 const char* kVersion = "plfbs-b200 0.1 (sm_100a)";
+
+
+
+// Device memory comes from one stream-ordered pool per device whose release
+// threshold is unbounded: plfbs_destroy returns a context's arrays to the pool
+// (no unmapping, which cost up to 0.8 s in a process's first frees) and the
+// next plfbs_create on that device reuses them. plfbs_release_cached trims it.
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pools[plfbs::kMaxDevices] = {};
+
+
+// Pinned host copies of the run status, recycled across contexts: freeing
+// pinned memory can stall for a long time on a busy host, so plfbs_destroy
+// returns the buffer here and only plfbs_release_cached frees them.
+std::vector<DevStats*> g_pinned_stats;
+
+}  // namespace
+
+namespace plfbs_capi {
 
 int set_err(plfbs_ctx* c, int code, const std::string& m) {
   if (c)
@@ -59,20 +52,6 @@ int set_err(plfbs_ctx* c, int code, const std::string& m) {
     g_err = m;
   return code;
 }
-
-#define CK(call)                                                                       \
-  do {                                                                                 \
-    cudaError_t e_ = (call);                                                           \
-    if (e_ != cudaSuccess)                                                             \
-      return set_err(ctx, PLFBS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-// Device memory comes from one stream-ordered pool per device whose release
-// threshold is unbounded: plfbs_destroy returns a context's arrays to the pool
-// (no unmapping, which cost up to 0.8 s in a process's first frees) and the
-// next plfbs_create on that device reuses them. plfbs_release_cached trims it.
-std::mutex g_pool_mutex;
-cudaMemPool_t g_pools[plfbs::kMaxDevices] = {};
 
 cudaMemPool_t device_pool(int device) {
   std::lock_guard<std::mutex> g(g_pool_mutex);
@@ -89,10 +68,41 @@ cudaMemPool_t device_pool(int device) {
   return g_pools[device];
 }
 
-// Pinned host copies of the run status, recycled across contexts: freeing
-// pinned memory can stall for a long time on a busy host, so plfbs_destroy
-// returns the buffer here and only plfbs_release_cached frees them.
-std::vector<DevStats*> g_pinned_stats;
+int pool_alloc(plfbs_ctx* ctx, void** dst, size_t n) {
+  cudaMemPool_t pool = device_pool(ctx->device);
+  if (!pool) return set_err(ctx, PLFBS_ERR_CUDA, "device memory pool creation failed");
+  CK(cudaMallocFromPoolAsync(dst, n, pool, ctx->stream));
+  ctx->allocs.push_back(*dst);
+  ctx->bytes += (int64_t)n;
+  return PLFBS_OK;
+}
+
+int dev_alloc(plfbs_ctx* ctx, void** dst, size_t n) {
+  n = std::max<size_t>(n, 16);
+  int rc = pool_alloc(ctx, dst, n);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(*dst, 0, n, ctx->stream));
+  return PLFBS_OK;
+}
+
+int check_device(int device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0)
+    return set_err(nullptr, PLFBS_ERR_NO_DEVICE, "no CUDA device with that index");
+  // one attribute (cudaGetDeviceProperties fills every field and can be slow)
+  int major = 0;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess ||
+      major != 10)
+    return set_err(nullptr, PLFBS_ERR_NO_DEVICE,
+                   "this library is built for sm_100a (B200); device major != 10");
+  return PLFBS_OK;
+}
+
+}  // namespace plfbs_capi
+
+using namespace plfbs_capi;
+
+namespace {
 
 DevStats* take_pinned_stats() {
   {
@@ -112,41 +122,9 @@ void give_pinned_stats(DevStats* p) {
   g_pinned_stats.push_back(p);
 }
 
-int pool_alloc(plfbs_ctx* ctx, void** dst, size_t n) {
-  cudaMemPool_t pool = device_pool(ctx->device);
-  if (!pool) return set_err(ctx, PLFBS_ERR_CUDA, "device memory pool creation failed");
-  CK(cudaMallocFromPoolAsync(dst, n, pool, ctx->stream));
-  ctx->allocs.push_back(*dst);
-  ctx->bytes += (int64_t)n;
-  return PLFBS_OK;
-}
 
-// Pageable-source copies: cudaMemcpyAsync returns once `src` has been staged,
-// so the caller may release it afterwards.
-template <typename T>
-int dev_upload(plfbs_ctx* ctx, void** dst, const std::vector<T>& src) {
-  const size_t n = std::max<size_t>(src.size(), 1) * sizeof(T);
-  int rc = pool_alloc(ctx, dst, n);
-  if (rc) return rc;
-  if (!src.empty())
-    CK(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice,
-                       ctx->stream));
-  return PLFBS_OK;
-}
 
-int dev_alloc(plfbs_ctx* ctx, void** dst, size_t n) {
-  n = std::max<size_t>(n, 16);
-  int rc = pool_alloc(ctx, dst, n);
-  if (rc) return rc;
-  CK(cudaMemsetAsync(*dst, 0, n, ctx->stream));
-  return PLFBS_OK;
-}
 
-#define TRY(x)                \
-  do {                        \
-    int r_ = (x);             \
-    if (r_ != PLFBS_OK) return r_; \
-  } while (0)
 
 // One time step: IBM, then 4 x (gradient, flux, update) (Solver_gpu.cu:667-833).
 void enqueue_step(const KernelArgs& a, int prec, cudaStream_t s) {
@@ -264,218 +242,8 @@ int check_fault(plfbs_ctx* ctx) {
   return PLFBS_OK;
 }
 
-// Device memory that lives only while the layout is built: returned to the
-// pool (stream-ordered) when the builder returns, on every path.
-struct ScratchList {
-  plfbs_ctx* ctx;
-  std::vector<void*> v;
-  explicit ScratchList(plfbs_ctx* c) : ctx(c) {}
-  ~ScratchList() {
-    for (void* p : v) cudaFreeAsync(p, ctx->stream);
-  }
-  template <typename T>
-  int alloc(T** dst, size_t bytes, bool zero) {
-    cudaMemPool_t pool = device_pool(ctx->device);
-    if (!pool) return set_err(ctx, PLFBS_ERR_CUDA, "device memory pool creation failed");
-    void* p = nullptr;
-    CK(cudaMallocFromPoolAsync(&p, std::max<size_t>(bytes, 16), pool, ctx->stream));
-    v.push_back(p);
-    if (zero) CK(cudaMemsetAsync(p, 0, std::max<size_t>(bytes, 16), ctx->stream));
-    *dst = static_cast<T*>(p);
-    return PLFBS_OK;
-  }
-  template <typename T>
-  int upload(const T** dst, const T* src, size_t count) {
-    T* p = nullptr;
-    TRY(alloc(&p, count * sizeof(T), false));
-    if (count) CK(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
-    *dst = p;
-    return PLFBS_OK;
-  }
-};
 
-// The face, stencil and gather arrays of a context, built on the device from
-// the caller's mesh arrays (layout.cu); sets args' layout pointers, L.K2 and
-// the mesh fingerprint.
-int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
-  Layout& L = ctx->L;
-  KernelArgs& a = ctx->args;
-  const bool fp32 = ctx->cfg.precision == PLFBS_FP32_DEVIATION;
-  const size_t C = L.C, F = L.F, Fi = L.Fi, B = L.B, T = C + B;
-  const size_t nnz = (size_t)m.stencil_offsets[C];
-  const size_t nwin = (C + plfbs::kFaceWindow - 1) / plfbs::kFaceWindow;
-  const size_t es = fp32 ? sizeof(float) : sizeof(double);
-  ScratchList S(ctx);
-  plfbs::DevMesh d{};
-  d.C = L.C;
-  d.F = L.F;
-  d.Fi = L.Fi;
-  d.B = L.B;
-  TRY(S.upload(&d.owner, m.owner, F));
-  TRY(S.upload(&d.neighbour, m.neighbour, F));
-  TRY(S.upload(&d.area, m.face_area, F));
-  TRY(S.upload(&d.normal, m.face_normal, 3 * F));
-  TRY(S.upload(&d.fcen, m.face_centroid, 3 * F));
-  TRY(S.upload(&d.sdt, m.streaming_dt, F));
-  TRY(S.upload(&d.vol, m.cell_volume, C));
-  TRY(S.upload(&d.ccen, m.cell_centroid, 3 * T));
-  TRY(S.upload(&d.st_off, m.stencil_offsets, C + 1));
-  TRY(S.upload(&d.st_cells, m.stencil_cells, nnz));
-  TRY(S.upload(&d.st_faces, m.stencil_faces, nnz));
-  TRY(S.upload(&d.bc_new, L.bc_new_of_old.data(), B));
-  TRY(S.upload(&d.bc_old, L.bc_old_of_new.data(), B));
-  void* p = nullptr;
-  TRY(dev_upload(ctx, &p, L.cell_new_of_old));  // kept: the IBM kernels map caller cells with it
-  d.cell_new = static_cast<const int32_t*>(p);
-  plfbs::LayoutScratch s{};
-  TRY(S.alloc(&s.own_cnt, 4 * C, true));
-  TRY(S.alloc(&s.own_off, 4 * C, false));
-  TRY(S.alloc(&s.cursor, 4 * C, true));
-  TRY(S.alloc(&s.deg, 4 * C, true));
-  TRY(S.alloc(&s.gcnt, 4 * C, true));
-  TRY(S.alloc(&s.wsum, 4 * nwin, false));
-  TRY(S.alloc(&s.wbase, 4 * (nwin + 1), false));
-  TRY(S.alloc(&s.seg, 4 * Fi, false));
-  TRY(S.alloc(&s.sig, 2 * Fi, false));
-  TRY(S.alloc(&s.info, 4 * sizeof(int32_t), false));
-  TRY(S.alloc(&s.fingerprint, sizeof(unsigned long long), true));
-  const int32_t info0[4] = {L.C, 0, 0, 0};
-  CK(cudaMemcpyAsync(s.info, info0, sizeof info0, cudaMemcpyHostToDevice, ctx->stream));
 
-  TRY(pool_alloc(ctx, &p, 4 * F));
-  ctx->face_order = static_cast<int32_t*>(p);
-  TRY(pool_alloc(ctx, &p, 8 * F));
-  int32_t* face_ids = static_cast<int32_t*>(p);
-  void* face[3];
-  for (void*& f : face) TRY(pool_alloc(ctx, &f, 4 * es * F));
-  TRY(pool_alloc(ctx, &p, 4 * (size_t)L.K * C));
-  int32_t* st_nbr = static_cast<int32_t*>(p);
-  CK(cudaMemsetAsync(st_nbr, 0xff, 4 * (size_t)L.K * C, ctx->stream));
-  void* w[3];
-  for (void*& x : w) TRY(dev_alloc(ctx, &x, es * L.K * C));
-  void* inv_volume = nullptr;
-  TRY(pool_alloc(ctx, &inv_volume, es * C));
-
-  plfbs::launch_layout_order(d, s, ctx->face_order, ctx->stream);
-  plfbs::launch_layout_records(d, s, ctx->cfg.precision, ctx->cfg.gradient_mode,
-                               ctx->cfg.visc * 3, 1.0 / ctx->cfg.gamma, ctx->face_order, face_ids,
-                               face[0], face[1], face[2], st_nbr, w[0], w[1], w[2], inv_volume,
-                               ctx->stream);
-  CK(cudaGetLastError());
-  struct {
-    int32_t info[4];
-    unsigned long long fp;
-  } back;
-  CK(cudaMemcpyAsync(back.info, s.info, sizeof back.info, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaMemcpyAsync(&back.fp, s.fingerprint, sizeof back.fp, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  if (back.info[0] < L.C) {
-    std::ostringstream e;
-    e << "singular least-squares matrix for cell (index " << back.info[0] << ", value 0)";
-    return set_err(ctx, PLFBS_ERR_MESH, e.str());
-  }
-  L.K2 = back.info[1];
-  if (fp32 && L.K2 > 16)
-    return set_err(ctx, PLFBS_ERR_MESH, "the FP32 form handles cells with at most 16 faces");
-  TRY(pool_alloc(ctx, &p, 4 * (size_t)L.K2 * C));
-  int32_t* gather = static_cast<int32_t*>(p);
-  CK(cudaMemsetAsync(gather, 0xff, 4 * (size_t)L.K2 * C, ctx->stream));
-  plfbs::launch_layout_gather(d, s, face_ids, gather, ctx->stream);
-  CK(cudaGetLastError());
-  // sizes folded into the device's sum over the arrays
-  uint64_t h = back.fp;
-  for (int64_t v : {(int64_t)L.C, (int64_t)L.F, (int64_t)L.Fi}) h = (h ^ (uint64_t)v) * 1099511628211ull;
-  ctx->fingerprint = h;
-  a.K2 = L.K2;
-  a.face_ids = face_ids;
-  a.face0 = face[0];
-  a.face1 = face[1];
-  a.face2 = face[2];
-  a.st_nbr = st_nbr;
-  a.st_wx = w[0];
-  a.st_wy = w[1];
-  a.st_wz = w[2];
-  a.gather = gather;
-  a.inv_volume = inv_volume;
-  a.ibm_map = d.cell_new;
-  return PLFBS_OK;
-}
-
-// The compact layout: face records and cells' weight sets that are
-// bitwise equal are stored once (layout.cu, dedupe), each item keeping an
-// index. Used where a table holds at most 1/8 of the items (structured
-// regions of a mesh repeat their geometry); otherwise the kernels read the
-// per-item arrays. The per-item arrays stay for the other readers.
-int build_compact_layout(plfbs_ctx* ctx) {
-  Layout& L = ctx->L;
-  KernelArgs& a = ctx->args;
-  ctx->compact_faces = ctx->compact_cells = 0;
-  const int fp32 = ctx->cfg.precision == PLFBS_FP32_DEVIATION;
-  const size_t es = fp32 ? 4 : 8;
-  ScratchList S(ctx);
-  plfbs::RecordSource src[2];
-  src[0] = {0, L.F, 0, fp32, a.face0, a.face1, a.face2};
-  src[1] = {1, L.C, L.K, fp32, a.st_wx, a.st_wy, a.st_wz};
-  plfbs::DedupeScratch d[2];
-  int nwin[2];
-  for (int k = 0; k < 2; k++) {
-    const size_t n = (size_t)src[k].n;
-    int P = 1;
-    while ((size_t)P < 2 * n && P < (1 << 30)) P <<= 1;
-    nwin[k] = (int)((n + plfbs::kFaceWindow - 1) / plfbs::kFaceWindow);
-    d[k].P = P;
-    TRY(S.alloc(&d[k].slot_hash, 8 * (size_t)P, true));
-    TRY(S.alloc(&d[k].slot_rep, 4 * (size_t)P, false));
-    CK(cudaMemsetAsync(d[k].slot_rep, 0x7f, 4 * (size_t)P, ctx->stream));
-    TRY(S.alloc(&d[k].item_slot, 4 * n, false));
-    TRY(S.alloc(&d[k].rep_of, 4 * n, false));
-    TRY(S.alloc(&d[k].is_rep, 4 * n, false));
-    TRY(S.alloc(&d[k].off, 4 * n, false));
-    TRY(S.alloc(&d[k].wsum, 4 * (size_t)nwin[k], false));
-    TRY(S.alloc(&d[k].wbase, 4 * (size_t)(nwin[k] + 1), false));
-    TRY(S.alloc(&d[k].info, 16, true));
-    plfbs::launch_dedupe_scan(src[k], d[k], ctx->stream);
-  }
-  CK(cudaGetLastError());
-  int32_t unique[2], overflow[2];
-  for (int k = 0; k < 2; k++) {
-    CK(cudaMemcpyAsync(&unique[k], d[k].wbase + nwin[k], 4, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(&overflow[k], d[k].info, 4, cudaMemcpyDeviceToHost, ctx->stream));
-  }
-  CK(cudaStreamSynchronize(ctx->stream));
-  void* p = nullptr;
-  for (int k = 0; k < 2; k++) {
-    const int n = src[k].n, U = unique[k];
-    if (overflow[k] || U <= 0 || U > n / 8) continue;
-    TRY(pool_alloc(ctx, &p, 4 * (size_t)n));
-    int32_t* index = static_cast<int32_t*>(p);
-    if (k == 0) {
-      void* t[3];
-      for (void*& x : t) TRY(pool_alloc(ctx, &x, 4 * es * (size_t)U));
-      plfbs::launch_dedupe_emit(src[k], d[k], index, t[0], t[1], t[2], ctx->stream);
-      a.face_rec = index;
-      a.frec0 = t[0];
-      a.frec1 = t[1];
-      a.frec2 = t[2];
-      ctx->compact_faces = U;
-      if (!fp32) {
-        TRY(pool_alloc(ctx, &p, 4 * (size_t)U));
-        plfbs::launch_record_sides(t[0], t[1], U, ctx->cfg.flavour, static_cast<int32_t*>(p),
-                                   ctx->stream);
-        a.frec_sides = static_cast<const int32_t*>(p);
-      }
-    } else {
-      TRY(pool_alloc(ctx, &p, 3 * es * (size_t)U * L.K));
-      plfbs::launch_dedupe_emit(src[k], d[k], index, p, nullptr, nullptr, ctx->stream);
-      a.cell_wset = index;
-      a.wtab = p;
-      ctx->compact_cells = U;
-    }
-  }
-  CK(cudaGetLastError());
-  a.compact = (ctx->compact_faces || ctx->compact_cells) ? 1 : 0;
-  return PLFBS_OK;
-}
 
 int check_ctx(plfbs_ctx* ctx) {
   if (!ctx) return set_err(nullptr, PLFBS_ERR_ARG, "null context");
@@ -508,105 +276,7 @@ int plfbs_ls_weights(const plfbs_mesh_view* mesh, int32_t gradient_mode, double*
 
 }  // extern "C"
 
-namespace {
-
-int check_device(int device) {
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0)
-    return set_err(nullptr, PLFBS_ERR_NO_DEVICE, "no CUDA device with that index");
-  // one attribute (cudaGetDeviceProperties fills every field and can be slow)
-  int major = 0;
-  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess ||
-      major != 10)
-    return set_err(nullptr, PLFBS_ERR_NO_DEVICE,
-                   "this library is built for sm_100a (B200); device major != 10");
-  return PLFBS_OK;
-}
-
-int polymesh_geometry(plfbs_ctx* ctx, const plfbs_polymesh_view& pm, double ref_dt,
-                      plfbs_mesh_arrays& out) {
-  const size_t P = pm.n_points, F = pm.n_faces, Fi = pm.n_internal, C = pm.n_cells;
-  const size_t B = F - Fi, T = C + B, nnz = 2 * Fi + B;
-  const size_t nwin = (C + plfbs::kFaceWindow - 1) / plfbs::kFaceWindow;
-  ScratchList S(ctx);
-  plfbs::DevPolyMesh d{};
-  d.P = pm.n_points;
-  d.F = pm.n_faces;
-  d.Fi = pm.n_internal;
-  d.C = pm.n_cells;
-  TRY(S.upload(&d.points, pm.points, 3 * P));
-  TRY(S.upload(&d.face_offsets, pm.face_offsets, F + 1));
-  TRY(S.upload(&d.face_points, pm.face_points, (size_t)pm.face_offsets[F]));
-  TRY(S.upload(&d.owner, pm.owner, F));
-  TRY(S.upload(&d.neighbour, pm.neighbour, Fi));
-  plfbs::GeometryOut o{};
-  TRY(S.alloc(&o.area, 8 * F, false));
-  TRY(S.alloc(&o.normal, 24 * F, false));
-  TRY(S.alloc(&o.fcen, 24 * F, false));
-  TRY(S.alloc(&o.sdt, 8 * F, false));
-  TRY(S.alloc(&o.vol, 8 * T, false));
-  TRY(S.alloc(&o.ccen, 24 * T, false));
-  TRY(S.alloc(&o.st_off, 4 * (C + 1), false));
-  TRY(S.alloc(&o.st_cells, 4 * nnz, false));
-  TRY(S.alloc(&o.st_faces, 4 * nnz, false));
-  plfbs::GeometryScratch g{};
-  TRY(S.alloc(&g.fcsum, 24 * F, false));
-  TRY(S.alloc(&g.cnt, 4 * C, true));
-  TRY(S.alloc(&g.cursor, 4 * C, true));
-  TRY(S.alloc(&g.own_off, 4 * C, false));
-  TRY(S.alloc(&g.wsum, 4 * nwin, false));
-  TRY(S.alloc(&g.wbase, 4 * (nwin + 1), false));
-  TRY(S.alloc(&g.info, 16, true));
-  plfbs::launch_polymesh_geometry(d, ref_dt, o, g, ctx->stream);
-  CK(cudaGetLastError());
-  auto down = [&](void* dst, const void* src, size_t bytes) {
-    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
-  };
-  CK(down(out.face_area, o.area, 8 * F));
-  CK(down(out.face_normal, o.normal, 24 * F));
-  CK(down(out.face_centroid, o.fcen, 24 * F));
-  CK(down(out.streaming_dt, o.sdt, 8 * F));
-  CK(down(out.cell_volume, o.vol, 8 * T));
-  CK(down(out.cell_centroid, o.ccen, 24 * T));
-  CK(down(out.stencil_offsets, o.st_off, 4 * (C + 1)));
-  CK(down(out.stencil_cells, o.st_cells, 4 * nnz));
-  CK(down(out.stencil_faces, o.st_faces, 4 * nnz));
-  CK(cudaStreamSynchronize(ctx->stream));
-  std::memcpy(out.owner, pm.owner, 4 * F);
-  if (Fi) std::memcpy(out.neighbour, pm.neighbour, 4 * Fi);
-  for (size_t f = Fi; f < F; f++) out.neighbour[f] = (int32_t)(C + f - Fi);
-  return PLFBS_OK;
-}
-
-}  // namespace
-
 extern "C" {
-
-int plfbs_polymesh_geometry(const plfbs_polymesh_view* mesh, double visc, double gamma,
-                            double fneq_min, int32_t device, plfbs_mesh_arrays* out) {
-  if (!mesh || !out || !out->owner || !out->neighbour || !out->face_area || !out->face_normal ||
-      !out->face_centroid || !out->streaming_dt || !out->cell_volume || !out->cell_centroid ||
-      !out->stencil_offsets || !out->stencil_cells || !out->stencil_faces)
-    return set_err(nullptr, PLFBS_ERR_ARG, "null argument");
-  if (!std::isfinite(visc) || !(gamma > 0) || !std::isfinite(fneq_min))
-    return set_err(nullptr, PLFBS_ERR_ARG, "geometry needs finite visc, fneq_min and gamma > 0");
-  std::string err;
-  int rc = plfbs::validate_polymesh(*mesh, err);
-  if (rc) return set_err(nullptr, rc, err);
-  if ((rc = check_device(device))) return rc;
-  // calc_face_delta_t: the cap 3 nu / (gamma fneq_min) (none when fneq_min is 0)
-  const double ref_dt = fneq_min != 0 ? visc * 3 / gamma / fneq_min : HUGE_VAL;
-  plfbs_ctx tmp;
-  tmp.device = device;
-  if (cudaSetDevice(device) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking) != cudaSuccess)
-    return set_err(nullptr, PLFBS_ERR_CUDA, "stream creation failed");
-  rc = polymesh_geometry(&tmp, *mesh, ref_dt, *out);
-  cudaStreamSynchronize(tmp.stream);  // the scratch frees are stream-ordered
-  cudaStreamDestroy(tmp.stream);
-  if (rc) g_err = tmp.err;
-  return rc;
-}
 
 int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plfbs_bc_view* bc,
                  const plfbs_ibm_view* ibm, int device, plfbs_ctx** out) {

@@ -1,0 +1,93 @@
+// Internals shared by the C-ABI translation units (capi.cpp: context
+// lifetime, time step, state and checkpoints; capi_layout.cpp: the device
+// layout builders and the polyMesh geometry entry point).
+#ifndef PLFBS_CAPI_INTERNAL_HPP
+#define PLFBS_CAPI_INTERNAL_HPP
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "plfbs.h"
+#include "plfbs_internal.hpp"
+
+struct plfbs_ctx {
+  int device = 0;
+  plfbs_config cfg{};
+  plfbs::Layout L;
+  int N = 0;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t step_exec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  plfbs::KernelArgs args{};
+  std::vector<void*> allocs;
+  int64_t bytes = 0;
+  plfbs::DevStats* stats_host = nullptr;  // pinned copy of the stats header
+  long long stages_done = 0;       // stages run through plfbs_run_stages in the current step
+  bool debug = false;
+  bool have_state = false;
+  int* wall_buf = nullptr;   // device wall list of plfbs_wall_forces (grown on demand)
+  int wall_cap = 0;
+  uint64_t fingerprint = 0;  // of the caller's mesh, checked when a checkpoint is loaded
+  int32_t* face_order = nullptr;  // device [F]: caller face of each device face
+  plfbs::FluxMaps flux_maps{};    // tensor maps of the TMA-staged flux kernel (FP64)
+  int compact_faces = 0;          // unique face records in the compact layout (0: none)
+  int compact_cells = 0;          // unique cell weight sets in the compact layout (0: none)
+  bool flux_maps_ok = false;
+  std::string err;
+};
+
+namespace plfbs_capi {
+
+// Records `m` as the context's error (or the global one for a null context)
+// and returns `code`.
+int set_err(plfbs_ctx* c, int code, const std::string& m);
+
+// The per-device stream-ordered memory pool (created on first use).
+cudaMemPool_t device_pool(int device);
+int pool_alloc(plfbs_ctx* ctx, void** dst, size_t n);
+int dev_alloc(plfbs_ctx* ctx, void** dst, size_t n);
+
+// PLFBS_OK, or PLFBS_ERR_NO_DEVICE for a missing or non-sm_100 device.
+int check_device(int device);
+
+// The face, stencil and gather arrays of a context on the device, and the
+// compact layout (capi_layout.cpp).
+int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m);
+int build_compact_layout(plfbs_ctx* ctx);
+
+}  // namespace plfbs_capi
+
+#define CK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return plfbs_capi::set_err(ctx, PLFBS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define TRY(x)                \
+  do {                        \
+    int r_ = (x);             \
+    if (r_ != PLFBS_OK) return r_; \
+  } while (0)
+
+namespace plfbs_capi {
+
+// Pageable-source copies: cudaMemcpyAsync returns once `src` has been staged,
+// so the caller may release it afterwards.
+template <typename T>
+int dev_upload(plfbs_ctx* ctx, void** dst, const std::vector<T>& src) {
+  const size_t n = std::max<size_t>(src.size(), 1) * sizeof(T);
+  int rc = pool_alloc(ctx, dst, n);
+  if (rc) return rc;
+  if (!src.empty())
+    CK(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice,
+                       ctx->stream));
+  return PLFBS_OK;
+}
+
+}  // namespace plfbs_capi
+
+#endif  // PLFBS_CAPI_INTERNAL_HPP
