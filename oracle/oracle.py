@@ -35,7 +35,7 @@ class _Problem(C.Structure):
                 ("tolerance", C.c_double), ("origin", C.c_double * 3),
                 ("lengths", C.c_double * 3), ("n_nodes", C.c_int), ("object_nodes", C.c_int),
                 ("node_ref", _dp), ("stiffness", C.c_double), ("radius", C.c_double),
-                ("depth", C.c_double)]
+                ("depth", C.c_double), ("flavour", C.c_int)]
 
 
 class _State(C.Structure):
@@ -145,6 +145,7 @@ class OracleRun:
         p.stiffness = float(cfg.get("stiffness", 0.0))
         p.radius = float(cfg.get("radius", 1.0))
         p.depth = float(cfg.get("depth", 1.0))
+        p.flavour = int(cfg.get("flavour", 0))  # 1: the reference CPU Solver's tables
         self.p = p
 
         self.state = np.ascontiguousarray(state0, np.float64).reshape(C_ + B, 4).copy()

@@ -20,6 +20,15 @@
  * (LBFS.cu:1467), the +-0.001 dt dead band (LBFS.cu:353-354) and the Neumann
  * ghost gradient g (1 - |n|) (LBFS.cu:1366-1368).
  *
+ * flavour = 1 restates the reference's CPU Solver instead (src/Solver.cpp:88-590
+ * and 840-1274, gradients.cpp:395-506 and 592-648, Solution.cpp:759-833):
+ * boundary types rho 1, 2, 6, 7 and velocity 1, 2, 6, 8; Dirichlet ghost
+ * gradients along the face normal, Neumann g (1 - n); on boundary faces the
+ * owner's gradient on the owner side; lattice nodes on the strict sign of
+ * e . n (no dead band, e . n = 0 takes the owner side); body force
+ * -pressure_gradient; no IBM. Pinned against the CPU Solver's own final states
+ * (tests/golden/cpu_*.npz).
+ *
  * State layout: 4 doubles per cell (u, v, w, rho), cells then ghosts.
  */
 #include <math.h>
@@ -46,6 +55,7 @@ typedef struct {
   int n_nodes, object_nodes;
   const double *node_ref;                /* [3N] x_ref, y_ref, z_ref interleaved */
   double stiffness, radius, depth;
+  int flavour;                           /* 0: the GPU kernels; 1: the CPU Solver */
 } oracle_problem;
 
 typedef struct {
@@ -171,6 +181,26 @@ static void update_bcs(const oracle_problem *p, double *q) {
     int j = C + b, o = p->owner[Fi + b];
     const double *nbq = q + 4 * o, *bc = p->bc_value + 4 * b;
     double *g = q + 4 * j;
+    if (p->flavour == 1) { /* Solution::update_unstructured_bcs, Solution.cpp:759-833 */
+      int rt = p->bc_rho_type[b], vt = p->bc_vel_type[b];
+      if (rt == 1)
+        g[3] = bc[3] - (nbq[3] - bc[3]);
+      else if (rt == 2)
+        g[3] = nbq[3] + 0.0 * bc[3];
+      else if (rt == 6 || rt == 7)
+        g[3] = bc[3];
+      for (int c = 0; c < 3; c++) {
+        if (vt == 1)
+          g[c] = bc[c] - (nbq[c] - bc[c]);
+        else if (vt == 2)
+          g[c] = nbq[c] + 0.0 * bc[c];
+        else if (vt == 6)
+          g[c] = bc[c] * 1.0;
+        else if (vt == 8)
+          g[c] = c == 1 ? -nbq[c] : nbq[c];
+      }
+      continue;
+    }
     if (p->bc_rho_type[b] == 1)
       g[3] = bc[3] - (nbq[3] - bc[3]);
     else if (p->bc_rho_type[b] == 2)
@@ -221,6 +251,22 @@ static void bc_gradients(const oracle_problem *p, const double *q, double *grad)
     double dq[4] = {2 * (bc[3] - s[3]), 2 * (bc[0] - s[0]), 2 * (bc[1] - s[1]), 2 * (bc[2] - s[2])};
     double *gj = grad + 12 * j;
     const double *go = grad + 12 * o;
+    if (p->flavour == 1) { /* Get_LS_Gradients / get_ghost_grads, gradients.cpp:395-506,592-648 */
+      int rt = p->bc_rho_type[b], vt = p->bc_vel_type[b];
+      for (int c = 0; c < 3; c++) {
+        if (rt == 1) gj[c] = dq[0] / dmag * n[c];
+        else if (rt == 2) gj[c] = go[c] * (1 - n[c]);
+        else if (rt == 6) gj[c] = 0.0;
+        else if (rt == 7) gj[c] = go[c];
+      }
+      for (int f = 1; f < 4; f++)
+        for (int c = 0; c < 3; c++) {
+          if (vt == 1 || vt == 8) gj[3 * f + c] = dq[f] / dmag * n[c];
+          else if (vt == 2) gj[3 * f + c] = go[3 * f + c] * (1 - n[c]);
+          else if (vt == 6) gj[3 * f + c] = 0.0;
+        }
+      continue;
+    }
     if (p->bc_rho_type[b] == 1) {
       for (int c = 0; c < 3; c++) gj[c] = dq[0] / dmag * nv[c];
     } else if (p->bc_rho_type[b] == 2) {
@@ -266,10 +312,17 @@ static void face_fluxes(const oracle_problem *p, const double *q, const double *
         double v;
         if (f == 0)
           v = (rt == 1) ? bc[3] : qo[3] - dotv;
+        else if (p->flavour == 1) /* populate_lattice_macros, Solver.cpp:862-904 */
+          v = (vt == 1) ? bc[f - 1] : (vt == 8 ? (f == 2 ? 0.0 : qo[qi_idx[f]]) : qo[qi_idx[f]] - dotv);
         else
           v = (vt == 1 || vt == 9) ? bc[f - 1] : qo[qi_idx[f]] - dotv;
         centre[f] = side_i[f] = side_n[f] = v;
-        for (int c = 0; c < 3; c++) G1[f][c] = G2[f][c] = G3[f][c] = g2[3 * f + c];
+        /* the GPU kernels use the ghost gradient on both sides (LBFS.cu:398-401),
+           the CPU Solver the owner's on the owner side */
+        for (int c = 0; c < 3; c++) {
+          G2[f][c] = G3[f][c] = g2[3 * f + c];
+          G1[f][c] = p->flavour == 1 ? g1[3 * f + c] : g2[3 * f + c];
+        }
       }
     } else {
       for (int f = 0; f < 4; f++) {
@@ -295,7 +348,18 @@ static void face_fluxes(const oracle_problem *p, const double *q, const double *
         double ek_g1 = EX[k] * G1[f][0] + EY[k] * G1[f][1] + EZ[k] * G1[f][2];
         double ek_g2 = EX[k] * G2[f][0] + EY[k] * G2[f][1] + EZ[k] * G2[f][2];
         double ek_g3 = EX[k] * G3[f][0] + EY[k] * G3[f][1] + EZ[k] * G3[f][2];
-        if (s > d1) {
+        if (p->flavour == 1) { /* strict sign, Solver.cpp:929-1271 */
+          if (s > 0) {
+            lat[f][k] = side_i[f] - ek_g1 * dt;
+            lat[f][k + 1] = side_n[f] + ek_g2 * dt;
+          } else if (s < 0) {
+            lat[f][k] = side_n[f] - ek_g2 * dt;
+            lat[f][k + 1] = side_i[f] + ek_g1 * dt;
+          } else {
+            lat[f][k] = side_i[f] - ek_g1 * dt;
+            lat[f][k + 1] = side_i[f] + ek_g1 * dt;
+          }
+        } else if (s > d1) {
           lat[f][k] = side_i[f] - ek_g1 * dt;
           lat[f][k + 1] = side_n[f] + ek_g2 * dt;
         } else if (s < -d1) {
@@ -470,7 +534,14 @@ int oracle_run(const oracle_problem *p, oracle_state *s, int n_stages, int stop_
     int rk = s->stage % 4;
     if (rk == 0) {
       memcpy(s->t0, s->t1, sizeof(double) * 4 * (size_t)C);
-      ibm_step(p, s);
+      if (p->flavour == 1) { /* force = -pressure_gradient on u, Solver.cpp:213,410,424 */
+        for (int i = 0; i < C; i++) {
+          s->force[3 * i] = -p->pressure_gradient;
+          s->force[3 * i + 1] = s->force[3 * i + 2] = 0.0;
+        }
+      } else {
+        ibm_step(p, s);
+      }
     }
     update_bcs(p, s->state);
     memset(res, 0, sizeof(double) * 4 * (size_t)C);

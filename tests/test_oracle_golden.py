@@ -85,3 +85,19 @@ def test_oracle_full_run(name):
     assert rel_err(o.t1, g["final_t1"][: d["ma"].n_cells]) < 1e-14
     assert rel_err(o.history, g["history"]) < 1e-12
     assert rel_err(o.node_x, g["final_nodes"][:, 0:3]) < 1e-15
+
+
+@pytest.mark.parametrize("name", golden_cases.CPU_NAMES)
+def test_oracle_cpu_flavour_matches_the_cpu_solver(name):
+    """The oracle's CPU-Solver restatement (flavour 1) against the reference CPU
+    Solver's own final state (tests/golden/cpu_*.npz): 1e-10 per field."""
+    d = golden_cases.build_cpu(name)
+    g = load_golden(name)
+    rt, vt, val = cases.bc_arrays(d["ma"], d["case"])
+    cfg = dict(golden_cases.oracle_cfg(d), flavour=1)
+    o = oracle.OracleRun(d["ma"], rt, vt, val, cfg, d["state0"])
+    o.run_steps(int(g["steps"][0]))
+    C = d["ma"].n_cells
+    for k in range(4):
+        a, b = o.state[:C, k], g["final_state"][:C, k]
+        assert np.linalg.norm(a - b) <= 1e-10 * np.linalg.norm(b), k
