@@ -17,7 +17,7 @@ from plfbs import capi, cases
 pytestmark = pytest.mark.gpu
 
 STAGE_TOL = 1e-12   # one RK stage, max relative error
-RUN_TOL = 1e-10     # whole runs, relative L2 per field
+RUN_TOL = 1e-10     # whole runs, relative L2 per field (the parity bar)
 
 
 def _solver(d, renumber=0, **over):
