@@ -265,6 +265,22 @@ const char* plfbs_last_error(const plfbs_ctx* ctx) {
   return ctx ? ctx->err.c_str() : g_err.c_str();
 }
 
+int plfbs_cell_order(const plfbs_mesh_view* mesh, int32_t renumber, int32_t* order) {
+  if (!mesh || !order || !mesh->owner || !mesh->neighbour)
+    return set_err(nullptr, PLFBS_ERR_ARG, "null argument");
+  const int C = mesh->n_cells, F = mesh->n_faces, Fi = mesh->n_internal;
+  if (C <= 0 || F <= 0 || Fi < 0 || Fi > F || (renumber != 0 && renumber != 1))
+    return set_err(nullptr, PLFBS_ERR_ARG, "cell order needs valid sizes and renumber 0 or 1");
+  for (int f = 0; f < Fi; f++)
+    if (mesh->owner[f] < 0 || mesh->owner[f] >= C || mesh->neighbour[f] < 0 ||
+        mesh->neighbour[f] >= C)
+      return set_err(nullptr, PLFBS_ERR_MESH, "internal face cell out of range");
+  const std::vector<int32_t> o =
+      plfbs::cell_order(C, Fi, mesh->owner, mesh->neighbour, renumber);
+  std::memcpy(order, o.data(), sizeof(int32_t) * (size_t)C);
+  return PLFBS_OK;
+}
+
 int plfbs_ls_weights(const plfbs_mesh_view* mesh, int32_t gradient_mode, double* lhs_inv,
                      double* rhs) {
   if (!mesh || !lhs_inv || !rhs) return set_err(nullptr, PLFBS_ERR_ARG, "null argument");

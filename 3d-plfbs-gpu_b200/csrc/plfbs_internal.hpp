@@ -187,6 +187,11 @@ int ls_weights(const plfbs_mesh_view& m, int mode, double* lhs_inv, double* rhs,
 // The error string plfbs_last_error(NULL) returns (capi.cpp).
 void set_global_error(const std::string& m);
 
+// The cell order (order[new] = caller cell): identity, or RCM for renumber 1
+// (setup.cpp).
+std::vector<int32_t> cell_order(int C, int Fi, const int32_t* owner, const int32_t* nb,
+                                int renumber);
+
 // Validate the views, renumber the cells, order the boundary faces and build
 // their records (setup.cpp).
 int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bc,

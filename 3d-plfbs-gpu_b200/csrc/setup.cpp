@@ -252,6 +252,14 @@ int validate_polymesh(const plfbs_polymesh_view& pm, std::string& err) {
   return PLFBS_OK;
 }
 
+std::vector<int32_t> cell_order(int C, int Fi, const int32_t* owner, const int32_t* nb,
+                                int renumber) {
+  if (renumber == 1) return rcm_order(C, Fi, owner, nb);
+  std::vector<int32_t> order(C);
+  std::iota(order.begin(), order.end(), 0);
+  return order;
+}
+
 int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bcv,
                    Layout& L, std::string& err) {
   const int C = m.n_cells, F = m.n_faces, Fi = m.n_internal;
@@ -374,13 +382,8 @@ int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfb
   }
 
   // --- renumbering ---------------------------------------------------------
-  L.cell_old_of_new.resize(C);
+  L.cell_old_of_new = cell_order(C, Fi, m.owner, m.neighbour, cfg.renumber);
   L.cell_new_of_old.resize(C);
-  if (cfg.renumber == 1) {
-    L.cell_old_of_new = rcm_order(C, Fi, m.owner, m.neighbour);
-  } else {
-    std::iota(L.cell_old_of_new.begin(), L.cell_old_of_new.end(), 0);
-  }
   for (int i = 0; i < C; i++) L.cell_new_of_old[L.cell_old_of_new[i]] = i;
 
   // Boundary faces by new owner (stable). The internal faces are ordered on

@@ -32,7 +32,7 @@ EXPORTS = ("plfbs_create", "plfbs_set_state", "plfbs_run", "plfbs_get_state",
            "plfbs_residual_norms_noalloc", "plfbs_release_cached", "plfbs_warm_start",
            "plfbs_checkpoint_bytes", "plfbs_save_checkpoint", "plfbs_load_checkpoint",
            "plfbs_wall_forces", "plfbs_get_layout", "plfbs_polymesh_geometry",
-           "plfbs_set_flux_kernel", "plfbs_set_layout_compression")
+           "plfbs_set_flux_kernel", "plfbs_set_layout_compression", "plfbs_cell_order")
 
 
 class MeshView(C.Structure):
@@ -117,6 +117,7 @@ def lib():
         L.plfbs_get_layout.argtypes = [C.c_void_p, _ip, _ip, _ip, _ip, _dp, _ip]
         L.plfbs_set_flux_kernel.argtypes = [C.c_void_p, C.c_int32]
         L.plfbs_set_layout_compression.argtypes = [C.c_void_p, C.c_int32]
+        L.plfbs_cell_order.argtypes = [C.POINTER(MeshView), C.c_int32, _ip]
         L.plfbs_polymesh_geometry.argtypes = [C.POINTER(PolyMeshView), C.c_double, C.c_double,
                                               C.c_double, C.c_int32, C.POINTER(MeshOut)]
         L.plfbs_save_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
@@ -162,6 +163,17 @@ def mesh_view(ma, keep):
     v.stencil_cells = _i(k(ma.stencil_cells, np.int32))
     v.stencil_faces = _i(k(ma.stencil_faces, np.int32))
     return v
+
+
+def cell_order(ma, renumber):
+    """Host-only: the cell order plfbs_create uses (order[new] = caller cell)."""
+    keep = []
+    v = mesh_view(ma, keep)
+    order = np.zeros(ma.n_cells, np.int32)
+    rc = lib().plfbs_cell_order(C.byref(v), int(renumber), _i(order))
+    if rc:
+        raise PlfbsError(rc, lib().plfbs_last_error(None).decode())
+    return order
 
 
 def ls_weights(ma, mode):

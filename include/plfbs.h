@@ -286,6 +286,12 @@ int plfbs_get_residual(plfbs_ctx* ctx, double* res, int32_t n_cells);
 int plfbs_get_layout(plfbs_ctx* ctx, int32_t* sizes, int32_t* cell_order, int32_t* face_order,
                      int32_t* stencil_nbr, double* stencil_w, int32_t* gather);
 
+/* Host-only: the cell order plfbs_create uses (order[new] = caller cell): the
+ * identity for renumber 0, reverse Cuthill-McKee over the internal faces for
+ * renumber 1 (start cells by ascending degree, neighbours by ascending degree,
+ * both stable). Needs owner, neighbour and the sizes of `mesh` only. */
+int plfbs_cell_order(const plfbs_mesh_view* mesh, int32_t renumber, int32_t* order);
+
 /* Host-only: the least-squares weights as gradients::pre_fill_LHS_and_RHS_matrix
  * computes them (gradients.cpp:214-313, determinant as written at :282-284):
  * lhs_inv [9C] row-major, rhs [3 nnz] per stencil entry. No GPU needed. */

@@ -48,3 +48,15 @@ def test_layout_oracle_is_consistent(name, ma):
         assert ((st >= -1) & (st < C + (F - Fi))).all()
         filled = st >= 0
         assert (filled[:-1] | ~filled[1:]).all()  # empty slots only at the end of a cell's list
+
+
+@pytest.mark.parametrize("name,ma", list(_meshes()), ids=lambda v: v if isinstance(v, str) else "")
+def test_library_cell_order_matches_the_oracle(plfbs_lib, name, ma):
+    """plfbs_cell_order (the order plfbs_create renumbers with) against the numpy
+    restatement of RCM; renumber 0 is the identity."""
+    want = layout_oracle.rcm_order(ma.n_cells, ma.n_internal, np.asarray(ma.owner),
+                                   np.asarray(ma.neighbour))
+    np.testing.assert_array_equal(capi.cell_order(ma, 1), want)
+    np.testing.assert_array_equal(capi.cell_order(ma, 0), np.arange(ma.n_cells))
+    with pytest.raises(capi.PlfbsError):
+        capi.cell_order(ma, 2)
