@@ -296,6 +296,7 @@ extern "C" {
 
 int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plfbs_bc_view* bc,
                  const plfbs_ibm_view* ibm, int device, plfbs_ctx** out) {
+  NvtxRange range("plfbs_create");
   if (!cfg || !mesh || !bc || !out) return set_err(nullptr, PLFBS_ERR_ARG, "null argument");
   *out = nullptr;
   if (cfg->precision != PLFBS_FP64 && cfg->precision != PLFBS_FP32_DEVIATION)
@@ -315,7 +316,11 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   ctx->device = device;
   ctx->cfg = *cfg;
   std::string err;
-  int rc = plfbs::prepare_layout(*cfg, *mesh, *bc, ctx->L, err);
+  int rc;
+  {
+    NvtxRange r("prepare_layout (host)");
+    rc = plfbs::prepare_layout(*cfg, *mesh, *bc, ctx->L, err);
+  }
   if (rc) {
     delete ctx;
     return set_err(nullptr, rc, err);
@@ -403,8 +408,14 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
                         encode_rows(&ctx->flux_maps.grad, a.grad, 12, L.C);
   if ((rc = dev_alloc(ctx, &p, (size_t)L.F * e4))) return fail(rc);
   a.flux = p;
-  if ((rc = build_device_layout(ctx, *mesh))) return fail(rc);
-  if ((rc = build_compact_layout(ctx))) return fail(rc);
+  {
+    NvtxRange r("device layout");
+    if ((rc = build_device_layout(ctx, *mesh))) return fail(rc);
+  }
+  {
+    NvtxRange r("compact layout");
+    if ((rc = build_compact_layout(ctx))) return fail(rc);
+  }
   if (fp32) {
     plfbs::BoundaryRecords32 b32;
     plfbs::boundary_records32(L, cfg->ref_rho, cfg->max_velocity, b32);
@@ -486,6 +497,7 @@ void plfbs_destroy(plfbs_ctx* ctx) {
 
 int plfbs_wall_forces(plfbs_ctx* ctx, const int32_t* wall_bc, int32_t n_wall, double* cd,
                       double* cl) {
+  NvtxRange range("plfbs_wall_forces");
   TRY(check_ctx(ctx));
   if (!cd || !cl || n_wall < 0 || (n_wall > 0 && !wall_bc))
     return set_err(ctx, PLFBS_ERR_ARG, "wall_forces needs the wall list and two outputs");
@@ -564,6 +576,7 @@ namespace {
 // deviation units), resets the run status and seeds the RK accumulators.
 int seed_state(plfbs_ctx* ctx, const double* rho, const double* u, const double* v,
                const double* w, bool conserved) {
+  NvtxRange range(conserved ? "plfbs_warm_start" : "plfbs_set_state");
   const Layout& L = ctx->L;
   const int64_t T = (int64_t)L.C + L.B;
   if (ctx->cfg.precision == PLFBS_FP32_DEVIATION) {
@@ -676,6 +689,7 @@ int plfbs_checkpoint_bytes(plfbs_ctx* ctx, int64_t* bytes) {
 }
 
 int plfbs_save_checkpoint(plfbs_ctx* ctx, void* buf, int64_t bytes) {
+  NvtxRange range("plfbs_save_checkpoint");
   TRY(check_ctx(ctx));
   if (!buf || bytes < checkpoint_size(ctx))
     return set_err(ctx, PLFBS_ERR_ARG, "checkpoint buffer smaller than plfbs_checkpoint_bytes");
@@ -727,6 +741,7 @@ int plfbs_save_checkpoint(plfbs_ctx* ctx, void* buf, int64_t bytes) {
 }
 
 int plfbs_load_checkpoint(plfbs_ctx* ctx, const void* buf, int64_t bytes) {
+  NvtxRange range("plfbs_load_checkpoint");
   TRY(check_ctx(ctx));
   if (!buf || bytes < (int64_t)sizeof(CheckpointHeader))
     return set_err(ctx, PLFBS_ERR_ARG, "checkpoint buffer too small");
@@ -786,6 +801,7 @@ int plfbs_load_checkpoint(plfbs_ctx* ctx, const void* buf, int64_t bytes) {
 }
 
 int plfbs_run(plfbs_ctx* ctx, int64_t max_steps, plfbs_stats* stats, double* history) {
+  NvtxRange range("plfbs_run");
   TRY(check_ctx(ctx));
   if (!ctx->have_state) return set_err(ctx, PLFBS_ERR_STATE, "run before set_state");
   if (ctx->stages_done != 0)
@@ -799,6 +815,7 @@ int plfbs_run(plfbs_ctx* ctx, int64_t max_steps, plfbs_stats* stats, double* his
   bool halt = ctx->stats_host->halt != 0;
   while (done < max_steps && !halt) {
     const long long n = std::min<long long>(batch, max_steps - done);
+    NvtxRange r("step batch");
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     for (long long k = 0; k < n; k++) CK(cudaGraphLaunch(ctx->step_exec, ctx->stream));
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
@@ -872,6 +889,7 @@ int plfbs_set_flux_kernel(plfbs_ctx* ctx, int32_t kind) {
 
 int plfbs_get_state(plfbs_ctx* ctx, double* rho, double* u, double* v, double* w,
                     int64_t n_total) {
+  NvtxRange range("plfbs_get_state");
   TRY(check_ctx(ctx));
   const Layout& L = ctx->L;
   const int64_t T = (int64_t)L.C + L.B;

@@ -5,6 +5,7 @@
 #define PLFBS_CAPI_INTERNAL_HPP
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <string>
@@ -40,6 +41,15 @@ struct plfbs_ctx {
 };
 
 namespace plfbs_capi {
+
+// A named NVTX range over a scope (visible to Nsight Systems and ncu; without a
+// tool attached the calls return at once).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Records `m` as the context's error (or the global one for a null context)
 // and returns `code`.

@@ -297,6 +297,7 @@ extern "C" {
 
 int plfbs_polymesh_geometry(const plfbs_polymesh_view* mesh, double visc, double gamma,
                             double fneq_min, int32_t device, plfbs_mesh_arrays* out) {
+  plfbs_capi::NvtxRange range("plfbs_polymesh_geometry");
   if (!mesh || !out || !out->owner || !out->neighbour || !out->face_area || !out->face_normal ||
       !out->face_centroid || !out->streaming_dt || !out->cell_volume || !out->cell_centroid ||
       !out->stencil_offsets || !out->stencil_cells || !out->stencil_faces)
