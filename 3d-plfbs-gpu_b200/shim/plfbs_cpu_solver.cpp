@@ -91,6 +91,8 @@ void Solver::General_Purpose_Solver_mk_i(unstructured_mesh& Mesh, Solution& soln
   }
 
   std::ofstream error_output((globals.output_file + "/error.txt").c_str(), std::ios::out);
+  plfbs_shim::RunLog run_log(globals.output_file + "/run.jsonl", Mesh.get_n_cells());
+  const char* exit_kind = "out_of_time";
   tecplot_output<double> tecplot;
   Solution residual_worker(T), temp_soln(T);
   gradients grads(T);
@@ -121,6 +123,7 @@ void Solver::General_Purpose_Solver_mk_i(unstructured_mesh& Mesh, Solution& soln
     const long long last = t + ran - 1;
     if (mg == 0 && last % out_step == 1 && ran > 0) {  // Solver.cpp:501-515
       pull();
+      run_log.step(last, st);
       error_output << last << ", " << st.max_error << ", " << st.rho_rms << ", " << st.u_rms
                    << ", " << st.v_rms << ", " << st.w_rms << " , FMG cycle: " << fmg << std::endl;
       std::cout << "time t=" << last * delta_t << " error e =" << st.max_error
@@ -134,12 +137,14 @@ void Solver::General_Purpose_Solver_mk_i(unstructured_mesh& Mesh, Solution& soln
       }
     }
     t += ran;
-    if (rc == PLFBS_ERR_DIVERGED) {  // the NaN / rho > 1000 exits, Solver.cpp:448-490
+    if (rc == PLFBS_ERR_DIVERGED) {
+      exit_kind = "diverged";  // the NaN / rho > 1000 exits, Solver.cpp:448-490
       plfbs_shim::report(ctx, "time step", rc);
       break;
     }
     if (st.converged) {
       converged = true;
+      exit_kind = "converged";
       break;
     }
     if (ran < n) break;
@@ -167,6 +172,7 @@ void Solver::General_Purpose_Solver_mk_i(unstructured_mesh& Mesh, Solution& soln
                                              residual_worker, delta_t_local.data(),
                                              local_fneq.data());
   }
+  run_log.end(exit_kind, t, pp.drag_coef, pp.lift_coef);
   // lossless copy of the final state (the text output keeps 6 digits)
   if (FILE* f = std::fopen((globals.output_file + "/state.bin").c_str(), "wb")) {
     std::fwrite(rho.data(), sizeof(double), T, f);

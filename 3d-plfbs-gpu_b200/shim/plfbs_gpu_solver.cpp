@@ -103,6 +103,8 @@ void gpu_solver::General_Purpose_Solver_mk_i(
   }
 
   std::ofstream error_output((globals.output_file + "/error.txt").c_str(), std::ios::out);
+  plfbs_shim::RunLog run_log(globals.output_file + "/run.jsonl", Mesh.get_n_cells());
+  const char* exit_kind = "out_of_time";
   tecplot_output<double> tecplot;
   Solution residual_worker(T);
   gradients grads(T);
@@ -151,6 +153,7 @@ void gpu_solver::General_Purpose_Solver_mk_i(
     const double max_error = st.max_error;
     if (mg == 0 && last % out_step == 1 && ran > 0) {  // Solver_gpu.cu:844-868
       pull();
+      run_log.step(last, st);
       error_output << last << ", " << max_error << ", " << st.rho_rms << ", " << st.u_rms << ", "
                    << st.v_rms << ", " << st.w_rms << " , FMG cycle: " << fmg << std::endl;
       std::cout << "time t=" << last * delta_t << " error e =" << max_error
@@ -166,11 +169,13 @@ void gpu_solver::General_Purpose_Solver_mk_i(
     }
     t += ran;
     if (rc == PLFBS_ERR_DIVERGED) {
+      exit_kind = "diverged";
       report(ctx, "time step", rc);
       break;
     }
     if (st.converged) {  // Solver_gpu.cu:870-895
       converged = true;
+      exit_kind = "converged";
       break;
     }
     if (ran < n) break;
@@ -197,6 +202,7 @@ void gpu_solver::General_Purpose_Solver_mk_i(
                                              local_fneq.data());
     output_objects((double)timesteps);
   }
+  run_log.end(exit_kind, t, pp.drag_coef, pp.lift_coef);
   // lossless checkpoint of the final state (the text output keeps 6 digits)
   if (FILE* f = std::fopen((globals.output_file + "/state.bin").c_str(), "wb")) {
     std::fwrite(rho.data(), sizeof(double), T, f);

@@ -6,6 +6,8 @@
 #ifndef PLFBS_SHIM_COMMON_HPP
 #define PLFBS_SHIM_COMMON_HPP
 
+#include <cmath>
+#include <cstdio>
 #include <iostream>
 #include <string>
 #include <vector>
@@ -120,6 +122,49 @@ inline plfbs_config config(global_variables& globals, domain_geometry& domain,
   cfg.flavour = flavour;
   return cfg;
 }
+
+// JSON-lines run log, <output_file>/run.jsonl: one record per output step
+// (the residual norms the reference writes to error.txt, plus the device time
+// of the steps since the previous record and the throughput they give) and a
+// last record with the exit and the wall drag and lift coefficients.
+class RunLog {
+ public:
+  RunLog(const std::string& path, long long cells) : f_(std::fopen(path.c_str(), "w")), cells_(cells) {}
+  ~RunLog() {
+    if (f_) std::fclose(f_);
+  }
+  RunLog(const RunLog&) = delete;
+  RunLog& operator=(const RunLog&) = delete;
+  void step(long long t, const plfbs_stats& st) {
+    if (!f_) return;
+    const double mcups = st.kernel_ms > 0 ? (double)cells_ * st.steps_run / (st.kernel_ms * 1e3) : 0.0;
+    std::fprintf(f_,
+                 "{\"step\": %lld, \"max_error\": %s, \"rho_rms\": %s, \"u_rms\": %s, "
+                 "\"v_rms\": %s, \"w_rms\": %s, \"steps_run\": %lld, \"kernel_ms\": %s, "
+                 "\"mcell_updates_per_s\": %s}\n",
+                 t, num(st.max_error).c_str(), num(st.rho_rms).c_str(), num(st.u_rms).c_str(),
+                 num(st.v_rms).c_str(), num(st.w_rms).c_str(), (long long)st.steps_run,
+                 num(st.kernel_ms).c_str(), num(mcups).c_str());
+    std::fflush(f_);
+  }
+  void end(const char* exit, long long steps, double cd, double cl) {
+    if (!f_) return;
+    std::fprintf(f_, "{\"exit\": \"%s\", \"steps\": %lld, \"cd\": %s, \"cl\": %s}\n", exit,
+                 steps, num(cd).c_str(), num(cl).c_str());
+    std::fflush(f_);
+  }
+
+ private:
+  // JSON has no NaN or infinity: those are written as null
+  static std::string num(double v) {
+    if (!std::isfinite(v)) return "null";
+    char b[32];
+    std::snprintf(b, sizeof b, "%.17g", v);
+    return b;
+  }
+  FILE* f_;
+  long long cells_;
+};
 
 }  // namespace plfbs_shim
 

@@ -5,6 +5,7 @@ oracle/_ref/plfbs_ref_b200 and plfbs_ref_cpu_b200 (built from the reference
 sources by `make -C oracle/ref integration`); skipped without them."""
 
 import glob
+import json
 import os
 
 import numpy as np
@@ -18,6 +19,15 @@ pytestmark = pytest.mark.gpu
 
 BIN = os.path.join(REPO, "oracle", "_ref", "plfbs_ref_b200")
 BIN_CPU = os.path.join(REPO, "oracle", "_ref", "plfbs_ref_cpu_b200")
+
+
+def _check_run_log(tmp_path):
+    """The shim's JSON-lines run log: one record per output step, the exit last."""
+    paths = glob.glob(os.path.join(str(tmp_path), "out", "*", "run.jsonl"))
+    assert len(paths) == 1, paths
+    recs = [json.loads(line) for line in open(paths[0]) if line.strip()]
+    assert recs and recs[-1]["exit"] in ("converged", "out_of_time", "diverged")
+    assert all("max_error" in r for r in recs[:-1])
 
 
 @pytest.mark.parametrize("name", ["cavity", "channel", "converge"])
@@ -35,6 +45,7 @@ def test_reference_program_with_plfbs(tmp_path, name):
     state = np.stack([raw[1], raw[2], raw[3], raw[0]], axis=1)
     for k in range(4):
         assert rel_l2(state[:, k], g["final_state"][:, k]) < 1e-10, k
+    _check_run_log(tmp_path)
     # the reference's 6-significant-digit text output agrees too on interior
     # cells (after a converged exit the host re-applies its CPU boundary update
     # to the ghosts before writing, Solver_gpu.cu:882, as the reference does)
@@ -61,6 +72,7 @@ def test_reference_program_with_plfbs_cpu_solver(tmp_path, name):
     state = np.stack([raw[1], raw[2], raw[3], raw[0]], axis=1)
     for k in range(4):
         assert rel_l2(state[:C, k], g["final_state"][:C, k]) < 1e-10, k
+    _check_run_log(tmp_path)
     u_txt = glob.glob(os.path.join(str(tmp_path), "out", "*", "u.txt"))[0]
     u = np.loadtxt(u_txt, delimiter=",")[:, 1]
     np.testing.assert_allclose(u[:C], g["final_state"][:C, 0], rtol=1e-5, atol=1e-9)
