@@ -269,8 +269,8 @@ int plfbs_cell_order(const plfbs_mesh_view* mesh, int32_t renumber, int32_t* ord
   if (!mesh || !order || !mesh->owner || !mesh->neighbour)
     return set_err(nullptr, PLFBS_ERR_ARG, "null argument");
   const int C = mesh->n_cells, F = mesh->n_faces, Fi = mesh->n_internal;
-  if (C <= 0 || F <= 0 || Fi < 0 || Fi > F || (renumber != 0 && renumber != 1))
-    return set_err(nullptr, PLFBS_ERR_ARG, "cell order needs valid sizes and renumber 0 or 1");
+  if (C <= 0 || F <= 0 || Fi < 0 || Fi > F || renumber < 0 || renumber > 2)
+    return set_err(nullptr, PLFBS_ERR_ARG, "cell order needs valid sizes and renumber 0, 1 or 2");
   for (int f = 0; f < Fi; f++)
     if (mesh->owner[f] < 0 || mesh->owner[f] >= C || mesh->neighbour[f] < 0 ||
         mesh->neighbour[f] >= C)
@@ -303,6 +303,8 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     return set_err(nullptr, PLFBS_ERR_ARG, "unknown precision mode");
   if (cfg->flavour != PLFBS_FLAVOUR_GPU && cfg->flavour != PLFBS_FLAVOUR_CPU_SOLVER)
     return set_err(nullptr, PLFBS_ERR_ARG, "unknown flavour");
+  if (cfg->renumber < 0 || cfg->renumber > 2)
+    return set_err(nullptr, PLFBS_ERR_ARG, "renumber must be 0, 1 or 2");
   if (cfg->flavour == PLFBS_FLAVOUR_CPU_SOLVER &&
       (cfg->precision != PLFBS_FP64 || (ibm && ibm->n_nodes > 0)))
     return set_err(nullptr, PLFBS_ERR_ARG,
@@ -362,6 +364,13 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     return fail(set_err(ctx, PLFBS_ERR_CUDA, "stream/event creation failed"));
   if (!(ctx->stats_host = take_pinned_stats()))
     return fail(set_err(ctx, PLFBS_ERR_CUDA, "cudaMallocHost failed"));
+  if (cfg->renumber == 2) {  // the order on the device, then the host's order-dependent part
+    NvtxRange r("device cell order");
+    std::vector<int32_t> order;
+    if ((rc = device_cell_order(ctx, *mesh, order))) return fail(rc);
+    if ((rc = plfbs::order_layout(*cfg, *mesh, *bc, std::move(order), ctx->L, err)))
+      return fail(set_err(ctx, rc, err));
+  }
 
   KernelArgs& a = ctx->args;
   const long long T = (long long)L.C + L.B;

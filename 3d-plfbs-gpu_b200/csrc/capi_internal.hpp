@@ -68,6 +68,10 @@ int check_device(int device);
 int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m);
 int build_compact_layout(plfbs_ctx* ctx);
 
+// The renumber-1 cell order (reverse Cuthill-McKee, order[new] = caller cell)
+// built on the device (renumber 2; capi_layout.cpp).
+int device_cell_order(plfbs_ctx* ctx, const plfbs_mesh_view& m, std::vector<int32_t>& order);
+
 }  // namespace plfbs_capi
 
 #define CK(call)                                                                       \

@@ -154,6 +154,84 @@ int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
   return PLFBS_OK;
 }
 
+// Components (beyond the cells without internal faces) the device order
+// starts one at a time; a mesh in more pieces takes the host order, which is
+// the same order.
+constexpr int kMaxDeviceComponents = 256;
+
+int device_cell_order(plfbs_ctx* ctx, const plfbs_mesh_view& m, std::vector<int32_t>& order) {
+  const int C = ctx->L.C, Fi = ctx->L.Fi;
+  const size_t nwin = (C + plfbs::kFaceWindow - 1) / plfbs::kFaceWindow;
+  ScratchList S(ctx);
+  plfbs::RcmDev r{};
+  r.C = C;
+  r.Fi = Fi;
+  TRY(S.upload(&r.owner, m.owner, Fi));
+  TRY(S.upload(&r.neighbour, m.neighbour, Fi));
+  TRY(S.alloc(&r.deg, 4 * (size_t)C, true));
+  TRY(S.alloc(&r.cursor, 4 * (size_t)C, true));
+  TRY(S.alloc(&r.cnt, 4 * (size_t)C, false));
+  TRY(S.alloc(&r.win_off, 4 * (size_t)C, false));
+  TRY(S.alloc(&r.wsum, 4 * nwin, false));
+  TRY(S.alloc(&r.wbase, 4 * (nwin + 1), false));
+  TRY(S.alloc(&r.off, 4 * ((size_t)C + 1), false));
+  TRY(S.alloc(&r.adj_key, 16 * (size_t)Fi, false));
+  TRY(S.alloc(&r.adj, 8 * (size_t)Fi, false));
+  TRY(S.alloc(&r.pos, 4 * (size_t)C, false));
+  TRY(S.alloc(&r.key, 8 * (size_t)C, false));
+  TRY(S.alloc(&r.order, 4 * (size_t)C, true));
+  TRY(S.alloc(&r.start, 8, false));
+  TRY(S.alloc(&r.info, 16, true));
+  CK(cudaMemsetAsync(r.pos, 0xff, 4 * (size_t)C, ctx->stream));
+  CK(cudaMemsetAsync(r.key, 0xff, 8 * (size_t)C, ctx->stream));
+  CK(cudaMemsetAsync(r.start, 0xff, 8, ctx->stream));
+  // the total of the last window scan over n items
+  auto scan_total = [&](int n, int& v) -> int {
+    const size_t w = (n + plfbs::kFaceWindow - 1) / plfbs::kFaceWindow;
+    CK(cudaMemcpyAsync(&v, r.wbase + w, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PLFBS_OK;
+  };
+  plfbs::launch_rcm_graph(r, ctx->stream);
+  CK(cudaGetLastError());
+  int hi = 0;  // cells placed so far
+  TRY(scan_total(C, hi));
+  if (hi < 0 || hi > C) return set_err(ctx, PLFBS_ERR_CUDA, "device cell order: bad count");
+  for (int comp = 0; hi < C; comp++) {
+    if (comp == kMaxDeviceComponents) {
+      order = plfbs::cell_order(C, Fi, m.owner, m.neighbour, 1);
+      return PLFBS_OK;
+    }
+    plfbs::launch_rcm_start(r, hi, ctx->stream);
+    int lo = hi++;
+    while (lo < hi) {  // one level per pass; every pass places cells or ends the piece
+      plfbs::launch_rcm_level(r, lo, hi, ctx->stream);
+      CK(cudaGetLastError());
+      int n = 0;
+      TRY(scan_total(hi - lo, n));
+      if (n < 0 || n > C - hi)
+        return set_err(ctx, PLFBS_ERR_CUDA, "device cell order: level size out of range");
+      lo = hi;
+      hi += n;
+    }
+  }
+  int32_t info[4];
+  order.resize(C);
+  CK(cudaMemcpyAsync(order.data(), r.order, 4 * (size_t)C, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(info, r.info, sizeof info, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (info[2] != 0)
+    return set_err(ctx, PLFBS_ERR_CUDA, "device cell order: placements out of range");
+  std::reverse(order.begin(), order.end());
+  std::vector<char> seen(C, 0);  // a permutation before anything is indexed with it
+  for (int c : order) {
+    if (c < 0 || c >= C || seen[c])
+      return set_err(ctx, PLFBS_ERR_CUDA, "device cell order is not a permutation");
+    seen[c] = 1;
+  }
+  return PLFBS_OK;
+}
+
 // The compact layout: face records and cells' weight sets that are
 // bitwise equal are stored once (layout.cu, dedupe), each item keeping an
 // index. Used where a table holds at most 1/8 of the items (structured

@@ -3,9 +3,10 @@
 // gather, inverse volumes and the mesh fingerprint; and the mesh arrays
 // themselves from a raw polyMesh (plfbs_polymesh_geometry).
 //
-// The host keeps validation, the cell renumbering (RCM is a sequential
-// breadth-first search) and the boundary records (a few percent of the
-// faces); everything O(faces) or O(stencil entries) happens here. The result
+// The host keeps validation, the boundary records (a few percent of the
+// faces) and, for renumber 1, the cell renumbering (a sequential breadth-first
+// search; renumber 2 builds the same order here, level by level); everything
+// O(faces) or O(stencil entries) happens here. The result
 // is bit-identical to evaluating the same formulas on the host: this file is
 // compiled without FMA contraction (-fmad=false), uses x * x where the
 // reference writes pow(x, 2.0) (which gcc also folds to one multiply), and
@@ -13,6 +14,7 @@
 #include <cstdint>
 
 #include "plfbs_internal.hpp"
+#include "rcm_levels.hpp"
 
 namespace plfbs {
 namespace {
@@ -642,6 +644,116 @@ __global__ void k_dedupe_emit(const RecordSource r, const int32_t* rep_of, const
   }
 }
 
+// --- Cuthill-McKee order by breadth-first levels (renumber 2) ---------------
+// The per-thread steps are rcm_levels.hpp's; the host drives one level at a
+// time (capi_layout.cpp device_cell_order). Index checks that fail count in
+// info[2] instead of touching memory.
+
+__device__ __forceinline__ rcm::Graph rcm_graph(const RcmDev& r) {
+  return rcm::Graph{r.C, r.off, r.adj, r.deg};
+}
+
+__global__ void k_rcm_degree(const RcmDev r) {
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < r.Fi; f += gridDim.x * blockDim.x) {
+    atomicAdd(&r.deg[r.owner[f]], 1);
+    atomicAdd(&r.deg[r.neighbour[f]], 1);
+  }
+}
+
+// Each internal face into both cells' adjacency (arbitrary order within a cell).
+__global__ void k_rcm_scatter(const RcmDev r) {
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < r.Fi; f += gridDim.x * blockDim.x) {
+    const int o = r.owner[f], n = r.neighbour[f];
+    r.adj_key[r.off[o] + atomicAdd(&r.cursor[o], 1)] = rcm::adj_entry(f, n);
+    r.adj_key[r.off[n] + atomicAdd(&r.cursor[n], 1)] = rcm::adj_entry(f, o);
+  }
+}
+
+// Each cell's adjacency into face order.
+__global__ void k_rcm_sort(const RcmDev r) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < r.C; c += gridDim.x * blockDim.x) {
+    const int e0 = r.off[c], e1 = r.off[c + 1];
+    rcm::sort_entries(r.adj_key + e0, e1 - e0);
+    for (int e = e0; e < e1; e++) r.adj[e] = (int32_t)(r.adj_key[e] & 0xffffffffu);
+  }
+}
+
+__global__ void k_rcm_isolated(const RcmDev r) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < r.C; c += gridDim.x * blockDim.x)
+    r.cnt[c] = r.deg[c] == 0 ? 1 : 0;
+}
+
+// Cells without internal faces first, by index (the window scan of the flags).
+__global__ void k_rcm_place_isolated(const RcmDev r) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < r.C; c += gridDim.x * blockDim.x) {
+    if (r.deg[c] != 0) continue;
+    const int q = r.wbase[c / kFaceWindow] + r.win_off[c];
+    r.order[q] = c;
+    r.pos[c] = q;
+  }
+}
+
+// Smallest (degree, cell) among the unvisited cells into *start.
+__global__ void k_rcm_start(const RcmDev r) {
+  unsigned long long best = rcm::kUnclaimed;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < r.C; c += gridDim.x * blockDim.x)
+    if (r.pos[c] < 0) {
+      const unsigned long long k = rcm::start_key(r.deg[c], c);
+      best = k < best ? k : best;
+    }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    const unsigned long long o = __shfl_xor_sync(0xffffffffu, best, d);
+    best = o < best ? o : best;
+  }
+  if ((threadIdx.x & 31) == 0 && best != rcm::kUnclaimed) atomicMin(r.start, best);
+}
+
+// One thread: the start at order[q]; *start reset for the next component.
+__global__ void k_rcm_place_start(const RcmDev r, int q) {
+  const unsigned long long s = *r.start;
+  *r.start = rcm::kUnclaimed;
+  const long long c = (long long)(s & 0xffffffffu);
+  if (s == rcm::kUnclaimed || c >= r.C || q < 0 || q >= r.C) {
+    atomicAdd(&r.info[2], 1);
+    return;
+  }
+  r.order[q] = (int32_t)c;
+  r.pos[c] = q;
+}
+
+__global__ void k_rcm_claim(const RcmDev r, int lo, int hi) {
+  const rcm::Graph g = rcm_graph(r);
+  for (int p = lo + blockIdx.x * blockDim.x + threadIdx.x; p < hi; p += gridDim.x * blockDim.x) {
+    const int v = r.order[p];
+    if (v < 0 || v >= r.C) {
+      atomicAdd(&r.info[2], 1);
+      continue;
+    }
+    rcm::claim(g, r.pos, r.key, p, v,
+               [](unsigned long long* a, unsigned long long x) { atomicMin(a, x); });
+  }
+}
+
+__global__ void k_rcm_count(const RcmDev r, int lo, int hi) {
+  const rcm::Graph g = rcm_graph(r);
+  for (int p = lo + blockIdx.x * blockDim.x + threadIdx.x; p < hi; p += gridDim.x * blockDim.x) {
+    const int v = r.order[p];
+    r.cnt[p - lo] = (v >= 0 && v < r.C) ? rcm::count_children(g, r.key, p, v) : 0;
+  }
+}
+
+__global__ void k_rcm_emit(const RcmDev r, int lo, int hi) {
+  const rcm::Graph g = rcm_graph(r);
+  for (int p = lo + blockIdx.x * blockDim.x + threadIdx.x; p < hi; p += gridDim.x * blockDim.x) {
+    const int v = r.order[p];
+    if (v < 0 || v >= r.C) continue;  // counted by k_rcm_claim
+    const long long first = (long long)hi + r.wbase[(p - lo) / kFaceWindow] + r.win_off[p - lo];
+    const int bad = rcm::emit_children(g, r.key, p, v, first, r.order, r.pos);
+    if (bad) atomicAdd(&r.info[2], bad);
+  }
+}
+
 int grid_for(long long n) {
   const long long g = (n + kLayoutBlock - 1) / kLayoutBlock;
   return (int)(g < 148 * 16 ? (g > 0 ? g : 1) : 148 * 16);
@@ -724,6 +836,41 @@ void launch_layout_gather(const DevMesh& m, const LayoutScratch& s, const int32_
   const int2* ids = reinterpret_cast<const int2*>(face_ids);
   k_gather_fill<<<grid_for(m.F), kLayoutBlock, 0, st>>>(m, ids, s.gcnt, gather);
   k_gather_sort<<<grid_for(m.C), kLayoutBlock, 0, st>>>(m, s.gcnt, gather);
+}
+
+void launch_rcm_graph(const RcmDev& r, cudaStream_t st) {
+  const int nwin = (r.C + kFaceWindow - 1) / kFaceWindow;
+  DevMesh m{};
+  m.C = r.C;
+  if (r.Fi > 0) k_rcm_degree<<<grid_for(r.Fi), kLayoutBlock, 0, st>>>(r);
+  k_window_scan<<<nwin, kWinBlock, 0, st>>>(m, r.deg, r.deg, r.win_off, r.wsum, r.info);
+  k_window_base<<<1, kWinBlock, 0, st>>>(r.wsum, nwin, r.wbase);
+  k_csr_offsets<<<grid_for(r.C + 1LL), kLayoutBlock, 0, st>>>(r.C, r.win_off, r.wbase, nwin,
+                                                              r.off);
+  if (r.Fi > 0) {
+    k_rcm_scatter<<<grid_for(r.Fi), kLayoutBlock, 0, st>>>(r);
+    k_rcm_sort<<<grid_for(r.C), kLayoutBlock, 0, st>>>(r);
+  }
+  k_rcm_isolated<<<grid_for(r.C), kLayoutBlock, 0, st>>>(r);
+  k_window_scan<<<nwin, kWinBlock, 0, st>>>(m, r.cnt, r.cnt, r.win_off, r.wsum, r.info);
+  k_window_base<<<1, kWinBlock, 0, st>>>(r.wsum, nwin, r.wbase);
+  k_rcm_place_isolated<<<grid_for(r.C), kLayoutBlock, 0, st>>>(r);
+}
+
+void launch_rcm_start(const RcmDev& r, int q, cudaStream_t st) {
+  k_rcm_start<<<grid_for(r.C), kLayoutBlock, 0, st>>>(r);
+  k_rcm_place_start<<<1, 1, 0, st>>>(r, q);
+}
+
+void launch_rcm_level(const RcmDev& r, int lo, int hi, cudaStream_t st) {
+  const int n = hi - lo, nwin = (n + kFaceWindow - 1) / kFaceWindow;
+  DevMesh m{};
+  m.C = n;
+  k_rcm_claim<<<grid_for(n), kLayoutBlock, 0, st>>>(r, lo, hi);
+  k_rcm_count<<<grid_for(n), kLayoutBlock, 0, st>>>(r, lo, hi);
+  k_window_scan<<<nwin, kWinBlock, 0, st>>>(m, r.cnt, r.cnt, r.win_off, r.wsum, r.info);
+  k_window_base<<<1, kWinBlock, 0, st>>>(r.wsum, nwin, r.wbase);
+  k_rcm_emit<<<grid_for(n), kLayoutBlock, 0, st>>>(r, lo, hi);
 }
 
 }  // namespace plfbs

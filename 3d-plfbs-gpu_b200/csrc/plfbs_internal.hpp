@@ -171,6 +171,37 @@ void launch_dedupe_scan(const RecordSource& r, const DedupeScratch& d, cudaStrea
 void launch_dedupe_emit(const RecordSource& r, const DedupeScratch& d, int32_t* index, void* t0,
                         void* t1, void* t2, cudaStream_t stream);
 
+// The Cuthill-McKee order built on the device by breadth-first levels
+// (renumber 2, rcm_levels.hpp): the order setup.cpp's rcm_order computes,
+// before its reversal.
+struct RcmDev {
+  int C, Fi;
+  const int32_t* owner;          // [Fi] caller internal faces
+  const int32_t* neighbour;      // [Fi]
+  int32_t* deg;                  // [C] zeroed: internal faces per cell
+  int32_t* cursor;               // [C] zeroed
+  int32_t* cnt;                  // [C] flags, then children per frontier position
+  int32_t* win_off;              // [C] offsets within a window of kFaceWindow
+  int32_t* wsum;                 // [windows of C]
+  int32_t* wbase;                // [windows of C + 1]: wbase[windows] = the scan's total
+  int32_t* off;                  // [C + 1] adjacency offsets
+  unsigned long long* adj_key;   // [2 Fi] (face << 32) | neighbour, sorted per cell
+  int32_t* adj;                  // [2 Fi] neighbours in face order
+  int32_t* pos;                  // [C] filled with -1: position in the order
+  unsigned long long* key;       // [C] filled with ~0: claim keys
+  int32_t* order;                // [C] zeroed
+  unsigned long long* start;     // [1]
+  int32_t* info;                 // [4] zeroed: [1] window-scan scratch, [2] refused placements
+};
+// Degrees, face-ordered adjacency, and the cells without internal faces at
+// the front of the order by index (their count at wbase[windows of C]).
+void launch_rcm_graph(const RcmDev& r, cudaStream_t stream);
+// The next component's start (smallest (degree, cell) unvisited) at order[q].
+void launch_rcm_start(const RcmDev& r, int q, cudaStream_t stream);
+// The level after order[lo, hi) at order[hi ..]; its size at
+// wbase[windows of (hi - lo)].
+void launch_rcm_level(const RcmDev& r, int lo, int hi, cudaStream_t stream);
+
 // FP32 boundary records for the deviation form (PLFBS_FP32_DEVIATION):
 // rounded once from the FP64 records, values as deviations (rho - rho0,
 // velocity / U).
@@ -188,14 +219,20 @@ int ls_weights(const plfbs_mesh_view& m, int mode, double* lhs_inv, double* rhs,
 void set_global_error(const std::string& m);
 
 // The cell order (order[new] = caller cell): identity, or RCM for renumber 1
-// (setup.cpp).
+// and 2 (setup.cpp; renumber 2 is the same order built on the device).
 std::vector<int32_t> cell_order(int C, int Fi, const int32_t* owner, const int32_t* nb,
                                 int renumber);
 
 // Validate the views, renumber the cells, order the boundary faces and build
-// their records (setup.cpp).
+// their records (setup.cpp). For renumber 2 it stops after the validation:
+// the caller builds the order on the device and calls order_layout.
 int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bc,
                    Layout& L, std::string& err);
+
+// The order-dependent part of prepare_layout for a given cell order (a
+// permutation of the cells): boundary face order and records.
+int order_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bc,
+                 std::vector<int32_t> order, Layout& L, std::string& err);
 
 // ---------------------------------------------------------------------------
 // Device side

@@ -254,7 +254,7 @@ int validate_polymesh(const plfbs_polymesh_view& pm, std::string& err) {
 
 std::vector<int32_t> cell_order(int C, int Fi, const int32_t* owner, const int32_t* nb,
                                 int renumber) {
-  if (renumber == 1) return rcm_order(C, Fi, owner, nb);
+  if (renumber == 1 || renumber == 2) return rcm_order(C, Fi, owner, nb);
   std::vector<int32_t> order(C);
   std::iota(order.begin(), order.end(), 0);
   return order;
@@ -382,7 +382,17 @@ int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfb
   }
 
   // --- renumbering ---------------------------------------------------------
-  L.cell_old_of_new = cell_order(C, Fi, m.owner, m.neighbour, cfg.renumber);
+  // renumber 2: the device builds the order, then plfbs_create calls
+  // order_layout with it
+  if (cfg.renumber == 2) return PLFBS_OK;
+  return order_layout(cfg, m, bcv, cell_order(C, Fi, m.owner, m.neighbour, cfg.renumber), L, err);
+}
+
+int order_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bcv,
+                 std::vector<int32_t> order, Layout& L, std::string& err) {
+  const int C = L.C, Fi = L.Fi, B = L.B;
+  const bool cpu = cfg.flavour == PLFBS_FLAVOUR_CPU_SOLVER;
+  L.cell_old_of_new = std::move(order);
   L.cell_new_of_old.resize(C);
   for (int i = 0; i < C; i++) L.cell_new_of_old[L.cell_old_of_new[i]] = i;
 

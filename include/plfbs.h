@@ -165,7 +165,9 @@ typedef struct {
   double lengths[3];          /* domain.X/Y/Z */
   int32_t gradient_mode;      /* PLFBS_GRAD_*, optionally | PLFBS_GRAD_EXACT_INVERSE */
   int32_t precision;          /* PLFBS_FP64 or PLFBS_FP32_DEVIATION */
-  int32_t renumber;           /* 1: reorder cells (RCM) and faces for locality */
+  int32_t renumber;           /* 0: caller's cell order; 1: reverse Cuthill-McKee (host
+                                 breadth-first search); 2: the same order built on the
+                                 device; faces are reordered for locality in every case */
   int32_t flavour;            /* PLFBS_FLAVOUR_*: whose reconstruction and boundary tables */
 } plfbs_config;
 
@@ -288,7 +290,7 @@ int plfbs_get_layout(plfbs_ctx* ctx, int32_t* sizes, int32_t* cell_order, int32_
 
 /* Host-only: the cell order plfbs_create uses (order[new] = caller cell): the
  * identity for renumber 0, reverse Cuthill-McKee over the internal faces for
- * renumber 1 (start cells by ascending degree, neighbours by ascending degree,
+ * renumber 1 and 2 (start cells by ascending degree, neighbours by ascending degree,
  * both stable). Needs owner, neighbour and the sizes of `mesh` only. */
 int plfbs_cell_order(const plfbs_mesh_view* mesh, int32_t renumber, int32_t* order);
 

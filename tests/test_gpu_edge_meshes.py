@@ -53,7 +53,7 @@ def test_tiny_meshes(plfbs_lib, kind):
                origin=(0, 0, 0), lengths=(c.X, c.Y, c.Z), gradient_mode=capi.GRAD_LS)
     o = oracle.OracleRun(ma, rt, vt, val, cfg, s0)
     o.run_steps(5)
-    for renumber in (0, 1):
+    for renumber in (0, 1, 2):
         s = capi.Solver(ma, rt, vt, val, dict(cfg, renumber=renumber))
         s.set_state(s0)
         s.run(5)

@@ -1,8 +1,9 @@
 """The layout built on the device (layout.cu) against its rules restated in
 numpy (layout_oracle): cell order, face order, stencil neighbours and
 weights, and the face-to-cell gather, bit for bit, in both precisions, with
-and without RCM renumbering, on the golden meshes, a hex box of several
-face windows and a jittered tetrahedral box."""
+and without RCM renumbering (host order, renumber 1; device order,
+renumber 2), on the golden meshes, a hex box of several face windows, a
+jittered tetrahedral box and meshes in several disjoint pieces."""
 
 import copy
 
@@ -39,7 +40,7 @@ def _check(ma, rt, vt, val, cfg, renumber, precision):
 
 
 @pytest.mark.parametrize("precision", [capi.FP64, capi.FP32_DEVIATION])
-@pytest.mark.parametrize("renumber", [0, 1])
+@pytest.mark.parametrize("renumber", [0, 1, 2])
 @pytest.mark.parametrize("name", golden_cases.NAMES)
 def test_layout_of_golden_meshes(plfbs_lib, name, renumber, precision):
     d = golden_cases.build(name)
@@ -65,7 +66,7 @@ def _tet_case():
     return cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min), c
 
 
-@pytest.mark.parametrize("renumber", [0, 1])
+@pytest.mark.parametrize("renumber", [0, 1, 2])
 @pytest.mark.parametrize("mesh,mode", [("box", capi.GRAD_LS), ("tets", capi.GRAD_HYBRID),
                                        ("tets", capi.GRAD_LS | capi.GRAD_EXACT_INVERSE)])
 def test_layout_of_larger_meshes(plfbs_lib, mesh, mode, renumber):
@@ -75,6 +76,60 @@ def test_layout_of_larger_meshes(plfbs_lib, mesh, mode, renumber):
     cfg = dict(visc=c.visc, dt=c.dt, max_velocity=c.mach, channel_height=c.Y,
                lengths=(c.X, c.Y, c.Z), gradient_mode=mode)
     _check(ma, rt, vt, val, cfg, renumber, capi.FP64)
+
+
+def _join(pms):
+    """One polyMesh of disjoint pieces: every piece's internal faces first,
+    then every piece's patches, cells and points numbered piece by piece."""
+    cell0 = np.cumsum([0] + [pm.n_cells for pm in pms])
+    pt0 = np.cumsum([0] + [len(pm.points) for pm in pms])
+    V = max(pm.faces.shape[1] for pm in pms)
+
+    def faces(pm, k, rows):
+        f = np.full((len(rows), V), -1, np.int32)
+        src = pm.faces[rows]
+        f[:, :src.shape[1]] = np.where(src >= 0, src + pt0[k], -1)
+        return f
+
+    fl, nv, own, nb, patches = [], [], [], [], []
+    for k, pm in enumerate(pms):
+        rows = np.arange(pm.n_internal)
+        fl.append(faces(pm, k, rows))
+        nv.append(pm.nverts[rows])
+        own.append(pm.owner[rows] + cell0[k])
+        nb.append(pm.neighbour + cell0[k])
+    start = sum(pm.n_internal for pm in pms)
+    for k, pm in enumerate(pms):
+        for name, ptype, s0, n in pm.patches:
+            rows = np.arange(s0, s0 + n)
+            fl.append(faces(pm, k, rows))
+            nv.append(pm.nverts[rows])
+            own.append(pm.owner[rows] + cell0[k])
+            patches.append((name, ptype, start, n))
+            start += n
+    return cases.PolyMesh(points=np.concatenate([pm.points for pm in pms]).astype(np.float32),
+                          faces=np.concatenate(fl), nverts=np.concatenate(nv).astype(np.int32),
+                          owner=np.concatenate(own).astype(np.int32),
+                          neighbour=np.concatenate(nb).astype(np.int32),
+                          n_cells=int(cell0[-1]), patches=patches)
+
+
+@pytest.mark.parametrize("pieces", [3, 400])
+def test_device_order_of_meshes_in_pieces(plfbs_lib, pieces):
+    """Pieces of different sizes, one of them a single cell (no internal face);
+    400 pieces (333 with internal faces) is past the device's component limit, where create takes the
+    host order (the same order)."""
+    sizes = [(5, 3, 2), (1, 1, 1), (4, 4, 4)] if pieces == 3 else \
+        [((k % 3) + 1, 1, (k % 2) + 1) for k in range(pieces)]
+    pms = [cases.uniform_box(*n, origin=(0.0, 0.0, 10.0 * k)) for k, n in enumerate(sizes)]
+    pm = _join(pms)
+    c = cases.Case(mesh_dir="", X=5, Y=4, Z=10 * pieces, dt=0.05, mach=0.05, reynolds=100.0,
+                   ref_length=4.0, bcs=[cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann")])
+    ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
+    rt, vt, val = cases.bc_arrays(ma, c)
+    cfg = dict(visc=c.visc, dt=c.dt, max_velocity=c.mach, channel_height=c.Y,
+               lengths=(c.X, c.Y, c.Z), gradient_mode=capi.GRAD_LS)
+    _check(ma, rt, vt, val, cfg, 2, capi.FP64)
 
 
 def test_singular_least_squares_matrix_is_reported(plfbs_lib):

@@ -58,5 +58,6 @@ def test_library_cell_order_matches_the_oracle(plfbs_lib, name, ma):
                                    np.asarray(ma.neighbour))
     np.testing.assert_array_equal(capi.cell_order(ma, 1), want)
     np.testing.assert_array_equal(capi.cell_order(ma, 0), np.arange(ma.n_cells))
+    np.testing.assert_array_equal(capi.cell_order(ma, 2), want)  # the device order's target
     with pytest.raises(capi.PlfbsError):
-        capi.cell_order(ma, 2)
+        capi.cell_order(ma, 3)
