@@ -22,7 +22,7 @@ using plfbs::Layout;
 
 namespace {
 
-std::string g_err;  // errors without a context
+thread_local std::string g_err;  // errors without a context, per calling thread
 
 const char* kVersion = "plfbs-b200 0.1 (sm_100a)";
 

@@ -860,7 +860,7 @@ struct plfbs_gnn {
 
 namespace {
 
-std::string g_gnn_err;
+thread_local std::string g_gnn_err;  // errors without a network, per calling thread
 
 int gerr(plfbs_gnn* g, int code, const std::string& m) {
   if (g)

@@ -18,7 +18,9 @@
  * unstructured_mesh.cpp:1346-1375). Per-cell state is four doubles (u, v, w,
  * rho). Every function returns PLFBS_OK (0) or a negative status; it never
  * exits the process and never traps the GPU; plfbs_last_error() explains the
- * last failure. A context is single-threaded and bound to one device.
+ * last failure. A context is single-threaded and bound to one device;
+ * different contexts may be used from different threads, and the message of a
+ * failure without a context (plfbs_last_error(NULL)) is kept per thread.
  */
 #ifndef PLFBS_H
 #define PLFBS_H
@@ -346,7 +348,7 @@ int plfbs_memory_bytes(plfbs_ctx* ctx, int64_t* bytes);
 int plfbs_residual_norms_noalloc(const double* residual, int64_t n_cells, double ref_rho,
                                  double max_velocity, double* out, void* stream);
 
-const char* plfbs_last_error(const plfbs_ctx* ctx);  /* ctx may be NULL: global error */
+const char* plfbs_last_error(const plfbs_ctx* ctx);  /* ctx may be NULL: this thread's last error */
 
 /* Frees the context (replaces the end of General_Purpose_Solver_mk_i; the
  * reference never frees its managed buffers). Its device arrays return to a

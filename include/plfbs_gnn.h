@@ -15,7 +15,7 @@
  * flat FP32 array, MLP by MLP in the order n, e, (e1, n1), ..., (eL, nL), d;
  * each as W1 [k][64] row-major, b1 [64], W2 [64][m], b2 [m].
  * All entry points return 0 or a negative PLFBS_ERR_* code (plfbs.h);
- * messages through plfbs_gnn_last_error.
+ * messages through plfbs_gnn_last_error (per thread for a NULL network).
  */
 #ifndef PLFBS_GNN_H
 #define PLFBS_GNN_H

@@ -95,6 +95,36 @@ def test_rejects_bad_config(plfbs_lib):
     assert e.value.code == capi.ERR_ARG
 
 
+def test_rejects_unknown_renumber(plfbs_lib):
+    ma, rt, vt, val = _cavity()
+    with pytest.raises(capi.PlfbsError) as e:
+        _create(ma, rt, vt, val, renumber=3)
+    assert e.value.code == capi.ERR_ARG and "renumber" in str(e.value)
+
+
+def test_context_free_errors_are_per_thread(plfbs_lib):
+    """plfbs_last_error(NULL) keeps each thread's own last failure: two threads
+    fail differently, each waits for the other's failure, then reads."""
+    import threading
+    L = capi.lib()
+    gate = threading.Barrier(2)
+    seen = {}
+
+    def fail(name, call):
+        assert call() != 0
+        gate.wait(timeout=30)
+        seen[name] = L.plfbs_last_error(None)
+
+    a = threading.Thread(target=fail, args=("pool", lambda: L.plfbs_release_cached(-1)))
+    b = threading.Thread(target=fail, args=("null", lambda: L.plfbs_cell_order(None, 0, None)))
+    for t in (a, b):
+        t.start()
+    for t in (a, b):
+        t.join(timeout=60)
+    assert b"device index" in seen["pool"]
+    assert seen["null"] == b"null argument"
+
+
 def test_null_context_calls_fail_cleanly(plfbs_lib):
     assert plfbs_lib.plfbs_run_stages(None, 1) == capi.ERR_ARG
     assert plfbs_lib.plfbs_set_debug(None, 1) == capi.ERR_ARG
