@@ -11,7 +11,8 @@ inputs; uniform-flow start.
 
 A step is one full time step: the IBM update and 4 RK stages over all cells
 and faces. `value` is device throughput in Mcell-updates/s (cells x steps /
-time, summed over ranks, max time over ranks) with everything resident in
+time, summed over ranks, max time over ranks; `per_rk_stage` is the same
+rate per RK stage, 4 x value) with everything resident in
 HBM; the working set (~0.5 GB) exceeds the 126 MB L2, so no flush is needed
 between steps. `e2e` times the whole drop-in call through the C ABI from host
 buffers: create (mesh upload, least-squares weights, layout), set_state,
@@ -575,6 +576,7 @@ def main():
                            "nodes": NNODES, "re": RE, "dt": DT,
                            "parallelism": "replicas" if world > 1 else "single",
                            "l2": "working set > L2 (no flush)"},
+                "per_rk_stage": {"value": 4 * value, "unit": "Mcell-stage-updates/s"},
                 "roofline": roof, "kernels": kern, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": KERNELS_PER_STEP * args.steps, "clocks": clk.summary(),
                 "final_max_error": float(hist[-1, 1]) if len(hist) else None}
