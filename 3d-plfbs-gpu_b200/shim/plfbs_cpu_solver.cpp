@@ -116,6 +116,7 @@ void Solver::General_Purpose_Solver_mk_i(unstructured_mesh& Mesh, Solution& soln
     plfbs_stats st;
     rc = plfbs_run(ctx, n, &st, hist.data());
     if (rc && rc != PLFBS_ERR_DIVERGED) {
+      exit_kind = "error";
       plfbs_shim::report(ctx, "plfbs_run", rc);
       break;
     }

@@ -145,6 +145,7 @@ void gpu_solver::General_Purpose_Solver_mk_i(
     plfbs_stats st;
     rc = plfbs_run(ctx, n, &st, hist.data());
     if (rc && rc != PLFBS_ERR_DIVERGED) {
+      exit_kind = "error";
       report(ctx, "plfbs_run", rc);
       break;
     }

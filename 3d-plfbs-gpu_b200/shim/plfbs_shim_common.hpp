@@ -126,7 +126,8 @@ inline plfbs_config config(global_variables& globals, domain_geometry& domain,
 // JSON-lines run log, <output_file>/run.jsonl: one record per output step
 // (the residual norms the reference writes to error.txt, plus the device time
 // of the steps since the previous record and the throughput they give) and a
-// last record with the exit and the wall drag and lift coefficients.
+// last record with the exit (converged, out_of_time, diverged or error) and the
+// drag and lift coefficients post-processing computed.
 class RunLog {
  public:
   RunLog(const std::string& path, long long cells) : f_(std::fopen(path.c_str(), "w")), cells_(cells) {}
