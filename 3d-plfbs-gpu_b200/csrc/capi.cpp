@@ -4,6 +4,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstddef>
 #include <cstring>
@@ -11,6 +12,7 @@
 #include <new>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "capi_internal.hpp"
@@ -245,11 +247,48 @@ int check_fault(plfbs_ctx* ctx) {
 
 
 
+// Waits at most `seconds` (none if <= 0) for the end of the launched steps
+// (ev1). Running out leaves the context busy: the steps are still in flight
+// and every call but plfbs_wait and plfbs_destroy returns PLFBS_ERR_TIMEOUT.
+int wait_steps(plfbs_ctx* ctx, double seconds) {
+  if (!(seconds > 0)) {
+    CK(cudaEventSynchronize(ctx->ev1));
+    ctx->busy = false;
+    return PLFBS_OK;
+  }
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::duration<double>(seconds);
+  for (;;) {
+    const cudaError_t e = cudaEventQuery(ctx->ev1);
+    if (e == cudaSuccess) {
+      ctx->busy = false;
+      return PLFBS_OK;
+    }
+    if (e != cudaErrorNotReady) CK(e);
+    if (std::chrono::steady_clock::now() >= deadline) {
+      ctx->busy = true;
+      return set_err(ctx, PLFBS_ERR_TIMEOUT,
+                     "the launched steps did not finish within the time limit; they are still "
+                     "in flight (plfbs_wait, then carry on)");
+    }
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+}
+
 int check_ctx(plfbs_ctx* ctx) {
   if (!ctx) return set_err(nullptr, PLFBS_ERR_ARG, "null context");
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess)
     return set_err(ctx, PLFBS_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  if (ctx->busy) {  // finished since the time-out?
+    e = cudaEventQuery(ctx->ev1);
+    if (e == cudaSuccess)
+      ctx->busy = false;
+    else if (e == cudaErrorNotReady)
+      return set_err(ctx, PLFBS_ERR_TIMEOUT,
+                     "steps of a timed-out run are still in flight (plfbs_wait first)");
+    else
+      return set_err(ctx, PLFBS_ERR_CUDA, std::string("cudaEventQuery: ") + cudaGetErrorString(e));
+  }
   return PLFBS_OK;
 }
 
@@ -828,6 +867,7 @@ int plfbs_run(plfbs_ctx* ctx, int64_t max_steps, plfbs_stats* stats, double* his
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     for (long long k = 0; k < n; k++) CK(cudaGraphLaunch(ctx->step_exec, ctx->stream));
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    TRY(wait_steps(ctx, ctx->timeout_s));
     TRY(read_stats(ctx));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
@@ -868,6 +908,25 @@ int plfbs_run(plfbs_ctx* ctx, int64_t max_steps, plfbs_stats* stats, double* his
   if (ctx->stats_host->diverged)
     return set_err(ctx, PLFBS_ERR_DIVERGED, "residual is NaN or rho exceeded 1000");
   return PLFBS_OK;
+}
+
+int plfbs_set_timeout(plfbs_ctx* ctx, double seconds) {
+  TRY(check_ctx(ctx));
+  if (!(seconds >= 0) || !std::isfinite(seconds))
+    return set_err(ctx, PLFBS_ERR_ARG, "timeout is a finite number of seconds >= 0");
+  ctx->timeout_s = seconds;
+  return PLFBS_OK;
+}
+
+int plfbs_wait(plfbs_ctx* ctx, double seconds) {
+  if (!ctx) return set_err(nullptr, PLFBS_ERR_ARG, "null context");
+  if (!(seconds >= 0) || !std::isfinite(seconds))
+    return set_err(ctx, PLFBS_ERR_ARG, "wait is a finite number of seconds >= 0");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess)
+    return set_err(ctx, PLFBS_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  if (!ctx->busy) return PLFBS_OK;
+  return wait_steps(ctx, seconds > 0 ? seconds : 1e-9);  // 0: just ask
 }
 
 int plfbs_set_layout_compression(plfbs_ctx* ctx, int32_t on) {

@@ -37,6 +37,8 @@ struct plfbs_ctx {
   int compact_faces = 0;          // unique face records in the compact layout (0: none)
   int compact_cells = 0;          // unique cell weight sets in the compact layout (0: none)
   bool flux_maps_ok = false;
+  double timeout_s = 0;  // bound on plfbs_run's waits for its step batches (0: none)
+  bool busy = false;     // a timed-out run's steps are still in flight (ev1 marks their end)
   std::string err;
 };
 

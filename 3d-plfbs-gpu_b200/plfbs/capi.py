@@ -14,8 +14,8 @@ import numpy as np
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "_lib", "libplfbs.so")
 
-OK, ERR_ARG, ERR_MESH, ERR_BC, ERR_CUDA, ERR_DIVERGED, ERR_NO_DEVICE, ERR_STATE = (
-    0, -1, -2, -3, -4, -5, -6, -7)
+OK, ERR_ARG, ERR_MESH, ERR_BC, ERR_CUDA, ERR_DIVERGED, ERR_NO_DEVICE, ERR_STATE, ERR_TIMEOUT = (
+    0, -1, -2, -3, -4, -5, -6, -7, -8)
 GRAD_LS, GRAD_HYBRID, GRAD_GREEN_GAUSS, GRAD_EXACT_INVERSE = 0, 1, 2, 0x100
 FP64, FP32_DEVIATION = 0, 1
 FLAVOUR_GPU, FLAVOUR_CPU_SOLVER = 0, 1
@@ -32,7 +32,8 @@ EXPORTS = ("plfbs_create", "plfbs_set_state", "plfbs_run", "plfbs_get_state",
            "plfbs_residual_norms_noalloc", "plfbs_release_cached", "plfbs_warm_start",
            "plfbs_checkpoint_bytes", "plfbs_save_checkpoint", "plfbs_load_checkpoint",
            "plfbs_wall_forces", "plfbs_get_layout", "plfbs_polymesh_geometry",
-           "plfbs_set_flux_kernel", "plfbs_set_layout_compression", "plfbs_cell_order")
+           "plfbs_set_flux_kernel", "plfbs_set_layout_compression", "plfbs_cell_order",
+           "plfbs_set_timeout", "plfbs_wait")
 
 
 class MeshView(C.Structure):
@@ -117,6 +118,8 @@ def lib():
         L.plfbs_get_layout.argtypes = [C.c_void_p, _ip, _ip, _ip, _ip, _dp, _ip]
         L.plfbs_set_flux_kernel.argtypes = [C.c_void_p, C.c_int32]
         L.plfbs_set_layout_compression.argtypes = [C.c_void_p, C.c_int32]
+        L.plfbs_set_timeout.argtypes = [C.c_void_p, C.c_double]
+        L.plfbs_wait.argtypes = [C.c_void_p, C.c_double]
         L.plfbs_cell_order.argtypes = [C.POINTER(MeshView), C.c_int32, _ip]
         L.plfbs_polymesh_geometry.argtypes = [C.POINTER(PolyMeshView), C.c_double, C.c_double,
                                               C.c_double, C.c_int32, C.POINTER(MeshOut)]
@@ -320,6 +323,19 @@ class Solver:
             self._check(rc)
         out["rc"] = rc
         return out, (hist[: int(st.steps_run)] if history else None)
+
+    def set_timeout(self, seconds):
+        """Bound plfbs_run's wait per batch of launched steps (0: no bound)."""
+        self._check(lib().plfbs_set_timeout(self.h, float(seconds)))
+
+    def wait(self, seconds):
+        """True once the steps of a timed-out run have ended, False if they are
+        still in flight after `seconds`."""
+        rc = lib().plfbs_wait(self.h, float(seconds))
+        if rc == ERR_TIMEOUT:
+            return False
+        self._check(rc)
+        return True
 
     def run_stages(self, n):
         self._check(lib().plfbs_run_stages(self.h, int(n)))

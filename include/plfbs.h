@@ -39,7 +39,8 @@ enum {
   PLFBS_ERR_CUDA = -4,        /* CUDA runtime error (message in last_error) */
   PLFBS_ERR_DIVERGED = -5,    /* NaN residual or rho > 1000 (Solver.cpp:448-493) */
   PLFBS_ERR_NO_DEVICE = -6,   /* no CUDA device / device not sm_100 */
-  PLFBS_ERR_STATE = -7        /* call out of order */
+  PLFBS_ERR_STATE = -7,       /* call out of order */
+  PLFBS_ERR_TIMEOUT = -8      /* a bounded wait ran out; the launched steps are still in flight */
 };
 
 /* Gradient weighting, gradients.cpp:259-265 ("LS", "hybrid", anything else = GG).
@@ -253,6 +254,19 @@ int plfbs_load_checkpoint(plfbs_ctx* ctx, const void* buf, int64_t bytes);
  * history (optional, may be NULL) receives 6 doubles per completed step:
  * step index, max_error, rho_rms, u_rms, v_rms, w_rms. */
 int plfbs_run(plfbs_ctx* ctx, int64_t max_steps, plfbs_stats* stats, double* history);
+
+/* Bounded waits (the reference waits without limit and exits on a CUDA error,
+ * Solver_gpu.cu:1419-1431). With a limit of `seconds` > 0, plfbs_run waits at
+ * most that long for each batch of up to 2048 launched steps; when it runs out
+ * it returns PLFBS_ERR_TIMEOUT without stats or history, and the batch stays
+ * in flight: until it ends, every call on the context but plfbs_wait and
+ * plfbs_destroy returns PLFBS_ERR_TIMEOUT. plfbs_wait waits at most `seconds`
+ * (0: only asks) and returns PLFBS_OK once the steps have ended; the context
+ * then carries on from them (their residual history is not returned; their
+ * steps count in the next stats). 0 (the default) waits without limit.
+ * plfbs_destroy always waits for work in flight. */
+int plfbs_set_timeout(plfbs_ctx* ctx, double seconds);
+int plfbs_wait(plfbs_ctx* ctx, double seconds);
 
 /* soln.clone(temp_soln) (Solver_gpu.cu:846,872,904): C + B values per array. */
 int plfbs_get_state(plfbs_ctx* ctx, double* rho, double* u, double* v, double* w,

@@ -128,6 +128,8 @@ def test_context_free_errors_are_per_thread(plfbs_lib):
 def test_null_context_calls_fail_cleanly(plfbs_lib):
     assert plfbs_lib.plfbs_run_stages(None, 1) == capi.ERR_ARG
     assert plfbs_lib.plfbs_set_debug(None, 1) == capi.ERR_ARG
+    assert plfbs_lib.plfbs_set_timeout(None, 1.0) == capi.ERR_ARG
+    assert plfbs_lib.plfbs_wait(None, 1.0) == capi.ERR_ARG
     plfbs_lib.plfbs_destroy(None)
 
 
