@@ -37,7 +37,7 @@ def _stale():
         return True
     t = os.path.getmtime(LIB)
     deps = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".hpp")]
-    deps.append(os.path.join(INCLUDE, "plfbs.h"))
+    deps += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
     return any(os.path.getmtime(d) > t for d in deps)
 
 
