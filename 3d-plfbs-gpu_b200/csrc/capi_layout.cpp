@@ -154,10 +154,12 @@ int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
   return PLFBS_OK;
 }
 
-// Components (beyond the cells without internal faces) the device order
-// starts one at a time; a mesh in more pieces takes the host order, which is
-// the same order.
+// The device order pays a few launches and one read-back per component and
+// per breadth-first level. A mesh in more pieces (beyond the cells without
+// internal faces), or with a longer chain of levels (a long thin mesh, whose
+// levels hold few cells each), takes the host order, which is the same order.
 constexpr int kMaxDeviceComponents = 256;
+constexpr int kMaxDeviceLevels = 8192;
 
 int device_cell_order(plfbs_ctx* ctx, const plfbs_mesh_view& m, std::vector<int32_t>& order) {
   const int C = ctx->L.C, Fi = ctx->L.Fi;
@@ -197,14 +199,16 @@ int device_cell_order(plfbs_ctx* ctx, const plfbs_mesh_view& m, std::vector<int3
   int hi = 0;  // cells placed so far
   TRY(scan_total(C, hi));
   if (hi < 0 || hi > C) return set_err(ctx, PLFBS_ERR_CUDA, "device cell order: bad count");
+  int levels = 0;
   for (int comp = 0; hi < C; comp++) {
-    if (comp == kMaxDeviceComponents) {
+    if (comp == kMaxDeviceComponents || levels > kMaxDeviceLevels) {
       order = plfbs::cell_order(C, Fi, m.owner, m.neighbour, 1);
       return PLFBS_OK;
     }
     plfbs::launch_rcm_start(r, hi, ctx->stream);
     int lo = hi++;
     while (lo < hi) {  // one level per pass; every pass places cells or ends the piece
+      if (++levels > kMaxDeviceLevels) break;  // the host order, above
       plfbs::launch_rcm_level(r, lo, hi, ctx->stream);
       CK(cudaGetLastError());
       int n = 0;

@@ -114,13 +114,19 @@ def _join(pms):
                           n_cells=int(cell0[-1]), patches=patches)
 
 
-@pytest.mark.parametrize("pieces", [3, 400])
-def test_device_order_of_meshes_in_pieces(plfbs_lib, pieces):
+@pytest.mark.parametrize("kind", ["pieces", "many_pieces", "chain"])
+def test_device_order_past_its_limits(plfbs_lib, kind):
     """Pieces of different sizes, one of them a single cell (no internal face);
-    400 pieces (333 with internal faces) is past the device's component limit, where create takes the
-    host order (the same order)."""
-    sizes = [(5, 3, 2), (1, 1, 1), (4, 4, 4)] if pieces == 3 else \
-        [((k % 3) + 1, 1, (k % 2) + 1) for k in range(pieces)]
+    400 pieces (333 with internal faces) is past the device's component limit
+    and a 9,000-cell chain (9,000 levels) past its level limit, where create
+    takes the host order (the same order)."""
+    if kind == "pieces":
+        sizes = [(5, 3, 2), (1, 1, 1), (4, 4, 4)]
+    elif kind == "many_pieces":
+        sizes = [((k % 3) + 1, 1, (k % 2) + 1) for k in range(400)]
+    else:
+        sizes = [(9000, 1, 1)]
+    pieces = len(sizes)
     pms = [cases.uniform_box(*n, origin=(0.0, 0.0, 10.0 * k)) for k, n in enumerate(sizes)]
     pm = _join(pms)
     c = cases.Case(mesh_dir="", X=5, Y=4, Z=10 * pieces, dt=0.05, mach=0.05, reynolds=100.0,
