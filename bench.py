@@ -80,11 +80,11 @@ def build_case():
     return pm, c, ma, nodes, state0
 
 
-def solver_cfg(c, precision=0):
+def solver_cfg(c, precision=0, renumber=0):
     return dict(visc=c.visc, gamma=1.0, dt=c.dt, domain_dt=0.5, max_velocity=c.mach,
                 ref_rho=1.0, tolerance=0.0, pressure_gradient=0.0, channel_height=c.Y,
-                origin=(0.0, 0.0, 0.0), lengths=(c.X, c.Y, c.Z), gradient_mode=0, renumber=0,
-                precision=precision)
+                origin=(0.0, 0.0, 0.0), lengths=(c.X, c.Y, c.Z), gradient_mode=0,
+                renumber=renumber, precision=precision)
 
 
 def ibm_cfg(nodes):
@@ -431,6 +431,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--renumber", type=int, default=0, choices=[0, 1, 2],
+                    help="cell order: 0 the mesh's (blockMesh), 1 RCM on the host, 2 on the device")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=20)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
@@ -470,7 +472,7 @@ def main():
     rt, vt, val = cases.bc_arrays(ma, c)
     log("case built: %d cells, %d faces" % (ma.n_cells, ma.n_faces))
     prec = capi.FP32_DEVIATION if args.precision == "fp32" else capi.FP64
-    solver = capi.Solver(ma, rt, vt, val, solver_cfg(c, prec), ibm=ibm_cfg(nodes),
+    solver = capi.Solver(ma, rt, vt, val, solver_cfg(c, prec, args.renumber), ibm=ibm_cfg(nodes),
                          device=local_rank)
 
     def barrier():
@@ -505,6 +507,8 @@ def main():
                   "update": prof["update"] / (4 * args.profile_steps)}
     total = sum(prof.values())
     workload = WORKLOAD if args.precision == "fp64" else WORKLOAD.replace("fp64", "fp32dev")
+    if args.renumber:  # another cell order: the committed traffic figures do not apply
+        workload += "_rcm"
     alg = algorithmic_bytes(ma.n_cells, ma.n_faces, ma.n_bc, fp32=args.precision == "fp32")
     peak, peak_kind = load_peaks()
     kern = {}
@@ -528,7 +532,8 @@ def main():
         for _ in range(E2E_REPS):
             barrier()
             t0 = time.perf_counter()
-            s2 = capi.Solver(ma, rt, vt, val, solver_cfg(c, prec), ibm=ibm_cfg(nodes),
+            s2 = capi.Solver(ma, rt, vt, val, solver_cfg(c, prec, args.renumber),
+                             ibm=ibm_cfg(nodes),
                              device=local_rank)
             t1 = time.perf_counter()
             s2.set_state(state0)
@@ -575,6 +580,7 @@ def main():
                 "config": {"workload": workload, "cells": ma.n_cells, "faces": ma.n_faces,
                            "nodes": NNODES, "re": RE, "dt": DT,
                            "parallelism": "replicas" if world > 1 else "single",
+                           "renumber": args.renumber,
                            "l2": "working set > L2 (no flush)"},
                 "per_rk_stage": {"value": 4 * value, "unit": "Mcell-stage-updates/s"},
                 "roofline": roof, "kernels": kern, "cpu_baseline": cpu, "e2e": e2e,
