@@ -125,6 +125,21 @@ def test_context_free_errors_are_per_thread(plfbs_lib):
     assert seen["null"] == b"null argument"
 
 
+def test_c_program_links_the_library(plfbs_lib, tmp_path):
+    """The public headers compile as strict C99 and a C program calls the
+    library's host-only entry points (tests/c_abi_check.c)."""
+    import subprocess
+    libdir = os.path.dirname(capi.LIB_PATH)
+    exe = str(tmp_path / "c_abi_check")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                    "-I", os.path.join(REPO, "include"),
+                    os.path.join(REPO, "tests", "c_abi_check.c"), "-o", exe,
+                    "-L" + libdir, "-lplfbs", "-Wl,-rpath," + libdir], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert r.stdout.startswith("plfbs")
+
+
 def test_null_context_calls_fail_cleanly(plfbs_lib):
     assert plfbs_lib.plfbs_run_stages(None, 1) == capi.ERR_ARG
     assert plfbs_lib.plfbs_set_debug(None, 1) == capi.ERR_ARG
