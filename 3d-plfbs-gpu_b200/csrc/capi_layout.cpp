@@ -154,12 +154,14 @@ int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
   return PLFBS_OK;
 }
 
-// The device order pays a few launches and one read-back per component and
-// per breadth-first level. A mesh in more pieces (beyond the cells without
-// internal faces), or with a longer chain of levels (a long thin mesh, whose
-// levels hold few cells each), takes the host order, which is the same order.
+// The device order pays a few launches and one read-back (tens of
+// microseconds) per component and per breadth-first level, the host order
+// about 50 ns per cell. A mesh in more pieces (beyond the cells without
+// internal faces), or with more levels than max(256, C / 512) (a long thin
+// mesh, whose levels hold few cells each), takes the host order, the same
+// order: the device's share then costs about as much as the host order.
 constexpr int kMaxDeviceComponents = 256;
-constexpr int kMaxDeviceLevels = 8192;
+inline int max_device_levels(int C) { return std::max(256, C / 512); }
 
 int device_cell_order(plfbs_ctx* ctx, const plfbs_mesh_view& m, std::vector<int32_t>& order) {
   const int C = ctx->L.C, Fi = ctx->L.Fi;
@@ -200,15 +202,16 @@ int device_cell_order(plfbs_ctx* ctx, const plfbs_mesh_view& m, std::vector<int3
   TRY(scan_total(C, hi));
   if (hi < 0 || hi > C) return set_err(ctx, PLFBS_ERR_CUDA, "device cell order: bad count");
   int levels = 0;
+  const int max_levels = max_device_levels(C);
   for (int comp = 0; hi < C; comp++) {
-    if (comp == kMaxDeviceComponents || levels > kMaxDeviceLevels) {
+    if (comp == kMaxDeviceComponents || levels > max_levels) {
       order = plfbs::cell_order(C, Fi, m.owner, m.neighbour, 1);
       return PLFBS_OK;
     }
     plfbs::launch_rcm_start(r, hi, ctx->stream);
     int lo = hi++;
     while (lo < hi) {  // one level per pass; every pass places cells or ends the piece
-      if (++levels > kMaxDeviceLevels) break;  // the host order, above
+      if (++levels > max_levels) break;  // the host order, above
       plfbs::launch_rcm_level(r, lo, hi, ctx->stream);
       CK(cudaGetLastError());
       int n = 0;

@@ -118,7 +118,7 @@ def _join(pms):
 def test_device_order_past_its_limits(plfbs_lib, kind):
     """Pieces of different sizes, one of them a single cell (no internal face);
     400 pieces (333 with internal faces) is past the device's component limit
-    and a 9,000-cell chain (9,000 levels) past its level limit, where create
+    and a 9,000-cell chain (9,000 levels) past its level budget, where create
     takes the host order (the same order)."""
     if kind == "pieces":
         sizes = [(5, 3, 2), (1, 1, 1), (4, 4, 4)]
