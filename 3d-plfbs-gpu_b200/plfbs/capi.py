@@ -231,8 +231,11 @@ class Solver:
 
     ``cfg`` keys: visc, gamma, dt (time_marching_step), domain_dt, max_velocity,
     ref_rho, tolerance, pressure_gradient, channel_height, origin, lengths,
-    gradient_mode, precision, renumber, flavour. ``ibm`` (optional): node_ref [N,3],
-    node_x [N,3], stiffness, radius, depth, object_nodes.
+    gradient_mode, precision (FP64 or FP32_DEVIATION), renumber (0 the mesh's
+    cell order, 1 reverse Cuthill-McKee on the host, 2 the same order built on
+    the device), flavour (FLAVOUR_GPU or FLAVOUR_CPU_SOLVER). ``ibm``
+    (optional): node_ref [N,3], node_x [N,3], stiffness, radius, depth,
+    object_nodes.
     """
 
     def __init__(self, ma, rho_type, vel_type, bc_value, cfg, ibm=None, device=0):
