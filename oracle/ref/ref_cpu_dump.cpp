@@ -1,12 +1,15 @@
 // ORACLE / TEST INFRASTRUCTURE — never part of the product path.
 //
-// Lossless final state of the reference CPU Solver (Solver.cpp). program::run
-// calls soln.output(...) right after the solver returns (program.cpp:107-116);
-// oracle/_ref/plfbs_ref_cpu is the reference program linked with
-// -Wl,--wrap on that member function, so the call lands here first: with
-// PLFBS_REF_DUMP=<dir> the state of every cell (interior and ghost) is written
-// as <dir>/cpu_final_state.npy, [total_nodes, 4] = (u, v, w, rho) in FP64, and
-// the reference's own output then runs unchanged.
+// Lossless final state of the reference's solver. program::run calls
+// soln.output(...) right after the solver returns (program.cpp:107-116);
+// oracle/_ref/plfbs_ref_cpu (CPU Solver, Solver.cpp) and plfbs_ref_gpu (the
+// reference's CUDA path, ref_gpu_device.cu) are the reference program linked
+// with -Wl,--wrap on that member function, so every call lands here first:
+// with PLFBS_REF_DUMP=<dir> the state of every cell (interior and ghost) is
+// written as <dir>/PLFBS_DUMP_NAME (cpu_final_state.npy unless the build
+// names another), [total_nodes, 4] = (u, v, w, rho) in FP64, the last call
+// (the final state) overwriting earlier ones, and the reference's own output
+// then runs unchanged.
 
 #include <cstdio>
 #include <cstdlib>
@@ -14,6 +17,10 @@
 #include <vector>
 
 #include "Solution.h"
+
+#ifndef PLFBS_DUMP_NAME
+#define PLFBS_DUMP_NAME "cpu_final_state.npy"
+#endif
 #include "domain_geometry.h"
 #include "global_variables.h"
 
@@ -40,7 +47,7 @@ void __wrap__ZN8Solution6outputENSt7__cxx1112basic_stringIcSt11char_traitsIcESaI
     const size_t total = 10 + hdr.size() + 1;
     hdr.append((64 - total % 64) % 64, ' ');
     hdr += '\n';
-    const std::string path = std::string(dir) + "/cpu_final_state.npy";
+    const std::string path = std::string(dir) + "/" PLFBS_DUMP_NAME;
     if (FILE* f = std::fopen(path.c_str(), "wb")) {
       const unsigned char magic[8] = {0x93, 'N', 'U', 'M', 'P', 'Y', 1, 0};
       const unsigned short len = (unsigned short)hdr.size();
