@@ -20,6 +20,9 @@ run, the per-step residual history read-back, get_state and destroy.
 
 --impl reference times the reference's own CPU Solver (oracle/_ref, built
 from the reference sources) on the same mesh and boundary conditions.
+`reference_gpu` (rank 0, one GPU, FP64) is the reference's own CUDA path
+(Solver_gpu.cu built for sm_100a) timed on the same case, outside the timed
+region: the reference-kernel figure beside `value`.
 """
 
 from __future__ import annotations
@@ -202,6 +205,52 @@ def reference_cpu_throughput(pm, c, nodes, sample_steps=1):
         "conditions (the CPU Solver has no IBM), setup subtracted via a 0-step run "
         "(%.1f s setup, %.1f s per step), serial" % (sample_steps, NX, NY, NZ, t_setup,
                                                     per_step))
+
+
+REF_GPU_BIN = os.path.join(REPO, "oracle", "_ref", "plfbs_ref_gpu")
+
+
+def reference_gpu_throughput(pm, c, nodes, steps=2001, every=100, limit=600):
+    """Mcell-updates/s of the reference's own CUDA path (oracle/_ref/plfbs_ref_gpu:
+    Solver_gpu.cu and its kernels built for sm_100a) on the same case: it prints
+    a progress line every `every` steps (Solver_gpu.cu:844-853), and the median
+    time between their arrivals, over `every`, is its time per step with its
+    setup and the occasional decade output left out."""
+    import copy
+    if not os.path.exists(REF_GPU_BIN):
+        return None, "oracle/_ref/plfbs_ref_gpu not built"
+    c = copy.copy(c)
+    stamps, rc = [], None
+    with tempfile.TemporaryDirectory(prefix="plfbs_refgpu_") as wd:
+        cases.write_polymesh(os.path.join(wd, "polyMesh"), pm)
+        node_file = os.path.join(wd, "nodes.txt")
+        cases.write_spring_network(node_file, nodes)
+        c.steps, c.gpu_solver, c.output_step = steps, 1, every
+        c.output_dir = os.path.join(wd, "out") + "/"
+        c.obj_nodes_file, c.obj_num_nodes = node_file, len(nodes)
+        c.mesh_dir = os.path.join(wd, "polyMesh")
+        xml = os.path.join(wd, "case.xml")
+        cases.write_xml(xml, c)
+        p = subprocess.Popen([REF_GPU_BIN, xml], cwd=wd, stdout=subprocess.PIPE,
+                             stderr=subprocess.DEVNULL, text=True)
+        timer = threading.Timer(limit, p.kill)  # this process only
+        timer.start()
+        try:
+            for line in p.stdout:
+                if line.startswith("time t="):
+                    stamps.append(time.perf_counter())
+            rc = p.wait()
+        finally:
+            timer.cancel()
+    if rc != 0 or len(stamps) < 3:
+        return None, "the reference CUDA path exited with %s after %d progress lines" % (
+            rc, len(stamps))
+    gaps = sorted(b - a for a, b in zip(stamps, stamps[1:]))
+    per_step = gaps[len(gaps) // 2] / every
+    return pm.n_cells / per_step / 1e6, (
+        "the reference's Solver_gpu.cu path built for sm_100a on the same case (IBM included), "
+        "%d steps, median of %d intervals of %d steps between its progress lines (setup and "
+        "decade outputs left out), %.3f ms per step" % (steps, len(gaps), every, 1e3 * per_step))
 
 
 def reduce_max(x, dist=None, device="cuda"):
@@ -434,6 +483,8 @@ def main():
     ap.add_argument("--renumber", type=int, default=0, choices=[0, 1, 2],
                     help="cell order: 0 the mesh's (blockMesh), 1 RCM on the host, 2 on the device")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own CUDA path on the same case")
     ap.add_argument("--profile-steps", type=int, default=20)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
                     help="fp32: the FP32 deviation form (the headline line is fp64)")
@@ -571,6 +622,11 @@ def main():
         v, sample = reference_cpu_throughput(pm, c, nodes, sample_steps=1)
         if v is not None:
             cpu = {"value": v, "unit": METRIC, "cores": 1, "kind": "reference", "sample": sample}
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu and args.precision == "fp64":
+        v, sample = reference_gpu_throughput(pm, c, nodes)
+        ref_gpu = {"value": v, "unit": METRIC, "sample": sample}
+        log("reference GPU: %r" % ref_gpu)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
@@ -583,7 +639,8 @@ def main():
                            "renumber": args.renumber,
                            "l2": "working set > L2 (no flush)"},
                 "per_rk_stage": {"value": 4 * value, "unit": "Mcell-stage-updates/s"},
-                "roofline": roof, "kernels": kern, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roof, "kernels": kern, "cpu_baseline": cpu,
+                "reference_gpu": ref_gpu, "e2e": e2e,
                 "gpu_launches": KERNELS_PER_STEP * args.steps, "clocks": clk.summary(),
                 "final_max_error": float(hist[-1, 1]) if len(hist) else None}
         print(json.dumps(line))
