@@ -169,7 +169,7 @@ def load_traffic(kernel, workload):
 REF_BIN = os.path.join(REPO, "oracle", "_ref", "plfbs_ref")
 
 
-def _run_ref_cpu(workdir, pm, c, nodes, steps):
+def _run_ref_cpu(workdir, pm, c, nodes, steps, mesh_dir=None, progress=None, limit=1200):
     import shutil
     c.steps = steps
     c.gpu_solver = 0
@@ -181,18 +181,40 @@ def _run_ref_cpu(workdir, pm, c, nodes, steps):
         cases.write_spring_network(node_file, nodes)
     c.obj_nodes_file = node_file
     c.obj_num_nodes = len(nodes)
-    c.mesh_dir = os.path.join(workdir, "polyMesh")
+    c.mesh_dir = mesh_dir or os.path.join(workdir, "polyMesh")
     xml = os.path.join(workdir, "case.xml")
     cases.write_xml(xml, c)
-    t0 = time.perf_counter()
-    subprocess.run([REF_BIN, xml], cwd=workdir, check=True, stdout=subprocess.DEVNULL,
-                   stderr=subprocess.DEVNULL)
-    return time.perf_counter() - t0
+    # the time from the program's "Running Solver" line (printed right before
+    # it calls the solver, program.cpp:106) to its exit: the mesh import and
+    # the rest of the setup before it are left out
+    p = subprocess.Popen([REF_BIN, xml], cwd=workdir, stdout=subprocess.PIPE,
+                         stderr=subprocess.DEVNULL, text=True)
+    timer = threading.Timer(limit, p.kill)  # this process only
+    timer.start()
+    t_solver = None
+    stamps = []  # arrivals of its progress lines ("time t=", Solver.cpp:501-508)
+    try:
+        for line in p.stdout:
+            now = time.perf_counter()
+            if t_solver is None and line.startswith("Running Solver"):
+                t_solver = now
+            elif line.startswith("time t="):
+                stamps.append(now)
+        rc = p.wait()
+    finally:
+        timer.cancel()
+    t_end = time.perf_counter()
+    if rc != 0 or t_solver is None:
+        raise subprocess.CalledProcessError(rc, REF_BIN)
+    if progress is not None:
+        progress.extend(stamps)
+    return t_end - t_solver
 
 
 def reference_cpu_throughput(pm, c, nodes, sample_steps=1):
-    """Mcell-updates/s of the reference CPU Solver: wall time of a run of
-    `sample_steps` steps minus that of a 0-step run (mesh import and setup)."""
+    """Mcell-updates/s of the reference CPU Solver: the solver's time in a run
+    of `sample_steps` steps minus that in a 0-step run (its own setup and the
+    final output), each timed from the program's "Running Solver" line."""
     if not os.path.exists(REF_BIN):
         return None, "oracle/_ref/plfbs_ref not built"
     with tempfile.TemporaryDirectory(prefix="plfbs_refcpu_") as wd:
@@ -202,9 +224,9 @@ def reference_cpu_throughput(pm, c, nodes, sample_steps=1):
     per_step = max(t_run - t_setup, 1e-9) / sample_steps
     return pm.n_cells / per_step / 1e6, (
         "%d time step(s) of the reference CPU Solver on the same %dx%dx%d mesh and boundary "
-        "conditions (the CPU Solver has no IBM), setup subtracted via a 0-step run "
-        "(%.1f s setup, %.1f s per step), serial" % (sample_steps, NX, NY, NZ, t_setup,
-                                                    per_step))
+        "conditions (the CPU Solver has no IBM), timed from its \"Running Solver\" line with "
+        "the solver's setup subtracted via a 0-step run (%.1f s setup, %.1f s per step), "
+        "serial" % (sample_steps, NX, NY, NZ, t_setup, per_step))
 
 
 REF_GPU_BIN = os.path.join(REPO, "oracle", "_ref", "plfbs_ref_gpu")
@@ -251,6 +273,77 @@ def reference_gpu_throughput(pm, c, nodes, steps=2001, every=100, limit=600):
         "the reference's Solver_gpu.cu path built for sm_100a on the same case (IBM included), "
         "%d steps, median of %d intervals of %d steps between its progress lines (setup and "
         "decade outputs left out), %.3f ms per step" % (steps, len(gaps), every, 1e3 * per_step))
+
+
+def _mem_available():
+    """MemAvailable of the host in bytes (None if unknown)."""
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return None
+
+
+def reference_cpu_aggregate(pm, c, nodes, steps=11, every=2):
+    """Mcell-updates/s of the reference CPU Solver on all the host threads it
+    can use: the Solver is serial, so P independent instances run at once, P
+    the threads available to this process, bounded so that P times one
+    instance's peak memory stays within half of MemAvailable and P times its
+    files (about 100 MB of text output) within half of the free space of the
+    temporary directory. Each instance
+    runs `steps` steps printing a progress line every `every` steps
+    (Solver.cpp:501-508); the Solver writes its text output after a progress
+    line only while its residual crosses a new decade (the first few lines),
+    so an instance's step time is the shorter of its last two intervals over
+    `every`. The aggregate is the sum of the instances' rates. Returns
+    (value, cores, sample)."""
+    import copy
+    import resource
+    from concurrent.futures import ThreadPoolExecutor
+    v1, sample1 = reference_cpu_throughput(pm, copy.copy(c), nodes, sample_steps=1)
+    if v1 is None:
+        return None, 0, sample1
+    threads = len(os.sched_getaffinity(0))
+    rss = resource.getrusage(resource.RUSAGE_CHILDREN).ru_maxrss * 1024  # one instance's peak
+    avail = _mem_available()
+    P = threads if not avail or rss <= 0 else max(1, min(threads, int(0.5 * avail // rss)))
+    import shutil
+    P = max(1, min(P, int(0.5 * shutil.disk_usage(tempfile.gettempdir()).free // (128 << 20))))
+    if P == 1:
+        return v1, 1, sample1
+    with tempfile.TemporaryDirectory(prefix="plfbs_refcpu_") as wd:
+        mesh_dir = os.path.join(wd, "polyMesh")
+        cases.write_polymesh(mesh_dir, pm)
+
+        def instance(i):
+            d = os.path.join(wd, "i%d" % i)
+            os.makedirs(d)
+            ci = copy.copy(c)
+            ci.output_step = every
+            stamps = []
+            _run_ref_cpu(d, pm, ci, nodes, steps, mesh_dir, progress=stamps)
+            gaps = [b - a for a, b in zip(stamps, stamps[1:])]
+            return min(gaps[-2:]) / every if len(gaps) >= 2 else None
+
+        try:
+            with ThreadPoolExecutor(max_workers=P) as ex:
+                per_step = list(ex.map(instance, range(P)))
+        except Exception as e:  # the single-instance figure stands
+            return v1, 1, sample1 + "; %d concurrent instances failed (%s)" % (P, e)
+    if any(t is None or t <= 0 for t in per_step):
+        return v1, 1, sample1 + "; %d concurrent instances gave no step time" % P
+    value = sum(pm.n_cells / t / 1e6 for t in per_step)
+    return value, P, (
+        "%d concurrent instances of the serial reference CPU Solver (the host threads "
+        "available, within half of MemAvailable at %.2f GB per instance and half of the free "
+        "temporary disk space), each %d time steps of "
+        "the same %d-cell mesh timed between its progress lines every %d steps past its "
+        "decade outputs (%.3g-%.3g s per step); sum of their rates. One instance alone: "
+        "%.3f Mcell-updates/s" % (P, rss / 1e9, steps, pm.n_cells, every, min(per_step),
+                                  max(per_step), v1))
 
 
 def reduce_max(x, dist=None, device="cuda"):
@@ -444,7 +537,7 @@ def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
     pm, c, ma, nodes, _ = build_case()
-    value, sample = reference_cpu_throughput(pm, c, nodes, sample_steps=1)
+    value, cores, sample = reference_cpu_aggregate(pm, c, nodes)
     cfg = {"workload": WORKLOAD, "cells": ma.n_cells, "faces": ma.n_faces,
            "nodes": NNODES, "re": RE, "dt": DT,
            "parallelism": "replicas" if world > 1 else "single"}
@@ -456,7 +549,7 @@ def run_reference_arm(args, rank, world):
             "ms_per_step": ma.n_cells / value / 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": cfg,
-            "cpu_baseline": {"value": value, "unit": METRIC, "cores": 1, "kind": "reference",
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
