@@ -324,7 +324,8 @@ int plfbs_ls_weights(const plfbs_mesh_view* mesh, int32_t gradient_mode, double*
                      double* rhs) {
   if (!mesh || !lhs_inv || !rhs) return set_err(nullptr, PLFBS_ERR_ARG, "null argument");
   std::string err;
-  int rc = plfbs::ls_weights(*mesh, gradient_mode, lhs_inv, rhs, err);
+  int rc = plfbs::validate_mesh(*mesh, err, nullptr);  // it indexes with the caller's arrays
+  if (rc == PLFBS_OK) rc = plfbs::ls_weights(*mesh, gradient_mode, lhs_inv, rhs, err);
   if (rc) g_err = err;
   return rc;
 }

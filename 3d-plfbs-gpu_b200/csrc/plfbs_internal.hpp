@@ -210,8 +210,13 @@ struct BoundaryRecords32 {
 };
 void boundary_records32(const Layout& L, double rho0, double uref, BoundaryRecords32& o);
 
+// The checks of a caller's mesh arrays that everything indexing with them
+// relies on (setup.cpp); *K_out (may be null) receives the largest stencil.
+int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out);
+
 // Least-squares weights exactly as gradients::pre_fill_LHS_and_RHS_matrix
-// (gradients.cpp:214-313): lhs_inv [9C], rhs [3 nnz], caller numbering.
+// (gradients.cpp:214-313): lhs_inv [9C], rhs [3 nnz], caller numbering. The
+// mesh must have passed validate_mesh.
 int ls_weights(const plfbs_mesh_view& m, int mode, double* lhs_inv, double* rhs,
                std::string& err);
 

@@ -260,8 +260,12 @@ std::vector<int32_t> cell_order(int C, int Fi, const int32_t* owner, const int32
   return order;
 }
 
-int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bcv,
-                   Layout& L, std::string& err) {
+// The checks of a caller's mesh arrays (first failing index in loop order):
+// sizes, null arrays, face owners and neighbours, positive finite geometry,
+// cell volumes, stencil offsets and entries. Everything that indexes with the
+// caller's indices (the layout, the least-squares export) runs after them.
+// *K_out receives the largest stencil.
+int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out) {
   const int C = m.n_cells, F = m.n_faces, Fi = m.n_internal;
   if (C <= 0 || F <= 0 || Fi < 0 || Fi > F) {
     err = "mesh sizes must satisfy n_cells > 0, n_faces > 0, 0 <= n_internal <= n_faces";
@@ -274,18 +278,10 @@ int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfb
     return PLFBS_ERR_ARG;
   }
   const int B = F - Fi;
-  if (B > 0 && (!bcv.rho_type || !bcv.vel_type || !bcv.value)) {
-    err = "null boundary array";
-    return PLFBS_ERR_ARG;
-  }
   if ((long long)F * 2 >= (1LL << 31)) {
     err = "too many faces for the 31-bit gather encoding";
     return PLFBS_ERR_MESH;
   }
-  L.C = C;
-  L.F = F;
-  L.Fi = Fi;
-  L.B = B;
   const long long T = (long long)C + B;
   // --- mesh consistency (first failing index in loop order) ----------------
   auto face_problem = [&](int f) -> int {
@@ -356,6 +352,24 @@ int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfb
     err = "empty gradient stencil";
     return PLFBS_ERR_MESH;
   }
+  if (K_out) *K_out = K;
+  return PLFBS_OK;
+}
+
+int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bcv,
+                   Layout& L, std::string& err) {
+  int K = 0;
+  const int vrc = validate_mesh(m, err, &K);
+  if (vrc) return vrc;
+  const int C = m.n_cells, F = m.n_faces, Fi = m.n_internal, B = F - Fi;
+  if (B > 0 && (!bcv.rho_type || !bcv.vel_type || !bcv.value)) {
+    err = "null boundary array";
+    return PLFBS_ERR_ARG;
+  }
+  L.C = C;
+  L.F = F;
+  L.Fi = Fi;
+  L.B = B;
   L.K = K;
   const bool cpu = cfg.flavour == PLFBS_FLAVOUR_CPU_SOLVER;
   for (int b = 0; b < B; b++) {

@@ -312,7 +312,9 @@ int plfbs_cell_order(const plfbs_mesh_view* mesh, int32_t renumber, int32_t* ord
 
 /* Host-only: the least-squares weights as gradients::pre_fill_LHS_and_RHS_matrix
  * computes them (gradients.cpp:214-313, determinant as written at :282-284):
- * lhs_inv [9C] row-major, rhs [3 nnz] per stencil entry. No GPU needed. */
+ * lhs_inv [9C] row-major, rhs [3 nnz] per stencil entry. The mesh is checked
+ * first as plfbs_create checks it (PLFBS_ERR_ARG / PLFBS_ERR_MESH with the first
+ * failing index). No GPU needed. */
 int plfbs_ls_weights(const plfbs_mesh_view* mesh, int32_t gradient_mode, double* lhs_inv,
                      double* rhs);
 
