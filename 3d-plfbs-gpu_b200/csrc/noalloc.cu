@@ -44,6 +44,10 @@ __device__ __forceinline__ double na_warp_sum(double v) {
 // Block b reduces cells [b * 4096, (b + 1) * 4096); the last block to finish
 // sums the partials in block order and writes
 // out = {max_error, rho_rms, u_rms, v_rms, w_rms}.
+// VEC: the residual array is 32-byte aligned and each cell's record moves as
+// one 256-bit load; otherwise (a caller's pointer of lesser alignment) as four
+// 8-byte loads.
+template <bool VEC>
 __global__ void __launch_bounds__(kNaThreads)
 k_residual_norms_scratch(const double* __restrict__ res, long long n, double inv_ref_rho,
                          double inv_ref_mom, double* scratch, double* out) {
@@ -53,7 +57,17 @@ k_residual_norms_scratch(const double* __restrict__ res, long long n, double inv
   for (int k = 0; k < kNaCellsPerThread; k++) {
     const long long i = base + (long long)k * kNaThreads + threadIdx.x;
     if (i < n) {
-      const double u = res[4 * i], v = res[4 * i + 1], w = res[4 * i + 2], r = res[4 * i + 3];
+      double u, v, w, r;
+      if (VEC) {
+        asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+            : "=d"(u), "=d"(v), "=d"(w), "=d"(r)
+            : "l"(res + 4 * i));
+      } else {
+        u = res[4 * i];
+        v = res[4 * i + 1];
+        w = res[4 * i + 2];
+        r = res[4 * i + 3];
+      }
       s[0] = fma(r, r, s[0]);
       s[1] = fma(u, u, s[1]);
       s[2] = fma(v, v, s[2]);
@@ -111,7 +125,10 @@ k_residual_norms_scratch(const double* __restrict__ res, long long n, double inv
   }
 }
 
-// Device address of g_noalloc_scratch, looked up once per device.
+// Device address of g_noalloc_scratch per device: looked up again on every
+// call made outside stream capture (so it follows a device reset or another
+// driver context), and the last address seen is what a call under capture
+// uses.
 std::mutex g_na_mutex;
 double* g_na_ptr[kNaMaxDevices] = {};
 
@@ -138,29 +155,48 @@ extern "C" int plfbs_residual_norms_noalloc(const double* residual, int64_t n_ce
     return na_fail(PLFBS_ERR_ARG, "residual_norms_noalloc: ref_rho and max_velocity must be > 0");
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kNaMaxDevices)
+  if (e != cudaSuccess)
     return na_fail(PLFBS_ERR_NO_DEVICE, std::string("residual_norms_noalloc: cudaGetDevice: ") +
                                             cudaGetErrorString(e));
-  if (!g_na_ptr[dev]) {
-    // first call on this device: look up the device address of the scratch
+  if (dev < 0 || dev >= kNaMaxDevices)
+    return na_fail(PLFBS_ERR_NO_DEVICE, "residual_norms_noalloc: device ordinal " +
+                                            std::to_string(dev) + " is beyond the " +
+                                            std::to_string(kNaMaxDevices) +
+                                            " devices this entry point supports");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(s, &cap);
+  if (e != cudaSuccess) {
+    cap = cudaStreamCaptureStatusActive;  // the query itself is refused during some captures
+    cudaGetLastError();
+  }
+  if (cap == cudaStreamCaptureStatusNone) {
+    // the device address of the scratch in the current context
     double* p = nullptr;
     e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
       return na_fail(PLFBS_ERR_CUDA, std::string("residual_norms_noalloc: cudaGetSymbolAddress: ") +
                                          cudaGetErrorString(e));
     g_na_ptr[dev] = p;
+  } else if (!g_na_ptr[dev]) {
+    return na_fail(PLFBS_ERR_STATE,
+                   "residual_norms_noalloc: the first call on a device must come before any "
+                   "stream capture (it looks up the scratch's device address)");
   }
   double* scratch = g_na_ptr[dev];
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   // the completion counter must start at zero whatever an earlier call left
   e = cudaMemsetAsync(scratch + 4 * kNaMaxBlocks, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess)
     return na_fail(PLFBS_ERR_CUDA, std::string("residual_norms_noalloc: cudaMemsetAsync: ") +
                                        cudaGetErrorString(e));
   const int blocks = (int)((n_cells + kNaCellsPerBlock - 1) / kNaCellsPerBlock);
-  k_residual_norms_scratch<<<blocks, kNaThreads, 0, s>>>(residual, n_cells, 1.0 / ref_rho,
-                                                         1.0 / (ref_rho * max_velocity), scratch,
-                                                         out);
+  const double irr = 1.0 / ref_rho, irm = 1.0 / (ref_rho * max_velocity);
+  if ((reinterpret_cast<uintptr_t>(residual) & 31) == 0)
+    k_residual_norms_scratch<true><<<blocks, kNaThreads, 0, s>>>(residual, n_cells, irr, irm,
+                                                                 scratch, out);
+  else
+    k_residual_norms_scratch<false><<<blocks, kNaThreads, 0, s>>>(residual, n_cells, irr, irm,
+                                                                  scratch, out);
   e = cudaGetLastError();
   if (e != cudaSuccess)
     return na_fail(PLFBS_ERR_CUDA, std::string("residual_norms_noalloc: launch: ") +

@@ -10,7 +10,7 @@
  *                                                   src/Solver_gpu.cu:150-917)
  * called from program.cpp:107-109. A thin C++ shim with that exact signature
  * copies the mesh/BC/object getters into the plain views below and drives
- * create -> set_state -> run -> get_state -> destroy (see INTEGRATION.md).
+ * create -> set_state -> run -> get_state -> destroy.
  *
  * Conventions: all arrays are borrowed for the duration of the call only and
  * use the caller's numbering (cells 0..C-1, then one ghost per boundary face,
@@ -356,11 +356,14 @@ int plfbs_memory_bytes(plfbs_ctx* ctx, int64_t* bytes);
  * Its only scratch is a file-scope __device__ array of 65,792 bytes (2048
  * block partials + a counter) that every GPU loading this library holds until
  * exit, so n_cells is limited to 8,388,608; larger inputs are rejected with
- * PLFBS_ERR_ARG. The first call on each device looks up that array's device
- * address with cudaGetSymbolAddress; make that first call before any stream
- * capture. All calls share the array: calls that overlap on the GPU (other
- * streams, other host threads) race and must be serialised by the caller.
- * Errors are reported through plfbs_last_error(NULL). */
+ * PLFBS_ERR_ARG. A call made outside stream capture looks up that array's
+ * device address in the current context with cudaGetSymbolAddress; a call
+ * under capture reuses the address the last uncaptured call on that device
+ * found, so make the first call on each device before any stream capture
+ * (and one again after a device reset). All calls share the array: calls
+ * that overlap on the GPU (other streams, other host threads) race and must
+ * be serialised by the caller. Errors are reported through
+ * plfbs_last_error(NULL). */
 int plfbs_residual_norms_noalloc(const double* residual, int64_t n_cells, double ref_rho,
                                  double max_velocity, double* out, void* stream);
 

@@ -1,6 +1,6 @@
 """Regenerate the golden fixtures tests/golden/<case>.npz from the reference.
 
-    make -C oracle/ref && python tests/golden/make_golden.py
+    make -C oracle/ref REF=<reference checkout>/src && python tests/golden/make_golden.py
 
 Runs oracle/_ref/plfbs_ref (the reference program, built from its own
 sources; its CUDA kernels execute serially on the host) on each case of

@@ -55,6 +55,50 @@ def test_noalloc_norms_match_run_twice(plfbs_lib):
     s.close()
 
 
+def _norms_numpy(res, ref_rho, u_ref):
+    """The residual norms of residuals.cpp:95-147 in float64 numpy."""
+    n = res.shape[0]
+    rms = np.sqrt((res.astype(np.float64) ** 2).sum(axis=0) / n)  # u, v, w, rho
+    rho = rms[3] / ref_rho
+    u, v, w = rms[:3] / (ref_rho * u_ref)
+    return np.array([max(w, u, v), rho, u, v, w])
+
+
+@pytest.mark.parametrize("n", [4097, 1000003, MAX_CELLS])
+def test_noalloc_random_sizes_no_device_memory(plfbs_lib, n):
+    """Ragged and maximal sizes against numpy, twice in a row, with the device's
+    free memory and torch's allocated bytes unchanged across the second call;
+    the same residuals 8 bytes off a 32-byte boundary take the scalar loads."""
+    import torch
+
+    rng = np.random.Generator(np.random.PCG64(n))
+    res_h = rng.standard_normal((n, 4)) * np.array([1e-3, 2e-3, 5e-4, 1e-4])
+    want = _norms_numpy(res_h, 1.2, 0.05)
+    buf = torch.zeros(4 * n + 4, dtype=torch.float64, device="cuda")
+    buf[:4 * n] = torch.from_numpy(res_h.ravel()).cuda()
+    out = torch.full((2, 5), float("nan"), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    assert buf.data_ptr() % 32 == 0
+    for call in range(2):
+        torch.cuda.synchronize()
+        free0, alloc0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
+        rc = plfbs_lib.plfbs_residual_norms_noalloc(buf.data_ptr(), n, 1.2, 0.05,
+                                                    out[call].data_ptr(), stream)
+        assert rc == 0, plfbs_lib.plfbs_last_error(None)
+        torch.cuda.synchronize()
+        if call == 1:  # the first call may load the library's device code
+            assert torch.cuda.mem_get_info()[0] == free0
+            assert torch.cuda.memory_allocated() == alloc0
+        assert rel_err(out[call].cpu().numpy(), want) < TOL, (call, out[call], want)
+    # unaligned: the same values one double further on
+    buf[1:4 * n + 1] = torch.from_numpy(res_h.ravel()).cuda()
+    rc = plfbs_lib.plfbs_residual_norms_noalloc(buf.data_ptr() + 8, n, 1.2, 0.05,
+                                                out[0].data_ptr(), stream)
+    assert rc == 0, plfbs_lib.plfbs_last_error(None)
+    torch.cuda.synchronize()
+    assert rel_err(out[0].cpu().numpy(), want) < TOL
+
+
 def test_noalloc_rejects_oversize_input(plfbs_lib):
     import torch
 
