@@ -466,26 +466,29 @@ def write_polymesh(dirpath, pm: PolyMesh):
     with open(os.path.join(dirpath, "owner"), "w") as f:
         f.write(_header("labelList", "owner", note))
         f.write("\n%d\n(\n" % F)
-        f.write("\n".join(str(int(v)) for v in pm.owner))
+        f.write("\n".join(map(str, np.asarray(pm.owner).tolist())))
         f.write("\n)\n")
     with open(os.path.join(dirpath, "neighbour"), "w") as f:
         f.write(_header("labelList", "neighbour", note))
         f.write("\n%d\n(\n" % Fi)
-        f.write("\n".join(str(int(v)) for v in pm.neighbour))
+        f.write("\n".join(map(str, np.asarray(pm.neighbour).tolist())))
         f.write("\n)\n")
     with open(os.path.join(dirpath, "points"), "w") as f:
         f.write(_header("vectorField", "points"))
         f.write("\n%d\n(\n" % P)
-        f.write("\n".join("(%.9g %.9g %.9g)" % (float(x), float(y), float(z))
-                          for x, y, z in pm.points))
+        # %.9g of each coordinate as a Python float (the points are float32)
+        f.write("\n".join(map("(%.9g %.9g %.9g)".__mod__,
+                              map(tuple, np.asarray(pm.points, np.float64).tolist()))))
         f.write("\n)\n")
     with open(os.path.join(dirpath, "faces"), "w") as f:
         f.write(_header("faceList", "faces"))
         f.write("\n%d\n(\n" % F)
-        lines = []
-        for row, n in zip(pm.faces, pm.nverts):
-            lines.append("%d(%s)" % (n, " ".join(str(int(v)) for v in row[:n])))
-        f.write("\n".join(lines))
+        nverts = np.asarray(pm.nverts).tolist()
+        rows = np.asarray(pm.faces).tolist()
+        fmt = {}
+        for n in set(nverts):
+            fmt[n] = ("%d(" % n + " ".join(["%d"] * n) + ")").__mod__
+        f.write("\n".join(fmt[n](tuple(row[:n])) for row, n in zip(rows, nverts)))
         f.write("\n)\n")
     with open(os.path.join(dirpath, "boundary"), "w") as f:
         f.write(_header("polyBoundaryMesh", "boundary"))

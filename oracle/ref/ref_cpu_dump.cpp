@@ -13,6 +13,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <iostream>
 #include <string>
 #include <vector>
 
@@ -60,5 +61,8 @@ void __wrap__ZN8Solution6outputENSt7__cxx1112basic_stringIcSt11char_traitsIcESaI
   }
   __real__ZN8Solution6outputENSt7__cxx1112basic_stringIcSt11char_traitsIcESaIcEEER16global_variablesR15domain_geometry(
       self, loc, g, d);
+  // End marker of the text output, for a caller that times the solver's
+  // steps between its progress lines and must leave this output out.
+  std::cout << "plfbs-output-done" << std::endl;
 }
 }

@@ -101,6 +101,39 @@ def build(name):
     return dict(pm=pm, case=c, nodes=nodes, state0=state0, ma=ma)
 
 
+def build_tgv_tets(n=12, jitter=0.2, gradient_calc="GG", steps=100, seed=11):
+    """The unstructured stress case at small size: n^3 hexes with interior
+    nodes jittered uniformly by +-jitter of the spacing (seeded), each split
+    into 6 tetrahedra, no-slip walls (Dirichlet velocity, Neumann density), a
+    Taylor-Green field of amplitude 0.05 at rest density, Re 400 on L = n,
+    dt 0.05. Green-Gauss gradients by default: their 2 V I matrix inverts
+    exactly under the reference's cofactor formula, so the reference itself
+    runs tetrahedra with a sound gradient (its least-squares inverse does not,
+    gradients.cpp:282-284). Returns dict(pm, case, nodes, state0, ma)."""
+    u0 = 0.05
+    pm = cases.jittered_tet_box(n, jitter=jitter, seed=seed, patch_types=["wall"] * 6)
+    c = cases.Case(mesh_dir="", X=n, Y=n, Z=n, dt=0.05, mach=u0, reynolds=400.0, ref_length=n,
+                   tolerance=0.0, steps=steps, gpu_solver=0, gradient_calc=gradient_calc,
+                   bcs=[cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann")])
+    ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
+    x = np.asarray(ma.cell_centroid).reshape(-1, 3) * (2 * np.pi / n)
+    s0 = np.zeros((ma.total_cells, 4))
+    s0[:, 0] = u0 * np.sin(x[:, 0]) * np.cos(x[:, 1]) * np.cos(x[:, 2])
+    s0[:, 1] = -u0 * np.cos(x[:, 0]) * np.sin(x[:, 1]) * np.cos(x[:, 2])
+    s0[:, 3] = 1.0
+    return dict(pm=pm, case=c, nodes=np.zeros((0, 3)), state0=s0, ma=ma)
+
+
+def failure_step(lines):
+    """The step at which the reference CPU Solver stopped on a diverged field
+    ("rho failure" / "nan failure" followed by the step, Solver.cpp:448-493),
+    or None."""
+    for k, line in enumerate(lines):
+        if line.strip() in ("rho failure", "nan failure"):
+            return int(lines[k + 1])
+    return None
+
+
 def oracle_cfg(d):
     """The scalar configuration the solver sees for a golden case."""
     c = d["case"]

@@ -35,9 +35,10 @@ def write_restart(out_dir, state):
 
 
 def run_reference(workdir, pm, case, nodes=None, init_state=None, dump=True, timeout=600,
-                  binary=None):
+                  binary=None, log=None):
     """Write ``pm``/``case`` under ``workdir``, run the reference program (or
-    ``binary``, another build of it), return the .npy dumps it wrote."""
+    ``binary``, another build of it), return the .npy dumps it wrote. With a
+    list ``log``, the console lines of the (last) run are appended to it."""
     binary = binary or REF_BIN
     workdir = os.path.abspath(workdir)
     os.makedirs(workdir, exist_ok=True)
@@ -68,7 +69,10 @@ def run_reference(workdir, pm, case, nodes=None, init_state=None, dump=True, tim
     os.makedirs(dump_dir, exist_ok=True)
     if dump:
         env["PLFBS_REF_DUMP"] = dump_dir
-    subprocess.run([binary, xml], cwd=workdir, env=env, check=True,
-                   stdout=subprocess.DEVNULL, timeout=timeout)
+    p = subprocess.run([binary, xml], cwd=workdir, env=env, check=True, timeout=timeout,
+                       stdout=subprocess.PIPE if log is not None else subprocess.DEVNULL,
+                       text=True)
+    if log is not None:
+        log.extend(p.stdout.splitlines())
     return {os.path.splitext(os.path.basename(p))[0]: np.load(p)
             for p in glob.glob(os.path.join(dump_dir, "*.npy"))}

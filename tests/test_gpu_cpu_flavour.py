@@ -50,3 +50,59 @@ def test_gpu_flavour_differs_from_the_cpu_solver(plfbs_lib):
     s.run(int(g["steps"][0]))
     C = d["ma"].n_cells
     assert rel_l2(s.get_state()[:C, 0], g["final_state"][:C, 0]) > 1e-6
+
+
+def _tet_solver(d, flavour):
+    c = d["case"]
+    cfg = dict(visc=c.visc, gamma=1.0, dt=c.dt, domain_dt=0.5, pressure_gradient=0.0,
+               channel_height=c.Y, max_velocity=c.mach, ref_rho=1.0, tolerance=0.0,
+               origin=(0, 0, 0), lengths=(c.X, c.Y, c.Z), gradient_mode=capi.GRAD_GREEN_GAUSS,
+               renumber=1, flavour=flavour)
+    rt, vt, val = cases.bc_arrays(d["ma"], c)
+    return capi.Solver(d["ma"], rt, vt, val, cfg)
+
+
+def test_cpu_flavour_on_20_percent_jittered_tets(plfbs_lib, tmp_path):
+    """The unstructured stress mesh at small size (12^3 hexes, nodes jittered
+    +-20 %, 10,368 tets, Taylor-Green, Re 400, Green-Gauss): 100 steps against
+    the reference CPU Solver run here (1e-10 relative L2), then on to the
+    reference's own divergence test, which both fail in the same step."""
+    import os
+
+    import refrun
+    from conftest import REPO
+    binary = os.path.join(REPO, "oracle", "_ref", "plfbs_ref_cpu")
+    if not os.path.exists(binary):
+        pytest.skip("oracle/_ref/plfbs_ref_cpu not built (needs the reference sources)")
+    d = golden_cases.build_tgv_tets(jitter=0.2, steps=100)
+    want = refrun.run_reference(str(tmp_path / "r100"), d["pm"], d["case"],
+                                init_state=d["state0"], binary=binary)["cpu_final_state"]
+    s = _tet_solver(d, capi.FLAVOUR_CPU_SOLVER)
+    s.set_state(d["state0"])
+    st, _ = s.run(100)
+    C = d["ma"].n_cells
+    got = s.get_state()[:C]
+    for k in range(4):
+        assert rel_l2(got[:, k], want[:C, k]) < 1e-10, k
+    d400 = golden_cases.build_tgv_tets(jitter=0.2, steps=400)
+    log = []
+    refrun.run_reference(str(tmp_path / "r400"), d400["pm"], d400["case"],
+                         init_state=d400["state0"], binary=binary, dump=False, log=log)
+    fail = golden_cases.failure_step(log)  # the reference's loop index t
+    assert fail is not None
+    st, _ = s.run(400)
+    assert st["rc"] == capi.ERR_DIVERGED
+    assert st["steps_done"] == fail + 1
+    s.close()
+
+
+def test_gpu_flavour_diverges_on_20_percent_jittered_tets(plfbs_lib):
+    """The GPU kernels' tables on the same mesh fail the same test too (the
+    reference's GPU path has no tetrahedra to compare with: exactly six
+    neighbours, LBFS.cu:1549-1556)."""
+    d = golden_cases.build_tgv_tets(jitter=0.2, steps=400)
+    s = _tet_solver(d, capi.FLAVOUR_GPU)
+    s.set_state(d["state0"])
+    st, _ = s.run(400)
+    assert st["rc"] == capi.ERR_DIVERGED and 250 < st["steps_done"] < 400
+    s.close()
