@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <new>
 #include <sstream>
@@ -77,6 +78,17 @@ int pool_alloc(plfbs_ctx* ctx, void** dst, size_t n) {
   ctx->allocs.push_back(*dst);
   ctx->bytes += (int64_t)n;
   return PLFBS_OK;
+}
+
+int scratch_alloc(plfbs_ctx* ctx, void** dst, size_t n) {
+  cudaMemPool_t pool = device_pool(ctx->device);
+  if (!pool) return set_err(ctx, PLFBS_ERR_CUDA, "device memory pool creation failed");
+  CK(cudaMallocFromPoolAsync(dst, std::max<size_t>(n, 16), pool, ctx->stream));
+  return PLFBS_OK;
+}
+
+void scratch_free(plfbs_ctx* ctx, void* p) {
+  if (p) cudaFreeAsync(p, ctx->stream);
 }
 
 int dev_alloc(plfbs_ctx* ctx, void** dst, size_t n) {
@@ -156,21 +168,20 @@ int capture_step(plfbs_ctx* ctx) {
 
 int reset_force(plfbs_ctx* ctx) {
   const int C = ctx->L.C;
-  if (ctx->args.fforce_x) {
-    std::vector<float> base(C, (float)(ctx->cfg.pressure_gradient / ctx->cfg.max_velocity));
-    CK(cudaMemcpyAsync(ctx->args.fforce_x, base.data(), C * sizeof(float), cudaMemcpyHostToDevice,
-                       ctx->stream));
-    CK(cudaMemsetAsync(ctx->args.fforce_y, 0, C * sizeof(float), ctx->stream));
-    CK(cudaMemsetAsync(ctx->args.fforce_z, 0, C * sizeof(float), ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+  const KernelArgs& a = ctx->args;
+  if (a.fforce_x) {
+    plfbs::launch_fill(a.fforce_x, C, (float)(ctx->cfg.pressure_gradient / ctx->cfg.max_velocity),
+                       ctx->stream);
+    CK(cudaMemsetAsync(a.fforce_y, 0, C * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(a.fforce_z, 0, C * sizeof(float), ctx->stream));
+  } else if (a.force_x) {
+    plfbs::launch_fill(a.force_x, C, ctx->cfg.pressure_gradient, ctx->stream);
+    CK(cudaMemsetAsync(a.force_y, 0, C * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(a.force_z, 0, C * sizeof(double), ctx->stream));
+  } else {
     return PLFBS_OK;
   }
-  if (!ctx->args.force_x) return PLFBS_OK;
-  std::vector<double> base(C, ctx->cfg.pressure_gradient);
-  CK(cudaMemcpyAsync(ctx->args.force_x, base.data(), C * sizeof(double), cudaMemcpyHostToDevice,
-                     ctx->stream));
-  CK(cudaMemsetAsync(ctx->args.force_y, 0, C * sizeof(double), ctx->stream));
-  CK(cudaMemsetAsync(ctx->args.force_z, 0, C * sizeof(double), ctx->stream));
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   return PLFBS_OK;
 }
@@ -465,6 +476,13 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     NvtxRange r("compact layout");
     if ((rc = build_compact_layout(ctx))) return fail(rc);
   }
+  {  // caller index -> device index, cells then ghosts (state transfer)
+    std::vector<int32_t> perm((size_t)T);
+    for (long long o = 0; o < L.C; o++) perm[o] = L.cell_new_of_old[o];
+    for (long long b = 0; b < L.B; b++) perm[L.C + b] = L.C + L.bc_new_of_old[b];
+    if ((rc = dev_upload(ctx, &p, perm))) return fail(rc);
+    ctx->perm = static_cast<int32_t*>(p);
+  }
   if (fp32) {
     plfbs::BoundaryRecords32 b32;
     plfbs::boundary_records32(L, cfg->ref_rho, cfg->max_velocity, b32);
@@ -522,6 +540,28 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     a.node_vel = static_cast<double*>(p);
     if ((rc = dev_alloc(ctx, &p, 3 * (size_t)N * sizeof(double)))) return fail(rc);
     a.node_force = static_cast<double*>(p);
+    {  // the kernels take the nodes by the cell of their reference position
+       // (the stencil origin of k_ibm), so a warp's nodes share cells
+      std::vector<int64_t> key(N);
+      for (int n = 0; n < N; n++) {
+        const double* xr = ibm->x_ref + 3 * (size_t)n;
+        const double r0 = (xr[0] - cfg->origin[0]) / dx;
+        const double r1 = std::fabs((xr[1] - cfg->origin[1]) / dx);
+        const double r2 = std::fabs((xr[2] - cfg->origin[2]) / dx);
+        const double lo[3] = {std::round(r0) - 1, std::round(r1) - 1, std::round(r2) - 1};
+        const bool ok = std::fabs(lo[0]) < 1e9 && std::fabs(lo[1]) < 1e9 &&
+                        std::fabs(lo[2]) < 1e9;  // false for NaN too
+        key[n] = ok ? (int64_t)lo[0] + (int64_t)lo[1] * a.ibm_xc +
+                          (int64_t)lo[2] * a.ibm_xc * (int64_t)a.ibm_yc
+                    : std::numeric_limits<int64_t>::max();
+      }
+      std::vector<int32_t> order(N);
+      for (int n = 0; n < N; n++) order[n] = n;
+      std::stable_sort(order.begin(), order.end(),
+                       [&](int32_t u, int32_t v) { return key[u] < key[v]; });
+      if ((rc = dev_upload(ctx, &p, order))) return fail(rc);
+      a.ibm_order = static_cast<const int32_t*>(p);
+    }
     if ((rc = reset_force(ctx))) return fail(rc);
   }
   if ((rc = capture_step(ctx))) return fail(rc);
@@ -622,39 +662,32 @@ int plfbs_release_cached(int32_t device) {
 namespace {
 
 // Uploads a state given in the caller's numbering (FP32 form: converted to
-// deviation units), resets the run status and seeds the RK accumulators.
+// deviation units), resets the run status and seeds the RK accumulators. The
+// four arrays go up as they are (from pinned memory at the copy engines'
+// rate, pageable memory through the driver's staging) and one kernel
+// interleaves and renumbers them into the state records.
 int seed_state(plfbs_ctx* ctx, const double* rho, const double* u, const double* v,
                const double* w, bool conserved) {
   NvtxRange range(conserved ? "plfbs_warm_start" : "plfbs_set_state");
   const Layout& L = ctx->L;
   const int64_t T = (int64_t)L.C + L.B;
-  if (ctx->cfg.precision == PLFBS_FP32_DEVIATION) {
-    // deviation units: velocity / U, rho - rho0
-    const double U = ctx->cfg.max_velocity, r0 = ctx->cfg.ref_rho;
-    std::vector<float> q(4 * (size_t)T);
-    for (int64_t o = 0; o < T; o++) {
-      const int64_t n = o < L.C ? L.cell_new_of_old[o] : L.C + L.bc_new_of_old[o - L.C];
-      q[4 * n] = (float)(u[o] / U);
-      q[4 * n + 1] = (float)(v[o] / U);
-      q[4 * n + 2] = (float)(w[o] / U);
-      q[4 * n + 3] = (float)(rho[o] - r0);
-    }
-    CK(cudaMemcpyAsync(ctx->args.state, q.data(), q.size() * sizeof(float),
-                       cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-  } else {
-    std::vector<double> q(4 * (size_t)T);
-    for (int64_t o = 0; o < T; o++) {
-      const int64_t n = o < L.C ? L.cell_new_of_old[o] : L.C + L.bc_new_of_old[o - L.C];
-      q[4 * n] = u[o];
-      q[4 * n + 1] = v[o];
-      q[4 * n + 2] = w[o];
-      q[4 * n + 3] = rho[o];
-    }
-    CK(cudaMemcpyAsync(ctx->args.state, q.data(), q.size() * sizeof(double),
-                       cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+  void* buf = nullptr;
+  TRY(scratch_alloc(ctx, &buf, 4 * sizeof(double) * (size_t)T));
+  double* d = static_cast<double*>(buf);
+  const double* src[4] = {rho, u, v, w};
+  int rc = PLFBS_OK;
+  for (int k = 0; k < 4 && rc == PLFBS_OK; k++) {
+    const cudaError_t e = cudaMemcpyAsync(d + k * T, src[k], sizeof(double) * (size_t)T,
+                                          cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess)
+      rc = set_err(ctx, PLFBS_ERR_CUDA, std::string("state upload: ") + cudaGetErrorString(e));
   }
+  if (rc == PLFBS_OK)
+    plfbs::launch_state_in(ctx->perm, T, d, d + T, d + 2 * T, d + 3 * T, ctx->cfg.precision,
+                           ctx->cfg.max_velocity, ctx->cfg.ref_rho, ctx->args.state, ctx->stream);
+  scratch_free(ctx, buf);
+  TRY(rc);
+  CK(cudaGetLastError());
   CK(cudaMemsetAsync(ctx->args.stats, 0, sizeof(DevStats), ctx->stream));
   plfbs::launch_seed(ctx->args, ctx->cfg.precision, conserved, ctx->stream);
   CK(cudaGetLastError());
@@ -715,19 +748,6 @@ int64_t checkpoint_size(const plfbs_ctx* ctx) {
   return (int64_t)sizeof(CheckpointHeader) + 4 * v * (T + ctx->L.C) + 9 * 8 * (int64_t)ctx->N;
 }
 
-// Moves n records of `rec` bytes between the caller's order (host) and the
-// internal order; `to_host` gathers, otherwise scatters.
-void permute_records(const plfbs_ctx* ctx, int64_t n, size_t rec, const char* src, char* dst,
-                     bool to_host) {
-  const Layout& L = ctx->L;
-  for (int64_t o = 0; o < n; o++) {
-    const int64_t k = o < L.C ? L.cell_new_of_old[o] : L.C + L.bc_new_of_old[o - L.C];
-    if (to_host)
-      std::memcpy(dst + o * rec, src + k * rec, rec);
-    else
-      std::memcpy(dst + k * rec, src + o * rec, rec);
-  }
-}
 }  // namespace
 
 int plfbs_checkpoint_bytes(plfbs_ctx* ctx, int64_t* bytes) {
@@ -768,16 +788,25 @@ int plfbs_save_checkpoint(plfbs_ctx* ctx, void* buf, int64_t bytes) {
   char* out = static_cast<char*>(buf);
   std::memcpy(out, &h, sizeof h);
   out += sizeof h;
-  std::vector<char> raw(rec * (size_t)T);
-  CK(cudaMemcpyAsync(raw.data(), ctx->args.state, rec * (size_t)T, cudaMemcpyDeviceToHost,
-                     ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  permute_records(ctx, T, rec, raw.data(), out, true);
+  // the state and the RK accumulator gathered into the caller's order on the
+  // device, then copied out
+  void* stage = nullptr;
+  TRY(scratch_alloc(ctx, &stage, rec * (size_t)T));
+  plfbs::launch_records(ctx->perm, T, (int)rec, ctx->args.state, stage, true, ctx->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, stage, rec * (size_t)T, cudaMemcpyDeviceToHost, ctx->stream);
   out += rec * (size_t)T;
-  CK(cudaMemcpyAsync(raw.data(), ctx->args.t1, rec * (size_t)L.C, cudaMemcpyDeviceToHost,
-                     ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  permute_records(ctx, L.C, rec, raw.data(), out, true);
+  if (e == cudaSuccess) {
+    plfbs::launch_records(ctx->perm, L.C, (int)rec, ctx->args.t1, stage, true, ctx->stream);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, stage, rec * (size_t)L.C, cudaMemcpyDeviceToHost, ctx->stream);
+  scratch_free(ctx, stage);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess)
+    return set_err(ctx, PLFBS_ERR_CUDA, std::string("checkpoint read-back: ") + cudaGetErrorString(e));
   out += rec * (size_t)L.C;
   if (ctx->N > 0) {
     const size_t n = 3 * (size_t)ctx->N * sizeof(double);
@@ -809,19 +838,29 @@ int plfbs_load_checkpoint(plfbs_ctx* ctx, const void* buf, int64_t bytes) {
   const size_t rec = ctx->cfg.precision == PLFBS_FP32_DEVIATION ? 16 : 32;
   const int64_t T = (int64_t)L.C + L.B;
   const char* in = static_cast<const char*>(buf) + sizeof h;
-  std::vector<char> raw(rec * (size_t)T);
-  permute_records(ctx, T, rec, in, raw.data(), false);
-  CK(cudaMemcpyAsync(ctx->args.state, raw.data(), rec * (size_t)T, cudaMemcpyHostToDevice,
-                     ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  // scattered from the caller's order on the device; at a step boundary t0
+  // equals t1
+  void* stage = nullptr;
+  TRY(scratch_alloc(ctx, &stage, rec * (size_t)T));
+  cudaError_t e = cudaMemcpyAsync(stage, in, rec * (size_t)T, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) {
+    plfbs::launch_records(ctx->perm, T, (int)rec, stage, ctx->args.state, false, ctx->stream);
+    e = cudaGetLastError();
+  }
   in += rec * (size_t)T;
-  permute_records(ctx, L.C, rec, in, raw.data(), false);
-  // at a step boundary t0 equals t1
-  CK(cudaMemcpyAsync(ctx->args.t1, raw.data(), rec * (size_t)L.C, cudaMemcpyHostToDevice,
-                     ctx->stream));
-  CK(cudaMemcpyAsync(ctx->args.t0, raw.data(), rec * (size_t)L.C, cudaMemcpyHostToDevice,
-                     ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(stage, in, rec * (size_t)L.C, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) {
+    plfbs::launch_records(ctx->perm, L.C, (int)rec, stage, ctx->args.t1, false, ctx->stream);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->args.t0, ctx->args.t1, rec * (size_t)L.C, cudaMemcpyDeviceToDevice,
+                        ctx->stream);
+  scratch_free(ctx, stage);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess)
+    return set_err(ctx, PLFBS_ERR_CUDA, std::string("checkpoint upload: ") + cudaGetErrorString(e));
   in += rec * (size_t)L.C;
   if (ctx->N > 0) {
     const size_t n = 3 * (size_t)ctx->N * sizeof(double);
@@ -964,15 +1003,21 @@ int plfbs_get_state(plfbs_ctx* ctx, double* rho, double* u, double* v, double* w
   const int64_t T = (int64_t)L.C + L.B;
   if (!rho || !u || !v || !w || n_total != T)
     return set_err(ctx, PLFBS_ERR_ARG, "get_state needs 4 arrays of n_cells + n_boundary values");
-  std::vector<double> q;
-  TRY(download4(ctx, ctx->args.state, (size_t)T, q, false));
-  for (int64_t o = 0; o < T; o++) {
-    const int64_t n = o < L.C ? L.cell_new_of_old[o] : L.C + L.bc_new_of_old[o - L.C];
-    u[o] = q[4 * n];
-    v[o] = q[4 * n + 1];
-    w[o] = q[4 * n + 2];
-    rho[o] = q[4 * n + 3];
-  }
+  void* buf = nullptr;
+  TRY(scratch_alloc(ctx, &buf, 4 * sizeof(double) * (size_t)T));
+  double* d = static_cast<double*>(buf);
+  plfbs::launch_state_out(ctx->perm, T, ctx->args.state, ctx->cfg.precision,
+                          ctx->cfg.max_velocity, ctx->cfg.ref_rho, d, d + T, d + 2 * T, d + 3 * T,
+                          ctx->stream);
+  cudaError_t e = cudaGetLastError();
+  double* dst[4] = {rho, u, v, w};
+  for (int k = 0; k < 4 && e == cudaSuccess; k++)
+    e = cudaMemcpyAsync(dst[k], d + k * T, sizeof(double) * (size_t)T, cudaMemcpyDeviceToHost,
+                        ctx->stream);
+  scratch_free(ctx, buf);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess)
+    return set_err(ctx, PLFBS_ERR_CUDA, std::string("state read-back: ") + cudaGetErrorString(e));
   return PLFBS_OK;
 }
 
@@ -1177,6 +1222,80 @@ int plfbs_profile_steps(plfbs_ctx* ctx, int64_t n_steps, double* ms) {
   }
   for (auto& e : ev) cudaEventDestroy(e);
   CK(cudaGetLastError());
+  TRY(read_stats(ctx));
+  return check_fault(ctx);
+}
+
+int plfbs_profile_kernels(plfbs_ctx* ctx, int64_t launches, double* ms) {
+  NvtxRange range("plfbs_profile_kernels");
+  TRY(check_ctx(ctx));
+  if (!ms || launches <= 0) return set_err(ctx, PLFBS_ERR_ARG, "need launches > 0 and an output");
+  if (!ctx->have_state || ctx->stages_done != 0)
+    return set_err(ctx, PLFBS_ERR_STATE, "profile needs a state at a step boundary");
+  TRY(read_stats(ctx));
+  if (ctx->stats_host->halt)
+    return set_err(ctx, PLFBS_ERR_STATE, "the run has halted: its kernels return at entry");
+  for (int k = 0; k < 5; k++) ms[k] = 0.0;
+  // everything the launches write that a later step reads, copied aside on
+  // the device and put back afterwards (flux, gradients and partial sums are
+  // recomputed by the next step before they are read)
+  const KernelArgs& a = ctx->args;
+  const Layout& L = ctx->L;
+  const int prec = ctx->cfg.precision;
+  const size_t e4 = prec == PLFBS_FP32_DEVIATION ? 16 : 32, es = e4 / 4;
+  const size_t T = (size_t)L.C + L.B, C = L.C, n3 = 3 * (size_t)ctx->N * sizeof(double);
+  std::vector<std::pair<void*, size_t>> keep = {
+      {a.state, e4 * T}, {a.t0, e4 * C}, {a.t1, e4 * C}, {a.stats, sizeof(DevStats)}};
+  for (void* f : {(void*)a.force_x, (void*)a.force_y, (void*)a.force_z, (void*)a.fforce_x,
+                  (void*)a.fforce_y, (void*)a.fforce_z})
+    if (f) keep.emplace_back(f, es * C);
+  if (ctx->N > 0)
+    for (void* f : {(void*)a.node_x, (void*)a.node_x0, (void*)a.node_vel, (void*)a.node_force})
+      keep.emplace_back(f, n3);
+  size_t total = 0;
+  for (auto& k : keep) total += (k.second + 255) / 256 * 256;
+  void* snap = nullptr;
+  TRY(scratch_alloc(ctx, &snap, total));
+  char* q = static_cast<char*>(snap);
+  cudaError_t e = cudaSuccess;
+  for (auto& k : keep) {
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(q, k.first, k.second, cudaMemcpyDeviceToDevice, ctx->stream);
+    q += (k.second + 255) / 256 * 256;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  // mean device time per launch of `launches` back-to-back launches
+  auto timed = [&](auto&& launch) -> double {
+    if (e != cudaSuccess) return 0.0;
+    cudaEventRecord(e0, ctx->stream);
+    for (int64_t i = 0; i < launches; i++) launch();
+    cudaEventRecord(e1, ctx->stream);
+    e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    float x = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&x, e0, e1);
+    return (double)x / (double)launches;
+  };
+  if (ctx->N > 0) ms[0] = timed([&] { plfbs::launch_ibm(a, prec, ctx->stream); });
+  ms[1] = timed([&] { plfbs::launch_gradient(a, prec, ctx->stream); });
+  ms[2] = timed([&] { plfbs::launch_flux(a, prec, ctx->stream); });
+  for (int rk = 0; rk < 4; rk++)
+    ms[3] += 0.25 * timed([&] { plfbs::launch_update(a, prec, rk, ctx->stream, false); });
+  ms[4] = timed([&] { plfbs::launch_finish(a, prec, ctx->stream); });
+  q = static_cast<char*>(snap);
+  for (auto& k : keep) {  // put back even after a failed launch
+    cudaMemcpyAsync(k.first, q, k.second, cudaMemcpyDeviceToDevice, ctx->stream);
+    q += (k.second + 255) / 256 * 256;
+  }
+  scratch_free(ctx, snap);
+  const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (e == cudaSuccess) e = e2;
+  if (e != cudaSuccess)
+    return set_err(ctx, PLFBS_ERR_CUDA, std::string("profile_kernels: ") + cudaGetErrorString(e));
   TRY(read_stats(ctx));
   return check_fault(ctx);
 }

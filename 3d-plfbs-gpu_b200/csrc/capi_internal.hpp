@@ -33,6 +33,7 @@ struct plfbs_ctx {
   int wall_cap = 0;
   uint64_t fingerprint = 0;  // of the caller's mesh, checked when a checkpoint is loaded
   int32_t* face_order = nullptr;  // device [F]: caller face of each device face
+  int32_t* perm = nullptr;        // device [C + B]: device index of each caller cell / ghost
   plfbs::FluxMaps flux_maps{};    // tensor maps of the TMA-staged flux kernel (FP64)
   int compact_faces = 0;          // unique face records in the compact layout (0: none)
   int compact_cells = 0;          // unique cell weight sets in the compact layout (0: none)
@@ -60,6 +61,10 @@ int set_err(plfbs_ctx* c, int code, const std::string& m);
 // The per-device stream-ordered memory pool (created on first use).
 cudaMemPool_t device_pool(int device);
 int pool_alloc(plfbs_ctx* ctx, void** dst, size_t n);
+// A transient buffer from the same pool, on the context's stream; give it
+// back with scratch_free (stream-ordered) when the work using it is enqueued.
+int scratch_alloc(plfbs_ctx* ctx, void** dst, size_t n);
+void scratch_free(plfbs_ctx* ctx, void* p);
 int dev_alloc(plfbs_ctx* ctx, void** dst, size_t n);
 
 // PLFBS_OK, or PLFBS_ERR_NO_DEVICE for a missing or non-sm_100 device.

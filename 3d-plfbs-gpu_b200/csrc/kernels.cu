@@ -22,6 +22,7 @@
 
 #include <cstdint>
 
+#include "ibm_spread.cuh"
 #include "plfbs_internal.hpp"
 
 namespace plfbs {
@@ -897,13 +898,15 @@ __device__ __forceinline__ void stencil_origin(const KernelArgs& a, const double
 // Eight threads per node, one per cell of its 2 x 2 x 2 stencil: each loads
 // its cell's state, the node's velocity is the sum over the eight (xor
 // butterfly, so every lane holds the same bits), every lane advances the node
-// and forms its force, and each lane spreads to its own cell with FP64
-// atomics. Lane 0 of a node writes the node's arrays.
+// and forms its force, and the warp spreads its lanes' forces with one FP64
+// atomic per distinct cell and component (spread_aggregated; nodes in the
+// spatial order ibm_order). Lane 0 of a node writes the node's arrays.
 __global__ void __launch_bounds__(kIbmBlock) k_ibm(const KernelArgs a) {
   if (halted(a)) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nd = t >> 3, sub = t & 7;
-  const bool active = nd < a.N;
+  const int slot = t >> 3, sub = t & 7;
+  const bool active = slot < a.N;
+  const int nd = active ? __ldg(a.ibm_order + slot) : 0;
   const int xc = a.ibm_xc, yc = a.ibm_yc;
   double x[3] = {0.0, 0.0, 0.0}, r[3] = {0.0, 0.0, 0.0};
   int lo[3] = {0, 0, 0};
@@ -932,6 +935,7 @@ __global__ void __launch_bounds__(kIbmBlock) k_ibm(const KernelArgs a) {
   for (int o = 1; o < 8; o <<= 1)
 #pragma unroll
     for (int c = 0; c < 3; c++) v[c] += __shfl_xor_sync(full, v[c], o);
+  const unsigned act = __ballot_sync(full, active);
   if (!active) return;
   double fn[3];
 #pragma unroll
@@ -951,15 +955,17 @@ __global__ void __launch_bounds__(kIbmBlock) k_ibm(const KernelArgs a) {
   stencil_origin(a, x, r, lo);
   const int ii = lo[0] + di, jj = lo[1] + dj, kk = lo[2] + dk;
   const long long cell = (long long)ii + (long long)jj * xc + (long long)kk * yc * xc;
+  int target = -1;
+  double f[3] = {0.0, 0.0, 0.0};
   if (cell < a.C && cell >= 0) {
     const double wx = 1 - fabs(ii + 0.5 - r[0]);
     const double wy = 1 - fabs(jj + 0.5 - r[1]);
     const double wz = 1 - fabs(kk + 0.5 - r[2]);
-    const int c = a.ibm_map[cell];
-    atomicAdd(a.force_x + c, fn[0] * wx * wy * wz * a.ibm_inv_dx3);
-    atomicAdd(a.force_y + c, fn[1] * wx * wy * wz * a.ibm_inv_dx3);
-    atomicAdd(a.force_z + c, fn[2] * wx * wy * wz * a.ibm_inv_dx3);
+    target = a.ibm_map[cell];
+#pragma unroll
+    for (int c = 0; c < 3; c++) f[c] = fn[c] * wx * wy * wz * a.ibm_inv_dx3;
   }
+  spread_aggregated(act, target, f, a.force_x, a.force_y, a.force_z);
 }
 
 // ---------------------------------------------------------------------------
@@ -1164,8 +1170,8 @@ static void launch_update_rk(const KernelArgs& a, int nb, cudaStream_t s) {
   else
     k_update<RK, 0><<<nb, kBlock, 0, s>>>(a);
 }
-void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t s) {
-  if (precision == PLFBS_FP32_DEVIATION) return launch_update32(a, rk, s);
+void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t s, bool finish) {
+  if (precision == PLFBS_FP32_DEVIATION) return launch_update32(a, rk, s, finish);
   const int nb = blocks_for(a.C, kBlock);
   switch (rk) {
     case 0: launch_update_rk<0>(a, nb, s); break;
@@ -1173,9 +1179,13 @@ void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t s) {
     case 2: launch_update_rk<2>(a, nb, s); break;
     default:
       launch_update_rk<3>(a, nb, s);
-      k_finish<<<1, kFinishBlock, 0, s>>>(a);
+      if (finish) k_finish<<<1, kFinishBlock, 0, s>>>(a);
       break;
   }
+}
+void launch_finish(const KernelArgs& a, int precision, cudaStream_t s) {
+  if (precision == PLFBS_FP32_DEVIATION) return launch_finish32(a, s);
+  k_finish<<<1, kFinishBlock, 0, s>>>(a);
 }
 void launch_seed(const KernelArgs& a, int precision, bool conserved, cudaStream_t s) {
   if (precision == PLFBS_FP32_DEVIATION) return launch_seed32(a, conserved, s);

@@ -19,6 +19,7 @@
 
 #include <cstdint>
 
+#include "ibm_spread.cuh"
 #include "plfbs_internal.hpp"
 
 namespace plfbs {
@@ -543,13 +544,14 @@ __global__ void k_seed32(const KernelArgs a) {
 
 // IBM with FP64 node positions and forces; velocities interpolated from the
 // FP32 state (times U) and forces spread as force / U in FP32.
-// Eight threads per node (as k_ibm). Node quantities stay FP64; the state is
+// Eight threads per node, warp-aggregated spreading (as k_ibm). Node quantities stay FP64; the state is
 // scaled by U when read and the spread force divided by U when written.
 __global__ void __launch_bounds__(kIbmBlock) k_ibm32(const KernelArgs a) {
   if (halted(a)) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nd = t >> 3, sub = t & 7;
-  const bool active = nd < a.N;
+  const int slot = t >> 3, sub = t & 7;
+  const bool active = slot < a.N;
+  const int nd = active ? __ldg(a.ibm_order + slot) : 0;
   const int xc = a.ibm_xc, yc = a.ibm_yc;
   const double U = a.uref;
   double x[3] = {0.0, 0.0, 0.0}, r[3] = {0.0, 0.0, 0.0};
@@ -586,6 +588,7 @@ __global__ void __launch_bounds__(kIbmBlock) k_ibm32(const KernelArgs a) {
   for (int o = 1; o < 8; o <<= 1)
 #pragma unroll
     for (int c = 0; c < 3; c++) v[c] += __shfl_xor_sync(full, v[c], o);
+  const unsigned act = __ballot_sync(full, active);
   if (!active) return;
   double fn[3];
 #pragma unroll
@@ -605,14 +608,16 @@ __global__ void __launch_bounds__(kIbmBlock) k_ibm32(const KernelArgs a) {
   origin(x);
   const int ii = lo[0] + di, jj = lo[1] + dj, kk = lo[2] + dk;
   const long long cell = (long long)ii + (long long)jj * xc + (long long)kk * yc * xc;
+  int target = -1;
+  float f[3] = {0.f, 0.f, 0.f};
   if (cell < a.C && cell >= 0) {
     const double wgt = (1 - fabs(ii + 0.5 - r[0])) * (1 - fabs(jj + 0.5 - r[1])) *
                        (1 - fabs(kk + 0.5 - r[2])) * a.ibm_inv_dx3 / U;
-    const int c = a.ibm_map[cell];
-    atomicAdd(a.fforce_x + c, (float)(fn[0] * wgt));
-    atomicAdd(a.fforce_y + c, (float)(fn[1] * wgt));
-    atomicAdd(a.fforce_z + c, (float)(fn[2] * wgt));
+    target = a.ibm_map[cell];
+#pragma unroll
+    for (int c = 0; c < 3; c++) f[c] = (float)(fn[c] * wgt);
   }
+  spread_aggregated(act, target, f, a.fforce_x, a.fforce_y, a.fforce_z);
 }
 
 inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
@@ -646,7 +651,7 @@ void launch_flux32(const KernelArgs& a, cudaStream_t s) {
     k_flux32<false><<<persistent_blocks(k_flux32<false>, kFluxBlock, a.F, resident), kFluxBlock,
                       0, s>>>(a);
 }
-void launch_update32(const KernelArgs& a, int rk, cudaStream_t s) {
+void launch_update32(const KernelArgs& a, int rk, cudaStream_t s, bool finish) {
   const int nb = blocks_for(a.C, kBlock);
   switch (rk) {
     case 0: launch_update32_rk<0>(a, nb, s); break;
@@ -654,9 +659,12 @@ void launch_update32(const KernelArgs& a, int rk, cudaStream_t s) {
     case 2: launch_update32_rk<2>(a, nb, s); break;
     default:
       launch_update32_rk<3>(a, nb, s);
-      k_finish32<<<1, kFinishBlock, 0, s>>>(a);
+      if (finish) k_finish32<<<1, kFinishBlock, 0, s>>>(a);
       break;
   }
+}
+void launch_finish32(const KernelArgs& a, cudaStream_t s) {
+  k_finish32<<<1, kFinishBlock, 0, s>>>(a);
 }
 void launch_seed32(const KernelArgs& a, bool conserved, cudaStream_t s) {
   if (conserved)

@@ -302,6 +302,7 @@ struct KernelArgs {
   double* node_x; double* node_x0; const double* node_ref; double* node_vel;
   double* node_force;   // [3N] interleaved
   const int32_t* ibm_map;  // caller cell index -> new cell index
+  const int32_t* ibm_order;  // [N] nodes in spatial order (by the cell of node_ref)
   double* partial;      // [nblk_update * 4] per-block squared-residual sums
   DevStats* stats;
   void* res_debug;      // double4 [C] (FP32 form: float4) or null
@@ -330,7 +331,11 @@ void launch_flux(const KernelArgs& a, int precision, cudaStream_t stream);
 // Sets the TMA-staged flux kernel's shared-memory size on the current device
 // (once) and returns its resident block count; call before capturing it.
 int prepare_flux_tma();
-void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t stream);
+// RK stage rk's update; the last stage (rk 3) ends with the residual reduction
+// (k_finish) unless `finish` is false (launch_finish runs it alone).
+void launch_update(const KernelArgs& a, int precision, int rk, cudaStream_t stream,
+                   bool finish = true);
+void launch_finish(const KernelArgs& a, int precision, cudaStream_t stream);
 void launch_seed(const KernelArgs& a, int precision, bool conserved, cudaStream_t stream);
 void launch_wall_forces(const KernelArgs& a, int precision, const int* walls, int n,
                         double visc_gamma, double gamma, double* out, cudaStream_t stream);
@@ -341,7 +346,26 @@ void launch_record_sides(const void* frec0, const void* frec1, int n, int flavou
                          cudaStream_t stream);
 void launch_gradient32(const KernelArgs& a, cudaStream_t stream);
 void launch_flux32(const KernelArgs& a, cudaStream_t stream);
-void launch_update32(const KernelArgs& a, int rk, cudaStream_t stream);
+void launch_update32(const KernelArgs& a, int rk, cudaStream_t stream, bool finish = true);
+void launch_finish32(const KernelArgs& a, cudaStream_t stream);
+
+// State transfer on the device (state_io.cu). perm[o] is the device index of
+// caller index o (cells, then one ghost per boundary face), T = C + B.
+// state_in: the caller's four FP64 field arrays (device copies) into the state
+// records (FP32 form: deviation units, velocity / U and rho - r0); state_out
+// the reverse; records: n records of rec_bytes (16 or 32) gathered into the
+// caller's order (to_caller) or scattered from it.
+void launch_state_in(const int32_t* perm, long long T, const double* rho, const double* u,
+                     const double* v, const double* w, int precision, double U, double r0,
+                     void* state, cudaStream_t stream);
+void launch_state_out(const int32_t* perm, long long T, const void* state, int precision,
+                      double U, double r0, double* rho, double* u, double* v, double* w,
+                      cudaStream_t stream);
+void launch_records(const int32_t* perm, long long n, int rec_bytes, const void* src, void* dst,
+                    bool to_caller, cudaStream_t stream);
+// p[0, n) = value
+void launch_fill(double* p, long long n, double value, cudaStream_t stream);
+void launch_fill(float* p, long long n, float value, cudaStream_t stream);
 void launch_seed32(const KernelArgs& a, bool conserved, cudaStream_t stream);
 
 #ifdef __CUDACC__

@@ -33,7 +33,7 @@ EXPORTS = ("plfbs_create", "plfbs_set_state", "plfbs_run", "plfbs_get_state",
            "plfbs_checkpoint_bytes", "plfbs_save_checkpoint", "plfbs_load_checkpoint",
            "plfbs_wall_forces", "plfbs_get_layout", "plfbs_polymesh_geometry",
            "plfbs_set_flux_kernel", "plfbs_set_layout_compression", "plfbs_cell_order",
-           "plfbs_set_timeout", "plfbs_wait")
+           "plfbs_set_timeout", "plfbs_wait", "plfbs_profile_kernels", "plfbs_fp64_fma_peak")
 
 
 class MeshView(C.Structure):
@@ -108,6 +108,8 @@ def lib():
             getattr(L, name).argtypes = [C.c_void_p, _dp, C.c_int32]
         L.plfbs_ls_weights.argtypes = [C.POINTER(MeshView), C.c_int32, _dp, _dp]
         L.plfbs_profile_steps.argtypes = [C.c_void_p, C.c_int64, _dp]
+        L.plfbs_profile_kernels.argtypes = [C.c_void_p, C.c_int64, _dp]
+        L.plfbs_fp64_fma_peak.argtypes = [C.c_int32, _dp]
         L.plfbs_memory_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
         L.plfbs_last_error.argtypes = [C.c_void_p]
         L.plfbs_destroy.argtypes = [C.c_void_p]
@@ -166,6 +168,15 @@ def mesh_view(ma, keep):
     v.stencil_cells = _i(k(ma.stencil_cells, np.int32))
     v.stencil_faces = _i(k(ma.stencil_faces, np.int32))
     return v
+
+
+def fp64_fma_peak(device=0):
+    """Measured FP64 FMA throughput of a device in GFLOP/s (plfbs_fp64_fma_peak)."""
+    g = C.c_double()
+    rc = lib().plfbs_fp64_fma_peak(int(device), C.byref(g))
+    if rc:
+        raise PlfbsError(rc, lib().plfbs_last_error(None).decode())
+    return g.value
 
 
 def cell_order(ma, renumber):
@@ -316,6 +327,26 @@ class Solver:
         rho, u, v, w = cols
         return np.stack([u, v, w, rho], axis=1)
 
+    def set_fields(self, rho, u, v, w):
+        """The state from four caller arrays of C+B FP64 values, passed to
+        plfbs_set_state as they are (pinned host memory copies at the copy
+        engines' rate)."""
+        cols = (rho, u, v, w)
+        for c in cols:
+            if not (isinstance(c, np.ndarray) and c.dtype == np.float64 and c.size == self.T
+                    and c.flags.c_contiguous):
+                raise ValueError("set_fields needs contiguous float64 arrays of C+B values")
+        self._check(lib().plfbs_set_state(self.h, *[_d(c) for c in cols], self.T))
+
+    def get_fields(self, rho, u, v, w):
+        """plfbs_get_state into four caller arrays of C+B FP64 values."""
+        cols = (rho, u, v, w)
+        for c in cols:
+            if not (isinstance(c, np.ndarray) and c.dtype == np.float64 and c.size == self.T
+                    and c.flags.c_contiguous and c.flags.writeable):
+                raise ValueError("get_fields needs writable contiguous float64 arrays")
+        self._check(lib().plfbs_get_state(self.h, *[_d(c) for c in cols], self.T))
+
     def run(self, max_steps, history=True):
         st = Stats()
         hist = np.zeros((max(int(max_steps), 1), 6)) if history else None
@@ -430,6 +461,13 @@ class Solver:
         ms = np.zeros(4)
         self._check(lib().plfbs_profile_steps(self.h, int(n), _d(ms)))
         return dict(zip(("ibm", "gradient", "flux", "update"), ms.tolist()))
+
+    def profile_kernels(self, launches):
+        """Mean device milliseconds per launch of each kernel kind, launched
+        back to back (plfbs_profile_kernels); the run is left as it was."""
+        ms = np.zeros(5)
+        self._check(lib().plfbs_profile_kernels(self.h, int(launches), _d(ms)))
+        return dict(zip(("ibm", "gradient", "flux", "update", "finish"), ms.tolist()))
 
     def memory_bytes(self):
         b = C.c_int64()

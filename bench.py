@@ -1,36 +1,50 @@
 #!/usr/bin/env python
 """Throughput of the LBFS explicit time step on B200 (one JSON line on rank 0).
 
-Workload: the sphere-in-channel case — a 128 x 64 x 64 uniform hex channel
-(524,288 cells, 1,593,344 faces) with an immersed sphere of diameter 16 cells
-at (32, 32, 32) carried by 3,217 Fibonacci-lattice nodes; inlet u = 0.05
-(Dirichlet velocity, Neumann density), outlet Neumann velocity with rho = 1,
-side walls Neumann in velocity and density (the GPU path has no slip type);
-Re = 100 on the diameter (nu = 0.008), RK dt 0.2, FP64. Synthetic, seeded
-inputs; uniform-flow start.
+Headline workload: the scale case — a 256 x 128 x 128 uniform hex channel
+(4,194,304 cells, 12,664,832 faces) with an immersed sphere of diameter 32
+cells at (64, 64, 64) carried by 12,869 Fibonacci-lattice nodes; inlet
+u = 0.05 (Dirichlet velocity, Neumann density), outlet Neumann velocity with
+rho = 1, side walls Neumann in velocity and density (the GPU path has no slip
+type); Re = 200 on the diameter (nu = 0.008), RK dt 0.2, FP64. Synthetic,
+seeded inputs; uniform-flow start.
 
 A step is one full time step: the IBM update and 4 RK stages over all cells
 and faces. `value` is device throughput in Mcell-updates/s (cells x steps /
-time, summed over ranks, max time over ranks; `per_rk_stage` is the same
-rate per RK stage, 4 x value) with everything resident in
-HBM; the working set (~0.5 GB) exceeds the 126 MB L2, so no flush is needed
-between steps. `e2e` times the whole drop-in call through the C ABI from host
-buffers: create (mesh upload, least-squares weights, layout), set_state,
-run, the per-step residual history read-back, get_state and destroy.
+time, summed over ranks, max time over ranks; `per_rk_stage` is the same rate
+per RK stage, 4 x value) with everything resident in HBM; the working set
+(~4.5 GB) exceeds the 126 MB L2, so no flush is needed between steps.
+`kernels` holds each kernel kind's device time per launch, launched back to
+back (no launch gaps), and their sum over one step against the step's own
+time. `roofline` is the flux kernel against the measured HBM copy bandwidth by
+the algorithmic bytes of the reference's layout, its DRAM bytes from a
+committed ncu capture (`dram_frac`), and its FP64 work against the measured
+FP64 FMA throughput (`fp64`).
+
+`e2e` times the whole drop-in call through the C ABI from pinned host buffers:
+create (mesh upload, least-squares weights, layout), set_state, run, the
+per-step residual history read-back, get_state and destroy. `secondary` holds
+the same device throughput on the sphere channel at 128 x 64 x 64 (3,217
+nodes, Re 100) and on the unstructured stress mesh (64^3 hexes, nodes
+jittered +-20 %, 6 tets each, Taylor-Green field).
 
 --impl reference times the reference's own CPU Solver (oracle/_ref, built
-from the reference sources) on the same mesh and boundary conditions.
-`reference_gpu` (rank 0, one GPU, FP64) is the reference's own CUDA path
-(Solver_gpu.cu built for sm_100a) timed on the same case, outside the timed
+from the reference sources) on the same mesh and boundary conditions, on all
+the host threads it can use. `cpu_baseline` is one instance of it;
+`reference_gpu` (rank 0, one GPU, FP64) the reference's own CUDA path
+(Solver_gpu.cu built for sm_100a) timed on the same case outside the timed
 region: the reference-kernel figure beside `value`.
 """
 
 from __future__ import annotations
 
 import argparse
+import copy
+import dataclasses
 import faulthandler
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -47,11 +61,34 @@ from plfbs import cases  # noqa: E402
 
 METRIC = "Mcell-updates/s"
 E2E_REPS = 3  # end-to-end repetitions (the median is reported)
-WORKLOAD = "sphere_channel_128x64x64_ibm3217_fp64"
-NX, NY, NZ = 128, 64, 64
-DIAM, CENTRE, NNODES = 16.0, (32.0, 32.0, 32.0), 3217
-U, RE, DT, STIFFNESS = 0.05, 100.0, 0.2, 0.5
+U, DT, STIFFNESS = 0.05, 0.2, 0.5
 KERNELS_PER_STEP = 14  # ibm + 4 x (gradient, flux, update) + finish
+
+
+@dataclasses.dataclass(frozen=True)
+class Channel:
+    """A sphere-in-channel case (uniform hexes, IBM sphere of Fibonacci nodes)."""
+    name: str
+    nx: int
+    ny: int
+    nz: int
+    diam: float
+    centre: tuple
+    nodes: int
+    re: float
+
+
+SCALE = Channel("sphere_channel_256x128x128_ibm12869_re200", 256, 128, 128, 32.0,
+                (64.0, 64.0, 64.0), 12869, 200.0)
+SPHERE = Channel("sphere_channel_128x64x64_ibm3217_re100", 128, 64, 64, 16.0,
+                 (32.0, 32.0, 32.0), 3217, 100.0)
+HEADLINE = SCALE
+TETS = dict(name="tgv_tets_64cubed_jitter0.2_re400", n=64, jitter=0.2, seed=11, u0=0.05,
+            re=400.0, dt=0.05, steps=50)
+# the reference CPU Solver has no IBM (Solver.cpp); the key sits in both
+# arms' config so that the lines describe the same case
+REF_CPU_NOTE = "the reference CPU Solver runs the mesh and boundary conditions without IBM"
+
 
 # Algorithmic bytes per launch (FP64, perfect reuse): per face the geometry
 # (normal, area, streaming dt, owner/neighbour offsets: 72 B) and the flux
@@ -66,17 +103,17 @@ def algorithmic_bytes(C, F, B, fp32=False):
             "update": 344 * C}
 
 
-def build_case():
-    pm = cases.uniform_box(NX, NY, NZ, patch_types=["inlet", "outlet", "side", "side", "side",
-                                                    "side"])
-    c = cases.Case(mesh_dir="", X=NX, Y=NY, Z=NZ, dt=DT, mach=U, reynolds=RE, ref_length=DIAM,
-                   tolerance=0.0, obj_radius=DIAM / 2, obj_depth=DIAM, obj_stiffness=STIFFNESS,
-                   obj_centre=CENTRE,
+def build_channel(w: Channel):
+    pm = cases.uniform_box(w.nx, w.ny, w.nz, patch_types=["inlet", "outlet", "side", "side",
+                                                          "side", "side"])
+    c = cases.Case(mesh_dir="", X=w.nx, Y=w.ny, Z=w.nz, dt=DT, mach=U, reynolds=w.re,
+                   ref_length=w.diam, tolerance=0.0, obj_radius=w.diam / 2, obj_depth=w.diam,
+                   obj_stiffness=STIFFNESS, obj_centre=w.centre,
                    bcs=[cases.BC("inlet", 1, 1, 0, 0, "dirichlet", "neumann"),
                         cases.BC("outlet", 1, 0, 0, 0, "neumann", "dirichlet"),
                         cases.BC("side", 1, 0, 0, 0, "neumann", "neumann")])
     ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
-    nodes = cases.fibonacci_sphere(NNODES, DIAM / 2, CENTRE)
+    nodes = cases.fibonacci_sphere(w.nodes, w.diam / 2, w.centre)
     state0 = np.zeros((ma.total_cells, 4))
     state0[:, 0] = U
     state0[:, 3] = 1.0
@@ -90,9 +127,17 @@ def solver_cfg(c, precision=0, renumber=0):
                 renumber=renumber, precision=precision)
 
 
-def ibm_cfg(nodes):
-    return dict(node_ref=nodes, stiffness=STIFFNESS, radius=DIAM / 2, depth=DIAM,
+def ibm_cfg(w: Channel, nodes):
+    return dict(node_ref=nodes, stiffness=STIFFNESS, radius=w.diam / 2, depth=w.diam,
                 object_nodes=len(nodes))
+
+
+def line_config(w: Channel, ma, world, renumber):
+    """The `config` of both arms' lines for workload w."""
+    return {"workload": w.name + "_fp64", "cells": ma.n_cells, "faces": ma.n_faces,
+            "nodes": w.nodes, "re": w.re, "dt": DT,
+            "parallelism": "replicas" if world > 1 else "single", "renumber": renumber,
+            "l2": "working set > L2 (no flush)", "reference_cpu_solver": REF_CPU_NOTE}
 
 
 class ClockSampler:
@@ -123,7 +168,7 @@ class ClockSampler:
                         self.reasons.add(name)
             except Exception:
                 pass
-            time.sleep(0.01)
+            time.sleep(0.005)
 
     def __enter__(self):
         if self.nv:
@@ -151,11 +196,13 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def load_traffic(kernel, workload):
-    """ncu DRAM bytes per launch of `kernel` on `workload`, committed under
-    profiles/traffic.json by the profiling recipe (null when absent)."""
+def load_profile(kind, kernel, workload):
+    """A per-launch figure of `kernel` on `workload` committed under profiles/
+    from an ncu capture: kind "traffic" (profiles/traffic.json, DRAM bytes
+    read + written) or "fp64" (profiles/fp64.json, FP64 thread instructions
+    {"dfma", "dadd", "dmul"}); None when absent."""
     try:
-        with open(os.path.join(REPO, "profiles", "traffic.json")) as f:
+        with open(os.path.join(REPO, "profiles", kind + ".json")) as f:
             t = json.load(f)
         return t.get(workload, {}).get(kernel)
     except Exception:
@@ -163,116 +210,144 @@ def load_traffic(kernel, workload):
 
 
 # ---------------------------------------------------------------------------
-# reference arm: the reference's CPU Solver (serial) on the same case
+# the reference program, timed between its own console lines
 # ---------------------------------------------------------------------------
 
-REF_BIN = os.path.join(REPO, "oracle", "_ref", "plfbs_ref")
-
-
-def _run_ref_cpu(workdir, pm, c, nodes, steps, mesh_dir=None, progress=None, limit=1200):
-    import shutil
-    c.steps = steps
-    c.gpu_solver = 0
-    c.output_dir = os.path.join(workdir, "out") + "/"
-    if os.path.isdir(os.path.join(workdir, "out")):
-        shutil.rmtree(os.path.join(workdir, "out"))
-    node_file = os.path.join(workdir, "nodes.txt")
-    if not os.path.exists(node_file):
-        cases.write_spring_network(node_file, nodes)
-    c.obj_nodes_file = node_file
-    c.obj_num_nodes = len(nodes)
-    c.mesh_dir = mesh_dir or os.path.join(workdir, "polyMesh")
-    xml = os.path.join(workdir, "case.xml")
-    cases.write_xml(xml, c)
-    # the time from the program's "Running Solver" line (printed right before
-    # it calls the solver, program.cpp:106) to its exit: the mesh import and
-    # the rest of the setup before it are left out
-    p = subprocess.Popen([REF_BIN, xml], cwd=workdir, stdout=subprocess.PIPE,
-                         stderr=subprocess.DEVNULL, text=True)
-    timer = threading.Timer(limit, p.kill)  # this process only
-    timer.start()
-    t_solver = None
-    stamps = []  # arrivals of its progress lines ("time t=", Solver.cpp:501-508)
-    try:
-        for line in p.stdout:
-            now = time.perf_counter()
-            if t_solver is None and line.startswith("Running Solver"):
-                t_solver = now
-            elif line.startswith("time t="):
-                stamps.append(now)
-        rc = p.wait()
-    finally:
-        timer.cancel()
-    t_end = time.perf_counter()
-    if rc != 0 or t_solver is None:
-        raise subprocess.CalledProcessError(rc, REF_BIN)
-    if progress is not None:
-        progress.extend(stamps)
-    return t_end - t_solver
-
-
-def reference_cpu_throughput(pm, c, nodes, sample_steps=1):
-    """Mcell-updates/s of the reference CPU Solver: the solver's time in a run
-    of `sample_steps` steps minus that in a 0-step run (its own setup and the
-    final output), each timed from the program's "Running Solver" line."""
-    if not os.path.exists(REF_BIN):
-        return None, "oracle/_ref/plfbs_ref not built"
-    with tempfile.TemporaryDirectory(prefix="plfbs_refcpu_") as wd:
-        cases.write_polymesh(os.path.join(wd, "polyMesh"), pm)
-        t_setup = _run_ref_cpu(wd, pm, c, nodes, 0)
-        t_run = _run_ref_cpu(wd, pm, c, nodes, sample_steps)
-    per_step = max(t_run - t_setup, 1e-9) / sample_steps
-    return pm.n_cells / per_step / 1e6, (
-        "%d time step(s) of the reference CPU Solver on the same %dx%dx%d mesh and boundary "
-        "conditions (the CPU Solver has no IBM), timed from its \"Running Solver\" line with "
-        "the solver's setup subtracted via a 0-step run (%.1f s setup, %.1f s per step), "
-        "serial" % (sample_steps, NX, NY, NZ, t_setup, per_step))
-
-
+REF_CPU_BIN = os.path.join(REPO, "oracle", "_ref", "plfbs_ref_cpu")
 REF_GPU_BIN = os.path.join(REPO, "oracle", "_ref", "plfbs_ref_gpu")
 
 
-def reference_gpu_throughput(pm, c, nodes, steps=2001, every=100, limit=600):
+def clean_intervals(events, output_step, steps):
+    """Step intervals of a reference run free of its text output.
+
+    `events` are (time, kind) in arrival order: kind "line" for a progress
+    line (printed after step t = 1 + k output_step, Solver.cpp:501-508 and
+    Solver_gpu.cu:844-853), "out" for the end marker of a decade output of
+    Solution::output (which follows a progress line), "end" for the CPU
+    Solver's "out of time" (after its last step, t = steps - 1). Between a
+    progress line and the next line or the end, the interval starts at the
+    output's end marker if one came. Returns [(seconds, steps)]."""
+    out = []
+    lines = [i for i, (_, k) in enumerate(events) if k == "line"]
+    for n, i in enumerate(lines):
+        t_line = 1 + n * output_step
+        nxt = next((j for j in range(i + 1, len(events)) if events[j][1] in ("line", "end")), None)
+        if nxt is None:
+            break
+        start = events[i][0]
+        for j in range(i + 1, nxt):
+            if events[j][1] == "out":
+                start = events[j][0]
+        nsteps = output_step if events[nxt][1] == "line" else steps - 1 - t_line
+        if nsteps > 0:
+            out.append((events[nxt][0] - start, nsteps))
+    return out
+
+
+def run_reference_timed(binary, workdir, pm, c, nodes, steps, output_step, mesh_dir=None,
+                        limit=1200):
+    """Runs the reference program on (pm, c) for `steps` steps with a progress
+    line every `output_step` steps; returns (rc, events) with events as
+    clean_intervals reads them. The mesh is written unless `mesh_dir` holds it."""
+    c = copy.copy(c)
+    c.steps, c.output_step = steps, output_step
+    c.gpu_solver = 1 if binary == REF_GPU_BIN else 0
+    c.output_dir = os.path.join(workdir, "out") + "/"
+    if os.path.isdir(c.output_dir):
+        shutil.rmtree(c.output_dir)
+    if mesh_dir is None:
+        mesh_dir = os.path.join(workdir, "polyMesh")
+        cases.write_polymesh(mesh_dir, pm)
+    c.mesh_dir = mesh_dir
+    node_file = os.path.join(workdir, "nodes.txt")
+    if not os.path.exists(node_file):
+        cases.write_spring_network(node_file, nodes)
+    c.obj_nodes_file, c.obj_num_nodes = node_file, len(nodes)
+    xml = os.path.join(workdir, "case.xml")
+    cases.write_xml(xml, c)
+    p = subprocess.Popen([binary, xml], cwd=workdir, stdout=subprocess.PIPE,
+                         stderr=subprocess.DEVNULL, text=True)
+    timer = threading.Timer(limit, p.kill)  # this process only
+    timer.start()
+    events = []
+    try:
+        for line in p.stdout:
+            now = time.perf_counter()
+            if line.startswith("time t="):
+                events.append((now, "line"))
+            elif line.startswith("plfbs-output-done"):
+                events.append((now, "out"))
+            elif line.startswith("out of time"):
+                events.append((now, "end"))
+        rc = p.wait()
+    finally:
+        timer.cancel()
+    return rc, events
+
+
+# The CPU Solver's sample: CPU_STEPS steps with one progress line (after step
+# 1; its decade output follows it), so the clean interval runs from the end
+# of that output to "out of time": CPU_STEPS - 2 steps.
+CPU_STEPS = 3
+
+
+def reference_cpu_instance(workdir, pm, c, nodes, mesh_dir):
+    """Seconds per step of one reference CPU Solver run and its clean
+    interval (start, end) on the perf_counter clock, or (None, reason)."""
+    rc, events = run_reference_timed(REF_CPU_BIN, workdir, pm, c, nodes, CPU_STEPS, 1000000,
+                                     mesh_dir=mesh_dir)
+    iv = clean_intervals(events, 1000000, CPU_STEPS)
+    if rc != 0 or not iv:
+        return None, "the reference CPU Solver exited with %s (%d console events)" % (rc,
+                                                                                      len(events))
+    end = next(t for t, k in events if k == "end")
+    secs, n = iv[-1]
+    return secs / n, (end - secs, end)
+
+
+def write_case_mesh(pm, workdir):
+    mesh_dir = os.path.join(workdir, "polyMesh")
+    cases.write_polymesh(mesh_dir, pm)
+    return mesh_dir
+
+
+def reference_cpu_throughput(pm, c, nodes, w: Channel):
+    """Mcell-updates/s of one instance of the reference CPU Solver (serial)."""
+    if not os.path.exists(REF_CPU_BIN):
+        return None, "oracle/_ref/plfbs_ref_cpu not built"
+    with tempfile.TemporaryDirectory(prefix="plfbs_refcpu_") as wd:
+        mesh_dir = write_case_mesh(pm, wd)
+        per_step, span = reference_cpu_instance(wd, pm, c, nodes, mesh_dir)
+    if per_step is None:
+        return None, span
+    return pm.n_cells / per_step / 1e6, (
+        "one instance of the reference CPU Solver (serial) on the same %dx%dx%d mesh and "
+        "boundary conditions (no IBM: the CPU Solver has none), %d steps of which %d timed "
+        "between its console lines, its text output left out (%.1f s per step)"
+        % (w.nx, w.ny, w.nz, CPU_STEPS, CPU_STEPS - 2, per_step))
+
+
+def reference_gpu_throughput(pm, c, nodes, steps=301, every=50, limit=900, mesh_dir=None):
     """Mcell-updates/s of the reference's own CUDA path (oracle/_ref/plfbs_ref_gpu:
     Solver_gpu.cu and its kernels built for sm_100a) on the same case: it prints
     a progress line every `every` steps (Solver_gpu.cu:844-853), and the median
-    time between their arrivals, over `every`, is its time per step with its
-    setup and the occasional decade output left out."""
-    import copy
+    time between them, with its decade text output left out, over `every`, is
+    its time per step with its setup left out."""
     if not os.path.exists(REF_GPU_BIN):
         return None, "oracle/_ref/plfbs_ref_gpu not built"
-    c = copy.copy(c)
-    stamps, rc = [], None
     with tempfile.TemporaryDirectory(prefix="plfbs_refgpu_") as wd:
-        cases.write_polymesh(os.path.join(wd, "polyMesh"), pm)
-        node_file = os.path.join(wd, "nodes.txt")
-        cases.write_spring_network(node_file, nodes)
-        c.steps, c.gpu_solver, c.output_step = steps, 1, every
-        c.output_dir = os.path.join(wd, "out") + "/"
-        c.obj_nodes_file, c.obj_num_nodes = node_file, len(nodes)
-        c.mesh_dir = os.path.join(wd, "polyMesh")
-        xml = os.path.join(wd, "case.xml")
-        cases.write_xml(xml, c)
-        p = subprocess.Popen([REF_GPU_BIN, xml], cwd=wd, stdout=subprocess.PIPE,
-                             stderr=subprocess.DEVNULL, text=True)
-        timer = threading.Timer(limit, p.kill)  # this process only
-        timer.start()
-        try:
-            for line in p.stdout:
-                if line.startswith("time t="):
-                    stamps.append(time.perf_counter())
-            rc = p.wait()
-        finally:
-            timer.cancel()
-    if rc != 0 or len(stamps) < 3:
+        rc, events = run_reference_timed(REF_GPU_BIN, wd, pm, c, nodes, steps, every,
+                                         mesh_dir=mesh_dir, limit=limit)
+    iv = [s / n for s, n in clean_intervals(events, every, steps)]
+    if rc != 0 or len(iv) < 2:
         return None, "the reference CUDA path exited with %s after %d progress lines" % (
-            rc, len(stamps))
-    gaps = sorted(b - a for a, b in zip(stamps, stamps[1:]))
-    per_step = gaps[len(gaps) // 2] / every
+            rc, sum(1 for _, k in events if k == "line"))
+    per_step = sorted(iv)[len(iv) // 2]
     return pm.n_cells / per_step / 1e6, (
         "the reference's Solver_gpu.cu path built for sm_100a on the same case (IBM included), "
         "%d steps, median of %d intervals of %d steps between its progress lines (setup and "
-        "decade outputs left out), %.3f ms per step" % (steps, len(gaps), every, 1e3 * per_step))
+        "decade text output left out), %.3f ms per step" % (steps, len(iv), every,
+                                                            1e3 * per_step))
 
 
 def _mem_available():
@@ -287,63 +362,65 @@ def _mem_available():
     return None
 
 
-def reference_cpu_aggregate(pm, c, nodes, steps=11, every=2):
+# host memory of one CPU Solver instance per cell (measured: 7.6 GB at 4.19 M
+# cells, 1.14 GB at 0.52 M), with a margin
+REF_CPU_BYTES_PER_CELL = 2400
+
+
+def aggregate(spans, cells):
+    """Whole-host Mcell-updates/s of concurrent instances, each a
+    (seconds per step, (start, end)) sample: the sum of their rates when the
+    timed intervals share a common instant (all instances were stepping at
+    once), else total cell-updates over the span from the first start to the
+    last end (a lower bound). Returns (value, how)."""
+    starts = [s for _, (s, _) in spans]
+    ends = [e for _, (_, e) in spans]
+    if max(starts) < min(ends):
+        return sum(cells / t / 1e6 for t, _ in spans), "sum of the instances' rates"
+    steps = sum((e - s) / t for t, (s, e) in spans)
+    return cells * steps / (max(ends) - min(starts)) / 1e6, (
+        "total cell-updates over the span of the timed intervals (they did not all overlap)")
+
+
+def reference_cpu_aggregate(pm, c, nodes):
     """Mcell-updates/s of the reference CPU Solver on all the host threads it
     can use: the Solver is serial, so P independent instances run at once, P
-    the threads available to this process, bounded so that P times one
-    instance's peak memory stays within half of MemAvailable and P times its
-    files (about 100 MB of text output) within half of the free space of the
-    temporary directory. Each instance
-    runs `steps` steps printing a progress line every `every` steps
-    (Solver.cpp:501-508); the Solver writes its text output after a progress
-    line only while its residual crosses a new decade (the first few lines),
-    so an instance's step time is the shorter of its last two intervals over
-    `every`. The aggregate is the sum of the instances' rates. Returns
-    (value, cores, sample)."""
-    import copy
-    import resource
+    the threads available to this process, bounded so that P instances' memory
+    stays within half of MemAvailable and their text output within half of the
+    free temporary disk space. Each instance is timed as
+    reference_cpu_instance. Returns (value, cores, sample, timed steps)."""
     from concurrent.futures import ThreadPoolExecutor
-    v1, sample1 = reference_cpu_throughput(pm, copy.copy(c), nodes, sample_steps=1)
-    if v1 is None:
-        return None, 0, sample1
+    if not os.path.exists(REF_CPU_BIN):
+        return None, 0, "oracle/_ref/plfbs_ref_cpu not built", 0
     threads = len(os.sched_getaffinity(0))
-    rss = resource.getrusage(resource.RUSAGE_CHILDREN).ru_maxrss * 1024  # one instance's peak
+    per = REF_CPU_BYTES_PER_CELL * pm.n_cells
     avail = _mem_available()
-    P = threads if not avail or rss <= 0 else max(1, min(threads, int(0.5 * avail // rss)))
-    import shutil
-    P = max(1, min(P, int(0.5 * shutil.disk_usage(tempfile.gettempdir()).free // (128 << 20))))
-    if P == 1:
-        return v1, 1, sample1
+    P = threads if not avail else max(1, min(threads, int(0.5 * avail // per)))
+    out_bytes = 120 * (pm.n_cells + pm.n_faces - pm.n_internal)  # one decade output
+    P = max(1, min(P, int(0.5 * shutil.disk_usage(tempfile.gettempdir()).free // out_bytes)))
     with tempfile.TemporaryDirectory(prefix="plfbs_refcpu_") as wd:
-        mesh_dir = os.path.join(wd, "polyMesh")
-        cases.write_polymesh(mesh_dir, pm)
+        mesh_dir = write_case_mesh(pm, wd)
 
         def instance(i):
             d = os.path.join(wd, "i%d" % i)
             os.makedirs(d)
-            ci = copy.copy(c)
-            ci.output_step = every
-            stamps = []
-            _run_ref_cpu(d, pm, ci, nodes, steps, mesh_dir, progress=stamps)
-            gaps = [b - a for a, b in zip(stamps, stamps[1:])]
-            return min(gaps[-2:]) / every if len(gaps) >= 2 else None
+            return reference_cpu_instance(d, pm, c, nodes, mesh_dir)
 
-        try:
-            with ThreadPoolExecutor(max_workers=P) as ex:
-                per_step = list(ex.map(instance, range(P)))
-        except Exception as e:  # the single-instance figure stands
-            return v1, 1, sample1 + "; %d concurrent instances failed (%s)" % (P, e)
-    if any(t is None or t <= 0 for t in per_step):
-        return v1, 1, sample1 + "; %d concurrent instances gave no step time" % P
-    value = sum(pm.n_cells / t / 1e6 for t in per_step)
+        with ThreadPoolExecutor(max_workers=P) as ex:
+            res = list(ex.map(instance, range(P)))
+    bad = [r for r in res if r[0] is None]
+    if bad:
+        return None, 0, bad[0][1], 0
+    value, how = aggregate(res, pm.n_cells)
+    per_step = [t for t, _ in res]
     return value, P, (
         "%d concurrent instances of the serial reference CPU Solver (the host threads "
-        "available, within half of MemAvailable at %.2f GB per instance and half of the free "
-        "temporary disk space), each %d time steps of "
-        "the same %d-cell mesh timed between its progress lines every %d steps past its "
-        "decade outputs (%.3g-%.3g s per step); sum of their rates. One instance alone: "
-        "%.3f Mcell-updates/s" % (P, rss / 1e9, steps, pm.n_cells, every, min(per_step),
-                                  max(per_step), v1))
+        "available, within half of MemAvailable and of the free temporary disk space), each "
+        "%d steps of the same %d-cell mesh and boundary conditions (no IBM: the CPU Solver has "
+        "none) of which the last %d are timed between its console lines with its text output "
+        "left out (%.3g-%.3g s per step); %s"
+        % (P, CPU_STEPS, pm.n_cells, CPU_STEPS - 2, min(per_step), max(per_step), how)), \
+        CPU_STEPS - 2
 
 
 def reduce_max(x, dist=None, device="cuda"):
@@ -371,7 +448,7 @@ TTR_WORKLOAD = "sphere_channel_64x32x32_D8_re100"
 
 def build_ttr_case(nx=64, ny=32, nz=32, D=8.0, re=100.0):
     """The learned-warm-start geometry (64 x 32 x 32 channel, sphere D = 8 at
-    (16, 16, 16), Fibonacci nodes at the node density of the headline case)."""
+    (16, 16, 16), Fibonacci nodes at the node density of the 128 x 64 x 64 case)."""
     pm = cases.uniform_box(nx, ny, nz, patch_types=["inlet", "outlet", "side", "side", "side",
                                                     "side"])
     c = cases.Case(mesh_dir="", X=nx, Y=ny, Z=nz, dt=DT, mach=U, reynolds=re, ref_length=D,
@@ -380,7 +457,8 @@ def build_ttr_case(nx=64, ny=32, nz=32, D=8.0, re=100.0):
                         cases.BC("outlet", 1, 0, 0, 0, "neumann", "dirichlet"),
                         cases.BC("side", 1, 0, 0, 0, "neumann", "neumann")])
     ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
-    n_nodes = int(round(4 * np.pi * (D / 2) ** 2 / (4 * np.pi * (DIAM / 2) ** 2 / NNODES)))
+    n_nodes = int(round(4 * np.pi * (D / 2) ** 2 /
+                        (4 * np.pi * (SPHERE.diam / 2) ** 2 / SPHERE.nodes)))
     nodes = cases.fibonacci_sphere(n_nodes, D / 2, (2 * D, ny / 2, nz / 2))
     state0 = np.zeros((ma.total_cells, 4))
     state0[:, 0] = U
@@ -446,51 +524,47 @@ def time_to_residual(args):
     return 0
 
 
+def build_tets(jitter=None):
+    """The unstructured stress case: 64^3 unit hexes with interior nodes
+    jittered (seeded) and each split into 6 tetrahedra (1,572,864 cells),
+    Taylor-Green initial field (U 0.05), Re 400 on L = 64, Dirichlet u = 0
+    walls, dt 0.05, exact-inverse least squares."""
+    n = TETS["n"]
+    pm = cases.jittered_tet_box(n, jitter=TETS["jitter"] if jitter is None else jitter,
+                                seed=TETS["seed"], patch_types=["wall"] * 6)
+    c = cases.Case(mesh_dir="", X=n, Y=n, Z=n, dt=TETS["dt"], mach=TETS["u0"],
+                   reynolds=TETS["re"], ref_length=n,
+                   bcs=[cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann")])
+    ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
+    x = np.asarray(ma.cell_centroid).reshape(-1, 3) * (2 * np.pi / n)
+    u0 = TETS["u0"]
+    state0 = np.zeros((ma.total_cells, 4))
+    state0[:, 0] = u0 * np.sin(x[:, 0]) * np.cos(x[:, 1]) * np.cos(x[:, 2])
+    state0[:, 1] = -u0 * np.cos(x[:, 0]) * np.sin(x[:, 1]) * np.cos(x[:, 2])
+    state0[:, 3] = 1.0
+    return pm, c, ma, state0
+
+
 def compare_precisions(args):
     """FP32 deviation form against the FP64 path on the other configurations:
-    `tets` = 64^3 unit hexes with interior nodes jittered (seeded), each split
-    into 6 tetrahedra (1,572,864 cells), Taylor-Green initial field (U 0.05),
-    Re 400 on L = 64, Dirichlet u = 0 walls, 500 steps of dt 0.05, exact-inverse
-    least squares (the reference's determinant is unstable on tets). Jitter
-    +-0.1 of the spacing: at +-0.2 the scheme diverges near t = 4.5 whatever
-    Re, U or dt (a mesh-quality instability), at +-0.1 and below it does not;
-    `scale` = 256 x 128 x 128 channel, sphere D 32 at (64, 64, 64) with 12,869
-    nodes, Re 200, 2000 steps. One JSON line: throughput, the flux kernel's
+    `tets` = the unstructured stress case (build_tets; jitter from --jitter,
+    500 steps: at +-0.2 the method itself diverges near t = 4.5, the reference
+    CPU Solver included, at +-0.1 it does not); `scale` = the 256 x 128 x 128
+    headline channel, 2000 steps. One JSON line: throughput, the flux kernel's
     fraction of the measured HBM bandwidth, per-field relative L2 of FP32
     against FP64, and (scale) Cd of both."""
     from plfbs import capi
     if args.compare == "tets":
-        n, u0, re, steps = 64, 0.05, 400.0, 500
-        pm = cases.jittered_tet_box(n, jitter=args.jitter, seed=11, patch_types=["wall"] * 6)
-        c = cases.Case(mesh_dir="", X=n, Y=n, Z=n, dt=args.compare_dt or 0.05, mach=u0,
-                       reynolds=re, ref_length=n,
-                       bcs=[cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann")])
-        ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
-        x = np.asarray(ma.cell_centroid).reshape(-1, 3) * (2 * np.pi / n)
-        state0 = np.zeros((ma.total_cells, 4))
-        state0[:, 0] = u0 * np.sin(x[:, 0]) * np.cos(x[:, 1]) * np.cos(x[:, 2])
-        state0[:, 1] = -u0 * np.cos(x[:, 0]) * np.sin(x[:, 1]) * np.cos(x[:, 2])
-        state0[:, 3] = 1.0
-        ibm, area, mode = None, None, capi.GRAD_EXACT_INVERSE
+        pm, c, ma, state0 = build_tets(args.jitter)
+        if args.compare_dt:
+            c.dt = args.compare_dt
+        ibm, area, mode, steps = None, None, capi.GRAD_EXACT_INVERSE, 500
         name = "tgv_tets_64cubed_jitter%g_re400" % args.jitter
     else:
-        nx, ny, nz, d, re, steps = 256, 128, 128, 32.0, 200.0, 2000
-        pm = cases.uniform_box(nx, ny, nz, patch_types=["inlet", "outlet", "side", "side",
-                                                        "side", "side"])
-        c = cases.Case(mesh_dir="", X=nx, Y=ny, Z=nz, dt=DT, mach=U, reynolds=re,
-                       ref_length=d, tolerance=0.0,
-                       bcs=[cases.BC("inlet", 1, 1, 0, 0, "dirichlet", "neumann"),
-                            cases.BC("outlet", 1, 0, 0, 0, "neumann", "dirichlet"),
-                            cases.BC("side", 1, 0, 0, 0, "neumann", "neumann")])
-        ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
-        nodes = cases.fibonacci_sphere(12869, d / 2, (64.0, 64.0, 64.0))
-        ibm = dict(node_ref=nodes, stiffness=STIFFNESS, radius=d / 2, depth=d,
-                   object_nodes=len(nodes))
-        state0 = np.zeros((ma.total_cells, 4))
-        state0[:, 0] = U
-        state0[:, 3] = 1.0
-        area, mode = np.pi * d * d / 4, 0
-        name = "sphere_channel_256x128x128_ibm12869_re200"
+        w = SCALE
+        pm, c, ma, nodes, state0 = build_channel(w)
+        ibm, area, mode, steps = ibm_cfg(w, nodes), np.pi * w.diam ** 2 / 4, 0, 2000
+        name = w.name
     rt, vt, val = cases.bc_arrays(ma, c)
     peak, peak_kind = load_peaks()
     out, states = {}, {}
@@ -507,13 +581,10 @@ def compare_precisions(args):
             return 1
         r = {"steps": int(st["steps_done"]), "ms_per_step": st["kernel_ms"] / steps,
              "mcell_updates_per_s": ma.n_cells * steps / st["kernel_ms"] / 1e3}
-        prof = s.profile_steps(10)
-        flux_ms = prof["flux"] / 40
+        k = s.profile_kernels(10)
         alg = algorithmic_bytes(ma.n_cells, ma.n_faces, ma.n_bc, fp32=prec_name == "fp32")
-        r["flux_ms"] = flux_ms
-        r["flux_hbm_frac"] = alg["flux"] / (flux_ms / 1e3) / 1e9 / peak
-        s.set_state(state0)
-        s.run(steps, history=False)  # the same state after exactly `steps` steps
+        r["flux_ms"] = k["flux"]
+        r["flux_hbm_frac"] = alg["flux"] / (k["flux"] / 1e3) / 1e9 / peak
         if area:
             r["cd"], r["cl"] = s.body_force(area)
         states[prec_name] = s.get_state()
@@ -536,25 +607,41 @@ def compare_precisions(args):
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
-    pm, c, ma, nodes, _ = build_case()
-    value, cores, sample = reference_cpu_aggregate(pm, c, nodes)
-    cfg = {"workload": WORKLOAD, "cells": ma.n_cells, "faces": ma.n_faces,
-           "nodes": NNODES, "re": RE, "dt": DT,
-           "parallelism": "replicas" if world > 1 else "single"}
+    w = HEADLINE
+    pm = cases.uniform_box(w.nx, w.ny, w.nz, patch_types=["inlet", "outlet", "side", "side",
+                                                          "side", "side"])
+    _, c, _, nodes, _ = build_channel_light(w)
+    value, cores, sample, timed = reference_cpu_aggregate(pm, c, nodes)
     if value is None:
         print(json.dumps({"impl": "reference", "unavailable": sample}))
         return 0
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
-            "n_gpus": world, "steps": 1, "warmup": 0, "requested_steps": args.steps,
-            "ms_per_step": ma.n_cells / value / 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": cfg,
+            "n_gpus": world, "steps": timed, "warmup": CPU_STEPS - timed,
+            "requested_steps": args.steps, "requested_warmup": args.warmup,
+            "steps_note": "each instance times %d step(s) after %d untimed ones: a step of "
+                          "this case takes the serial CPU Solver tens of seconds" % (
+                              timed, CPU_STEPS - timed),
+            "ms_per_step": pm.n_cells * cores / value / 1e3 if cores else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": line_config(w, pm, world, args.renumber),
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+def build_channel_light(w: Channel):
+    """The case description and nodes without the mesh arrays (the reference
+    arm reads the polyMesh itself)."""
+    c = cases.Case(mesh_dir="", X=w.nx, Y=w.ny, Z=w.nz, dt=DT, mach=U, reynolds=w.re,
+                   ref_length=w.diam, tolerance=0.0, obj_radius=w.diam / 2, obj_depth=w.diam,
+                   obj_stiffness=STIFFNESS, obj_centre=w.centre,
+                   bcs=[cases.BC("inlet", 1, 1, 0, 0, "dirichlet", "neumann"),
+                        cases.BC("outlet", 1, 0, 0, 0, "neumann", "dirichlet"),
+                        cases.BC("side", 1, 0, 0, 0, "neumann", "neumann")])
+    return None, c, None, cases.fibonacci_sphere(w.nodes, w.diam / 2, w.centre), None
 
 
 # ---------------------------------------------------------------------------
@@ -565,6 +652,122 @@ def log(msg):
     print("[bench] %s" % msg, file=sys.stderr, flush=True)
 
 
+def pinned_like(a):
+    """A copy of numpy array `a` in page-locked host memory (torch's pinned
+    allocator), contiguous; `a` itself when pinning is unavailable."""
+    import torch
+    a = np.ascontiguousarray(a)
+    try:
+        t = torch.empty(a.size, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+    except Exception:
+        return a
+    out = t.numpy().reshape(a.shape)
+    out[...] = a
+    return out
+
+
+def pinned_mesh(ma):
+    """The mesh arrays in pinned host memory (what a caller streaming meshes
+    to the GPU holds them in)."""
+    kw = {}
+    for f in dataclasses.fields(ma):
+        v = getattr(ma, f.name)
+        if isinstance(v, np.ndarray):
+            dt = np.int32 if v.dtype.kind in "iu" else np.float64
+            kw[f.name] = pinned_like(v.astype(dt, copy=False))
+    return dataclasses.replace(ma, **kw)
+
+
+def kernel_table(kt, ms_per_step, alg, peak):
+    """Per-kernel device time (back-to-back launches) and the HBM fraction of
+    the algorithmic bytes; `sum_over_step` = the kernels of one step over the
+    step's measured time."""
+    kern = {}
+    for k in ("gradient", "flux", "update"):
+        gbs = alg[k] / (kt[k] / 1e3) / 1e9
+        kern[k] = {"ms_per_launch": kt[k], "algorithmic_bytes": alg[k], "achieved_gbs": gbs,
+                   "frac": gbs / peak}
+    kern["ibm"] = {"ms_per_launch": kt["ibm"]}
+    kern["finish"] = {"ms_per_launch": kt["finish"]}
+    per_step = kt["ibm"] + 4 * (kt["gradient"] + kt["flux"] + kt["update"]) + kt["finish"]
+    for k in kern:
+        n = 4 if k in ("gradient", "flux", "update") else 1
+        kern[k]["share"] = n * kt[k] / per_step
+    kern["sum_ms_per_step"] = per_step
+    kern["sum_over_step"] = per_step / ms_per_step
+    return kern
+
+
+def flux_roofline(kt, alg, peak, peak_kind, workload, fp64_gflops, n_faces):
+    """The flux kernel's roofline record: the algorithmic bytes against the
+    measured HBM bandwidth (`frac`), its DRAM bytes per launch from the
+    committed ncu capture against the same peak (`dram_frac`), and its FP64
+    work from the same capture against the measured FP64 FMA throughput."""
+    t = kt["flux"] / 1e3
+    gbs = alg["flux"] / t / 1e9
+    roof = {"kernel": "flux", "bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+            "frac": gbs / peak, "peak_kind": peak_kind,
+            "algorithmic_bytes": alg["flux"], "ms_per_launch": kt["flux"]}
+    traffic = load_profile("traffic", "flux", workload)
+    roof["traffic"] = traffic
+    roof["dram_frac"] = traffic / t / 1e9 / peak if traffic else None
+    ins = load_profile("fp64", "flux", workload)
+    if ins and fp64_gflops:
+        flops = 2 * ins["dfma"] + ins["dadd"] + ins["dmul"]
+        n_ins = ins["dfma"] + ins["dadd"] + ins["dmul"]
+        roof["fp64"] = {"flops_per_launch": flops, "instructions_per_face": n_ins / n_faces,
+                        "achieved_gflops": flops / t / 1e9, "peak_gflops": fp64_gflops,
+                        "peak_kind": "measured (plfbs_fp64_fma_peak)",
+                        "flop_frac": flops / t / 1e9 / fp64_gflops,
+                        # a DADD or DMUL takes an issue slot of the FP64 pipe like a DFMA
+                        "pipe_frac": n_ins / t / (fp64_gflops * 1e9 / 2)}
+    return roof
+
+
+def secondary_channel(w: Channel, steps, warmup, device, peak, peak_kind, fp64_gflops):
+    from plfbs import capi
+    pm, c, ma, nodes, state0 = build_channel(w)
+    rt, vt, val = cases.bc_arrays(ma, c)
+    s = capi.Solver(ma, rt, vt, val, solver_cfg(c), ibm=ibm_cfg(w, nodes), device=device)
+    s.set_state(state0)
+    s.run(warmup, history=False)
+    st, _ = s.run(steps, history=False)
+    ms = st["kernel_ms"] / steps
+    kt = s.profile_kernels(20)
+    s.close()
+    alg = algorithmic_bytes(ma.n_cells, ma.n_faces, ma.n_bc)
+    wl = w.name + "_fp64"
+    return {"workload": wl, "cells": ma.n_cells, "faces": ma.n_faces, "nodes": w.nodes,
+            "steps": steps, "ms_per_step": ms, "value": ma.n_cells / ms / 1e3, "unit": METRIC,
+            "kernels": kernel_table(kt, ms, alg, peak),
+            "roofline": flux_roofline(kt, alg, peak, peak_kind, wl, fp64_gflops, ma.n_faces)}
+
+
+def secondary_tets(warmup, device, peak, peak_kind, fp64_gflops):
+    from plfbs import capi
+    pm, c, ma, state0 = build_tets()
+    rt, vt, val = cases.bc_arrays(ma, c)
+    cfg = solver_cfg(c)
+    cfg["gradient_mode"] = capi.GRAD_EXACT_INVERSE
+    s = capi.Solver(ma, rt, vt, val, cfg, device=device)
+    s.set_state(state0)
+    s.run(warmup, history=False)
+    steps = TETS["steps"]
+    st, _ = s.run(steps, history=False)
+    ms = st["kernel_ms"] / steps
+    kt = s.profile_kernels(20)
+    s.close()
+    alg = algorithmic_bytes(ma.n_cells, ma.n_faces, ma.n_bc)
+    wl = TETS["name"] + "_fp64"
+    return {"workload": wl, "cells": ma.n_cells, "faces": ma.n_faces, "steps": steps,
+            "note": "timed over the first %d steps after %d warm-up ones (t <= %.2f); at +-20 %% "
+                    "jitter the method diverges near t = 4.5, the reference CPU Solver "
+                    "included" % (steps, warmup, (steps + warmup) * TETS["dt"]),
+            "ms_per_step": ms, "value": ma.n_cells / ms / 1e3, "unit": METRIC,
+            "kernels": kernel_table(kt, ms, alg, peak),
+            "roofline": flux_roofline(kt, alg, peak, peak_kind, wl, fp64_gflops, ma.n_faces)}
+
+
 def main():
     faulthandler.enable()
     ap = argparse.ArgumentParser()
@@ -572,13 +775,17 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="scale", choices=["scale", "sphere"],
+                    help="scale: 256x128x128, 12,869 nodes (the headline); sphere: 128x64x64")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--renumber", type=int, default=0, choices=[0, 1, 2],
                     help="cell order: 0 the mesh's (blockMesh), 1 RCM on the host, 2 on the device")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA path on the same case")
-    ap.add_argument("--profile-steps", type=int, default=20)
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the 128x64x64 channel and the jittered-tet lines")
+    ap.add_argument("--profile-launches", type=int, default=20)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
                     help="fp32: the FP32 deviation form (the headline line is fp64)")
     ap.add_argument("--time-to-residual", type=float, default=None,
@@ -612,12 +819,13 @@ def main():
 
     from plfbs import capi
 
-    pm, c, ma, nodes, state0 = build_case()
+    w = SCALE if args.workload == "scale" else SPHERE
+    pm, c, ma, nodes, state0 = build_channel(w)
     rt, vt, val = cases.bc_arrays(ma, c)
-    log("case built: %d cells, %d faces" % (ma.n_cells, ma.n_faces))
+    log("case built: %s, %d cells, %d faces" % (w.name, ma.n_cells, ma.n_faces))
     prec = capi.FP32_DEVIATION if args.precision == "fp32" else capi.FP64
-    solver = capi.Solver(ma, rt, vt, val, solver_cfg(c, prec, args.renumber), ibm=ibm_cfg(nodes),
-                         device=local_rank)
+    solver = capi.Solver(ma, rt, vt, val, solver_cfg(c, prec, args.renumber),
+                         ibm=ibm_cfg(w, nodes), device=local_rank)
 
     def barrier():
         if dist:
@@ -627,7 +835,6 @@ def main():
         return reduce_max(x, dist, "cuda")
 
     log("solver created")
-    # warm-up
     solver.set_state(state0)
     st, _ = solver.run(args.warmup, history=False)
     if st["rc"] != 0:
@@ -640,58 +847,49 @@ def main():
         raise RuntimeError("timed run stopped early: %r" % st)
     ms = max_over_ranks(st["kernel_ms"])
     value = replica_throughput(world, ma.n_cells, args.steps, ms)
-
     log("timed run: %.3f ms for %d steps" % (ms, args.steps))
-    # per-kernel device times (CUDA events between launches on the solver's stream)
-    prof = solver.profile_steps(args.profile_steps)
-    log("profile: %r" % prof)
-    per_launch = {"ibm": prof["ibm"] / args.profile_steps,
-                  "gradient": prof["gradient"] / (4 * args.profile_steps),
-                  "flux": prof["flux"] / (4 * args.profile_steps),
-                  "update": prof["update"] / (4 * args.profile_steps)}
-    total = sum(prof.values())
-    workload = WORKLOAD if args.precision == "fp64" else WORKLOAD.replace("fp64", "fp32dev")
-    if args.renumber:  # another cell order: the committed traffic figures do not apply
+
+    # per-kernel device time, launched back to back (the run is left as it was)
+    kt = solver.profile_kernels(args.profile_launches)
+    log("kernels: %r" % kt)
+    fp64_gflops = capi.fp64_fma_peak(local_rank) if rank == 0 else None
+    workload = w.name + ("_fp64" if args.precision == "fp64" else "_fp32dev")
+    if args.renumber:  # another cell order: the committed ncu figures do not apply
         workload += "_rcm"
     alg = algorithmic_bytes(ma.n_cells, ma.n_faces, ma.n_bc, fp32=args.precision == "fp32")
     peak, peak_kind = load_peaks()
-    kern = {}
-    for k in ("gradient", "flux", "update"):
-        gbs = alg[k] / (per_launch[k] / 1e3) / 1e9
-        kern[k] = {"ms_per_launch": per_launch[k], "share": prof[k] / total,
-                   "algorithmic_bytes": alg[k], "achieved_gbs": gbs, "frac": gbs / peak}
-    kern["ibm"] = {"ms_per_launch": per_launch["ibm"], "share": prof["ibm"] / total}
-    dom = max(("gradient", "flux", "update"), key=lambda k: prof[k])
-    roof = {"kernel": dom, "bound": "hbm", "achieved": kern[dom]["achieved_gbs"], "peak": peak,
-            "unit": "GB/s", "frac": kern[dom]["frac"], "peak_kind": peak_kind,
-            "traffic": load_traffic(dom, workload)}
+    kern = kernel_table(kt, ms / args.steps, alg, peak)
+    roof = flux_roofline(kt, alg, peak, peak_kind, workload, fp64_gflops, ma.n_faces)
 
-    # end to end through the C ABI from host buffers; the median of E2E_REPS
-    # repetitions (host-side timings on a shared machine vary from run to run)
+    # end to end through the C ABI from pinned host buffers; the median of
+    # E2E_REPS repetitions (host-side timings on a shared machine vary)
     e2e = None
+    solver.close()
     if not args.no_e2e:
-        barrier()
-        solver.close()
+        pma = pinned_mesh(ma)
+        fields_in = [pinned_like(state0[:, k]) for k in (3, 0, 1, 2)]
+        fields_out = [pinned_like(np.zeros(ma.total_cells)) for _ in range(4)]
+        nodes_p = pinned_like(nodes)
         reps = []
         for _ in range(E2E_REPS):
             barrier()
             t0 = time.perf_counter()
-            s2 = capi.Solver(ma, rt, vt, val, solver_cfg(c, prec, args.renumber),
-                             ibm=ibm_cfg(nodes),
-                             device=local_rank)
+            s2 = capi.Solver(pma, rt, vt, val, solver_cfg(c, prec, args.renumber),
+                             ibm=ibm_cfg(w, nodes_p), device=local_rank)
             t1 = time.perf_counter()
-            s2.set_state(state0)
+            s2.set_fields(*fields_in)
             t2 = time.perf_counter()
             st2, hist2 = s2.run(args.steps, history=True)
             t3 = time.perf_counter()
-            out = s2.get_state()
+            s2.get_fields(*fields_out)
             t4 = time.perf_counter()
             s2.close()
             t5 = time.perf_counter()
             reps.append((max_over_ranks(t5 - t0),
                          {"create_s": t1 - t0, "set_state_s": t2 - t1, "run_s": t3 - t2,
                           "get_state_s": t4 - t3, "destroy_s": t5 - t4}))
-            assert np.isfinite(out).all() and st2["steps_run"] == args.steps
+            assert all(np.isfinite(f).all() for f in fields_out)
+            assert st2["steps_run"] == args.steps
         reps.sort(key=lambda r: r[0])
         wall, phases = reps[len(reps) // 2]
         T = ma.total_cells
@@ -704,36 +902,53 @@ def main():
                "unit": METRIC,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "wall_s": wall, "includes": "create+set_state+run+history+get_state+destroy",
-               "repetitions": E2E_REPS, "of": "median", "walls_s": [r[0] for r in reps],
-               "phases": phases}
-    else:
-        solver.close()
-
+               "host_buffers": "pinned", "repetitions": E2E_REPS, "of": "median",
+               "walls_s": [r[0] for r in reps], "phases": phases}
     log("e2e: %r" % e2e)
-    cpu = None
+
+    # the reference CPU Solver (one instance, CPU only) runs while the other
+    # GPU measurements below do
+    cpu, cpu_thread = {}, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, sample = reference_cpu_throughput(pm, c, nodes, sample_steps=1)
-        if v is not None:
-            cpu = {"value": v, "unit": METRIC, "cores": 1, "kind": "reference", "sample": sample}
+        def cpu_job():
+            v, sample = reference_cpu_throughput(pm, c, nodes, w)
+            if v is not None:
+                cpu.update(value=v, unit=METRIC, cores=1, kind="reference", sample=sample)
+            else:
+                cpu.update(unavailable=sample)
+        cpu_thread = threading.Thread(target=cpu_job, daemon=True)
+        cpu_thread.start()
+
+    secondary = None
+    if rank == 0 and world == 1 and not args.no_secondary and args.precision == "fp64":
+        secondary = {}
+        if w is not SPHERE:
+            secondary["sphere"] = secondary_channel(SPHERE, 200, 20, local_rank, peak, peak_kind,
+                                                    fp64_gflops)
+            log("secondary sphere: %.1f Mcell/s" % secondary["sphere"]["value"])
+        secondary["tets"] = secondary_tets(5, local_rank, peak, peak_kind, fp64_gflops)
+        log("secondary tets: %.1f Mcell/s" % secondary["tets"]["value"])
+
     ref_gpu = None
     if rank == 0 and world == 1 and not args.no_reference_gpu and args.precision == "fp64":
         v, sample = reference_gpu_throughput(pm, c, nodes)
         ref_gpu = {"value": v, "unit": METRIC, "sample": sample}
         log("reference GPU: %r" % ref_gpu)
+    if cpu_thread is not None:
+        cpu_thread.join()
+        log("reference CPU: %r" % cpu)
 
     if rank == 0:
+        cfg = line_config(w, ma, world, args.renumber)
+        cfg["workload"] = workload
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
-                "config": {"workload": workload, "cells": ma.n_cells, "faces": ma.n_faces,
-                           "nodes": NNODES, "re": RE, "dt": DT,
-                           "parallelism": "replicas" if world > 1 else "single",
-                           "renumber": args.renumber,
-                           "l2": "working set > L2 (no flush)"},
+                "config": cfg,
                 "per_rk_stage": {"value": 4 * value, "unit": "Mcell-stage-updates/s"},
-                "roofline": roof, "kernels": kern, "cpu_baseline": cpu,
-                "reference_gpu": ref_gpu, "e2e": e2e,
+                "roofline": roof, "kernels": kern, "cpu_baseline": cpu if cpu else None,
+                "reference_gpu": ref_gpu, "e2e": e2e, "secondary": secondary,
                 "gpu_launches": KERNELS_PER_STEP * args.steps, "clocks": clk.summary(),
                 "final_max_error": float(hist[-1, 1]) if len(hist) else None}
         print(json.dumps(line))

@@ -323,6 +323,23 @@ int plfbs_ls_weights(const plfbs_mesh_view* mesh, int32_t gradient_mode, double*
  * ms[4] = {ibm, gradient, flux, update}. For profiling; the state advances. */
 int plfbs_profile_steps(plfbs_ctx* ctx, int64_t n_steps, double* ms);
 
+/* Per-kernel device time without launch gaps: each kernel kind launched
+ * `launches` times back to back between two CUDA events, mean milliseconds
+ * per launch in ms[5] = {ibm, gradient, flux, update (mean of the four RK
+ * stages), finish (the residual reduction)}; one step costs about
+ * ibm + 4 (gradient + flux + update) + finish. The kernels' outputs that a
+ * later step reads (state, RK accumulators, body force, nodes, run status)
+ * are copied aside on the device first and put back afterwards, so the run
+ * continues as if nothing had happened. For profiling; no reference
+ * counterpart. */
+int plfbs_profile_kernels(plfbs_ctx* ctx, int64_t launches, double* ms);
+
+/* FP64 fused multiply-add throughput of a device, measured (GFLOP/s, two per
+ * FMA): a one-wave kernel of independent FMA chains, best of five timed
+ * launches. The denominator of a kernel's FP64-pipe fraction; changes no
+ * device setting. No reference counterpart. */
+int plfbs_fp64_fma_peak(int32_t device, double* gflops);
+
 /* Which FP64 flux kernel the step uses: 0 = one thread per face gathering its
  * cells' state and gradients itself (the default); 1 = internal faces staged
  * through shared memory by a producer warp's tile::gather4 bulk tensor copies

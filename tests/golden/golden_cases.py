@@ -101,6 +101,26 @@ def build(name):
     return dict(pm=pm, case=c, nodes=nodes, state0=state0, ma=ma)
 
 
+def build_cavity32(cpu_solver=False, steps=2000):
+    """The plain-method lid-driven cavity at full size: a 32^3 uniform hex
+    unit cube (lattice units, dx = 1), Re 100 on L = 32, lid velocity 0.1
+    (Dirichlet velocity, Neumann density on every wall), dt 0.18, from rest
+    (u = 0, rho = 1), `steps` RK4 steps. Returns dict(pm, case, nodes,
+    state0, ma)."""
+    n = 32
+    pm = cases.uniform_box(n, n, n, patch_types=["wall", "wall", "wall", "lid", "wall", "wall"])
+    c = cases.Case(mesh_dir="", X=n, Y=n, Z=n, steps=steps, dt=0.18, mach=0.1, reynolds=100,
+                   ref_length=n, tolerance=0.0, gpu_solver=0 if cpu_solver else 1,
+                   obj_centre=(16.0, 16.0, 16.0),
+                   bcs=[cases.BC("wall", 1, 0, 0, 0, "dirichlet", "neumann"),
+                        cases.BC("lid", 1, 1, 0, 0, "dirichlet", "neumann")])
+    ma = cases.mesh_arrays(pm, c.visc, c.gamma, c.fneq_min)
+    s0 = np.zeros((ma.total_cells, 4))
+    s0[:, 3] = 1.0
+    nodes = np.zeros((0, 3)) if cpu_solver else np.array([[16.0, 16.0, 16.0]])
+    return dict(pm=pm, case=c, nodes=nodes, state0=s0, ma=ma)
+
+
 def build_tgv_tets(n=12, jitter=0.2, gradient_calc="GG", steps=100, seed=11):
     """The unstructured stress case at small size: n^3 hexes with interior
     nodes jittered uniformly by +-jitter of the spacing (seeded), each split

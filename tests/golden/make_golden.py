@@ -15,6 +15,14 @@ The CPU-Solver cases (golden_cases.CPU_NAMES) run oracle/_ref/plfbs_ref_cpu,
 the same program with <gpu_solver>0</gpu_solver> whose final state
 ref_cpu_dump.cpp writes losslessly; their fixtures cpu_<case>.npz hold the
 initial and final states.
+
+    python tests/golden/make_golden.py long
+
+writes the full-length lid-driven cavity fixtures instead (golden_cases
+build_cavity32: 32^3, Re 100, 2,000 steps from rest; about ten minutes of
+CPU): cavity32.npz from the reference's GPU kernels run serially on the host
+(final state, residual history, steps) and cpu_cavity32.npz from the
+reference CPU Solver (final state).
 """
 
 from __future__ import annotations
@@ -67,5 +75,26 @@ def main():
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+def main_long():
+    tmp = tempfile.mkdtemp(prefix="plfbs_golden_")
+    try:
+        d = golden_cases.build_cavity32()
+        dumps = refrun.run_reference(os.path.join(tmp, "cavity32"), d["pm"], d["case"],
+                                     init_state=d["state0"], timeout=3600)
+        out = {k: dumps[k] for k in ("final_state", "history", "steps_done")}
+        np.savez_compressed(os.path.join(HERE, "cavity32.npz"), **out)
+        d = golden_cases.build_cavity32(cpu_solver=True)
+        dumps = refrun.run_reference(os.path.join(tmp, "cpu_cavity32"), d["pm"], d["case"],
+                                     init_state=d["state0"], binary=CPU_BIN, timeout=3600)
+        np.savez_compressed(os.path.join(HERE, "cpu_cavity32.npz"),
+                            final_state=dumps["cpu_final_state"],
+                            steps=np.array([d["case"].steps], np.int32))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "long":
+        main_long()
+    else:
+        main()

@@ -48,3 +48,27 @@ def test_reference_gpu_timing_from_progress_lines(tmp_path, monkeypatch, rc):
         per_step = pm.n_cells / value / 1e6  # seconds
         assert 0.0014 < per_step < 0.0025, per_step  # 0.15 s per 100 steps; the 0.5 s one dropped
         assert "median of 5 intervals" in sample
+
+
+def test_clean_intervals_leave_out_the_text_output():
+    """A progress line followed by a decade output: the interval to the next
+    line starts at the output's end marker; the CPU Solver's last interval
+    ends at "out of time" after its last step."""
+    ev = [(0.0, "line"), (3.0, "out"), (5.0, "line"), (7.0, "line"), (8.0, "out"), (9.5, "end")]
+    # lines after steps 1, 3, 5 (output_step 2), 7 steps (t = 0 .. 6)
+    iv = bench.clean_intervals(ev, 2, 7)
+    assert iv == [(2.0, 2), (2.0, 2), (1.5, 1)]
+    # a run that never printed its end gives no interval after its last line
+    assert bench.clean_intervals(ev[:3], 2, 7) == [(2.0, 2)]
+
+
+def test_aggregate_of_concurrent_instances():
+    cells = 1_000_000
+    # all three stepping at once (common instant 2.5): the sum of their rates
+    spans = [(10.0, (0.0, 10.0)), (20.0, (2.5, 22.5)), (10.0, (1.0, 11.0))]
+    v, how = bench.aggregate(spans, cells)
+    assert abs(v - (0.1 + 0.05 + 0.1)) < 1e-12 and "sum" in how
+    # staggered: total cell-updates over the whole span, a lower bound
+    spans = [(10.0, (0.0, 10.0)), (10.0, (20.0, 30.0))]
+    v, how = bench.aggregate(spans, cells)
+    assert abs(v - 2 * cells / 30.0 / 1e6) < 1e-12 and "span" in how

@@ -17,7 +17,7 @@ from plfbs import capi, cases, gnn
 def _declared():
     src = "".join(open(os.path.join(REPO, "include", f)).read()
                   for f in sorted(os.listdir(os.path.join(REPO, "include"))) if f.endswith(".h"))
-    return sorted(set(re.findall(r"\b(plfbs_[a-z_]+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(plfbs_[a-z0-9_]+)\s*\(", src)))
 
 
 def test_exports_every_declared_symbol(plfbs_lib):

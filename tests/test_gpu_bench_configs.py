@@ -1,0 +1,130 @@
+"""Parity on the benchmarked configurations at full size, through the C ABI.
+
+  * 32^3 lid-driven cavity, 2,000 steps from rest, against the reference's
+    GPU kernels (fixture cavity32.npz, their host-serial run) and, in the
+    CPU-Solver flavour, against the reference CPU Solver (cpu_cavity32.npz);
+  * the 128 x 64 x 64 sphere channel (3,217 IBM nodes), 20 steps from the
+    bench's uniform start, against the reference's own CUDA path run here
+    (oracle/_ref/plfbs_ref_gpu) and against the C oracle;
+  * the 256 x 128 x 128 channel (12,869 nodes), 2 steps against the C oracle.
+
+Bar: relative L2 <= 1e-10 per field (the reference itself is defined only up
+to the order of its FP64 atomic additions); residual histories to 1e-10.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+import bench
+import golden_cases
+import oracle
+import refrun
+from conftest import REPO, load_golden, rel_err, rel_l2
+from plfbs import capi, cases
+
+pytestmark = pytest.mark.gpu
+
+RUN_TOL = 1e-10
+BIN_GPU = os.path.join(REPO, "oracle", "_ref", "plfbs_ref_gpu")
+
+
+def _cavity_solver(d, **over):
+    cfg = golden_cases.oracle_cfg(d)
+    cfg.update(over)
+    rt, vt, val = cases.bc_arrays(d["ma"], d["case"])
+    ibm = None
+    if d["nodes"].shape[0]:
+        ibm = dict(node_ref=d["nodes"], node_x=d["nodes"], stiffness=cfg["stiffness"],
+                   radius=cfg["radius"], depth=cfg["depth"], object_nodes=cfg["object_nodes"])
+    return capi.Solver(d["ma"], rt, vt, val, cfg, ibm=ibm)
+
+
+@pytest.mark.parametrize("renumber", [0, 1])
+def test_cavity32_2000_steps_matches_reference_kernels(plfbs_lib, renumber):
+    d = golden_cases.build_cavity32()
+    g = load_golden("cavity32")
+    s = _cavity_solver(d, renumber=renumber)
+    s.set_state(d["state0"])
+    st, hist = s.run(d["case"].steps)
+    assert st["rc"] == 0 and st["steps_done"] == int(g["steps_done"][0]) == 2000
+    got = s.get_state()
+    for k in range(4):
+        assert rel_l2(got[:, k], g["final_state"][:, k]) < RUN_TOL, k
+    assert rel_err(hist, g["history"]) < 1e-10
+    # the lid has driven the cavity well away from rest
+    assert np.abs(got[: d["ma"].n_cells, :3]).max() > 0.05
+    s.close()
+
+
+def test_cavity32_2000_steps_cpu_flavour_matches_cpu_solver(plfbs_lib):
+    d = golden_cases.build_cavity32(cpu_solver=True)
+    g = load_golden("cpu_cavity32")
+    s = _cavity_solver(d, renumber=1, flavour=capi.FLAVOUR_CPU_SOLVER)
+    s.set_state(d["state0"])
+    st, _ = s.run(int(g["steps"][0]))
+    assert st["rc"] == 0 and st["steps_done"] == 2000
+    C = d["ma"].n_cells
+    got = s.get_state()[:C]  # the CPU Solver leaves the ghosts of its output alone
+    for k in range(4):
+        assert rel_l2(got[:, k], g["final_state"][:C, k]) < RUN_TOL, k
+    s.close()
+
+
+def _channel(w):
+    pm, c, ma, nodes, state0 = bench.build_channel(w)
+    rt, vt, val = cases.bc_arrays(ma, c)
+    return pm, c, ma, nodes, state0, (rt, vt, val)
+
+
+def _oracle_cfg(w, c, nodes):
+    cfg = bench.solver_cfg(c)
+    cfg.update(node_ref=nodes, node_x=nodes, stiffness=bench.STIFFNESS, radius=w.diam / 2,
+               depth=w.diam, object_nodes=len(nodes))
+    return cfg
+
+
+def _run_ours(w, c, ma, nodes, state0, bcs, steps, renumber):
+    s = capi.Solver(ma, *bcs, bench.solver_cfg(c, renumber=renumber),
+                    ibm=bench.ibm_cfg(w, nodes))
+    s.set_state(state0)
+    st, hist = s.run(steps)
+    assert st["rc"] == 0 and st["steps_done"] == steps
+    out = s.get_state(), hist, s.nodes()[0]
+    s.close()
+    return out
+
+
+def test_sphere_channel_20_steps_against_reference_cuda_and_oracle(plfbs_lib, tmp_path):
+    """The 128 x 64 x 64 channel with its 3,217-node sphere, 20 steps."""
+    w, steps = bench.SPHERE, 20
+    pm, c, ma, nodes, state0, bcs = _channel(w)
+    got, hist, x = _run_ours(w, c, ma, nodes, state0, bcs, steps, renumber=1)
+    o = oracle.OracleRun(ma, *bcs, _oracle_cfg(w, c, nodes), state0)
+    o.run_steps(steps)
+    for k in range(4):
+        assert rel_l2(got[:, k], o.state[:, k]) < RUN_TOL, k
+    assert rel_err(hist, o.history) < 1e-10
+    assert np.abs(got[: ma.n_cells, 1:3]).max() > 1e-4  # the sphere has deflected the flow
+    if not os.path.exists(BIN_GPU):
+        pytest.skip("oracle/_ref/plfbs_ref_gpu not built (needs the reference sources)")
+    c.steps = steps
+    dumps = refrun.run_reference(str(tmp_path), pm, c, nodes=nodes, init_state=state0,
+                                 binary=BIN_GPU, timeout=900)
+    ref = dumps["ref_gpu_final_state"]
+    for k in range(4):
+        assert rel_l2(got[:, k], ref[:, k]) < RUN_TOL, k
+
+
+def test_scale_channel_2_steps_against_oracle(plfbs_lib):
+    """The 256 x 128 x 128 channel (4.19 M cells) with its 12,869-node sphere."""
+    w, steps = bench.SCALE, 2
+    pm, c, ma, nodes, state0, bcs = _channel(w)
+    got, hist, x = _run_ours(w, c, ma, nodes, state0, bcs, steps, renumber=0)
+    o = oracle.OracleRun(ma, *bcs, _oracle_cfg(w, c, nodes), state0)
+    o.run_steps(steps)
+    for k in range(4):
+        assert rel_l2(got[:, k], o.state[:, k]) < RUN_TOL, k
+    assert rel_err(hist, o.history) < 1e-10
+    assert rel_err(x, o.node_x) < 1e-12
