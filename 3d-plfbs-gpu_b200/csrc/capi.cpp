@@ -436,6 +436,15 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   a.nblk_update = (L.C + plfbs::kBlock - 1) / plfbs::kBlock;
   a.dt = cfg->time_marching_step;
   a.pg = 1.0 / cfg->gamma;
+  {
+    const double w[3] = {2.0 / 9.0, 1.0 / 9.0, 1.0 / 72.0};
+    for (int k = 0; k < 3; k++) {
+      a.eq[k][0] = w[k];
+      a.eq[k][1] = 3.0 * w[k];
+      a.eq[k][2] = 4.5 * a.pg * w[k];
+      a.eq[k][3] = 1.5 * a.pg * w[k];
+    }
+  }
   a.visc3 = cfg->visc * 3;
   // body force: +pressure_gradient on the GPU path (Solver_gpu.cu:700), the
   // CPU Solver's force = -pressure_gradient (Solver.cpp:213)

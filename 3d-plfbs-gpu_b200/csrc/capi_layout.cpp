@@ -298,9 +298,13 @@ int build_compact_layout(plfbs_ctx* ctx) {
       ctx->compact_faces = U;
       if (!fp32) {
         TRY(pool_alloc(ctx, &p, 4 * (size_t)U));
-        plfbs::launch_record_sides(t[0], t[1], U, ctx->cfg.flavour, static_cast<int32_t*>(p),
+        void* relax = nullptr;
+        TRY(pool_alloc(ctx, &relax, 16 * (size_t)U));
+        plfbs::launch_record_sides(t[0], t[1], t[2], U, ctx->cfg.flavour,
+                                   static_cast<int32_t*>(p), static_cast<double*>(relax),
                                    ctx->stream);
         a.frec_sides = static_cast<const int32_t*>(p);
+        a.frec_relax = static_cast<const double*>(relax);
       }
     } else {
       TRY(pool_alloc(ctx, &p, 3 * es * (size_t)U * L.K));

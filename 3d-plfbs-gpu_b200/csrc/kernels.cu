@@ -238,6 +238,12 @@ __device__ __forceinline__ void ghost_grad(const d4& q, const double go[12], con
   }
 }
 
+// A cell value at the face, q - t . g (t the offset from the face centroid
+// to the cell centroid), as three fused multiply-adds.
+__device__ __forceinline__ double reconstruct(double q, const double t[3], const double* g) {
+  return fma(-t[2], g[2], fma(-t[1], g[1], fma(-t[0], g[0], q)));
+}
+
 template <int EX, int EY, int EZ>
 __device__ __forceinline__ double edot(const double* g) {
   // e . g for a lattice direction with components in {-1, 0, 1}
@@ -285,8 +291,8 @@ template <int EX, int EY, int EZ, int FL>
 __device__ __forceinline__ void lattice_pair(const double si[4], const double sn[4],
                                              const double sc[4], const double g1[12],
                                              const double g2[12], int side, double dt,
-                                             double c45, double c15, double wgt, double& rhoI,
-                                             double m[3], double P[6], double& D) {
+                                             const double K[4], double& rhoI, double m[3],
+                                             double P[6], double& D) {
   constexpr bool diag = EX != 0 && EY != 0 && EZ != 0;
   // side (pair_side): 1 if s > d1, 2 if s < -d1, 0 in the dead band. Faces are
   // sorted by their branch signature, so these branches are uniform across
@@ -320,15 +326,14 @@ __device__ __forceinline__ void lattice_pair(const double si[4], const double sn
       qb[f] = fma(e, hdt, sc[f]);
     }
   }
-  // w rho (1 + 3 e.u + 4.5 (e.u)^2 / gamma - 1.5 u^2 / gamma), with
-  // c45 = 4.5 / gamma and c15 = 1.5 / gamma folded in
+  // w rho (1 + 3 e.u + 4.5 (e.u)^2 / gamma - 1.5 u^2 / gamma) as
+  // rho (w + 3w e.u + w c45 (e.u)^2 - w c15 u^2), K = (w, 3w, w c45, w c15)
+  // with c45 = 4.5 / gamma and c15 = 1.5 / gamma (kernel constants)
   const double eua = edot<EX, EY, EZ>(qa + 1), eub = -edot<EX, EY, EZ>(qb + 1);
   const double u2a = fma(qa[3], qa[3], fma(qa[2], qa[2], qa[1] * qa[1]));
   const double u2b = fma(qb[3], qb[3], fma(qb[2], qb[2], qb[1] * qb[1]));
-  const double fa =
-      wgt * qa[0] * fma(-c15, u2a, fma(c45 * eua, eua, fma(3.0, eua, 1.0)));
-  const double fb =
-      wgt * qb[0] * fma(-c15, u2b, fma(c45 * eub, eub, fma(3.0, eub, 1.0)));
+  const double fa = qa[0] * fma(-K[3], u2a, fma(K[2] * eua, eua, fma(K[1], eua, K[0])));
+  const double fb = qb[0] * fma(-K[3], u2b, fma(K[2] * eub, eub, fma(K[1], eub, K[0])));
   const double sum = fa + fb, dif = fa - fb;
   // The axis pairs come first and each is the first to write its m and P
   // component; (1, 1, 1) is the first diagonal pair: those writes assign.
@@ -382,8 +387,7 @@ __device__ __forceinline__ void face_flux_out(const KernelArgs& a, const int f, 
                                               const double dt, const double si[4],
                                               const double sn[4], const double sc[4],
                                               double g1[12], double g2[12]) {
-  const double pg = a.pg, c45 = 4.5 * pg, c15 = 1.5 * pg;
-  const double w0 = 2.0 / 9.0, w1 = 1.0 / 9.0, w7 = 1.0 / 72.0;
+  const double pg = a.pg;
   // the seven branch decisions up front: n is not needed again until the end;
   // with the compact layout they come precomputed per record (record_sides)
   unsigned sides;
@@ -398,11 +402,11 @@ __device__ __forceinline__ void face_flux_out(const KernelArgs& a, const int f, 
   }
   // centre node (k = 0): e = 0
   const double u2c = fma(sc[3], sc[3], fma(sc[2], sc[2], sc[1] * sc[1]));
-  double rhoI = w0 * sc[0] * fma(-c15, u2c, 1.0);
+  double rhoI = sc[0] * fma(-a.eq[0][3], u2c, a.eq[0][0]);
   double m[3], P[6], D;  // first written by the pairs below (see lattice_pair)
-  lattice_pair<1, 0, 0, FL>(si, sn, sc, g1, g2, sides & 3, dt, c45, c15, w1, rhoI, m, P, D);
-  lattice_pair<0, 1, 0, FL>(si, sn, sc, g1, g2, sides >> 2 & 3, dt, c45, c15, w1, rhoI, m, P, D);
-  lattice_pair<0, 0, 1, FL>(si, sn, sc, g1, g2, sides >> 4 & 3, dt, c45, c15, w1, rhoI, m, P, D);
+  lattice_pair<1, 0, 0, FL>(si, sn, sc, g1, g2, sides & 3, dt, a.eq[1], rhoI, m, P, D);
+  lattice_pair<0, 1, 0, FL>(si, sn, sc, g1, g2, sides >> 2 & 3, dt, a.eq[1], rhoI, m, P, D);
+  lattice_pair<0, 0, 1, FL>(si, sn, sc, g1, g2, sides >> 4 & 3, dt, a.eq[1], rhoI, m, P, D);
 #pragma unroll
   for (int k = 0; k < 4; k++) {  // (gx, gy, gz) -> (gx + gy, gx - gy, gz), see gdot
     const double s1 = g1[3 * k] + g1[3 * k + 1], r1 = g1[3 * k] - g1[3 * k + 1];
@@ -412,21 +416,31 @@ __device__ __forceinline__ void face_flux_out(const KernelArgs& a, const int f, 
     g2[3 * k] = s2;
     g2[3 * k + 1] = r2;
   }
-  lattice_pair<1, 1, 1, FL>(si, sn, sc, g1, g2, sides >> 6 & 3, dt, c45, c15, w7, rhoI, m, P, D);
-  lattice_pair<1, 1, -1, FL>(si, sn, sc, g1, g2, sides >> 8 & 3, dt, c45, c15, w7, rhoI, m, P, D);
-  lattice_pair<1, -1, 1, FL>(si, sn, sc, g1, g2, sides >> 10 & 3, dt, c45, c15, w7, rhoI, m, P, D);
-  lattice_pair<-1, 1, 1, FL>(si, sn, sc, g1, g2, sides >> 12 & 3, dt, c45, c15, w7, rhoI, m, P, D);
+  lattice_pair<1, 1, 1, FL>(si, sn, sc, g1, g2, sides >> 6 & 3, dt, a.eq[2], rhoI, m, P, D);
+  lattice_pair<1, 1, -1, FL>(si, sn, sc, g1, g2, sides >> 8 & 3, dt, a.eq[2], rhoI, m, P, D);
+  lattice_pair<1, -1, 1, FL>(si, sn, sc, g1, g2, sides >> 10 & 3, dt, a.eq[2], rhoI, m, P, D);
+  lattice_pair<-1, 1, 1, FL>(si, sn, sc, g1, g2, sides >> 12 & 3, dt, a.eq[2], rhoI, m, P, D);
   rhoI += D;
   P[0] += D;
   P[1] += D;
   P[2] += D;
 
-  // n, A and the relaxation factor 3 nu / (dt_s gamma) are read again here
-  // (an L1 hit) rather than held in registers through the pairs.
+  // n and A, and the relaxation factor tau = 3 nu / (dt_s gamma) as the
+  // pair ((1 - tau) A, tau A), are read again here (L1 hits; per record with
+  // the compact layout) rather than held in registers through the pairs.
   const d4 g0 = ld4(launder(CR ? a.frec0 : a.face0), r);
   const double nf[3] = {g0.x, g0.y, g0.z};
   const double area = g0.w;
-  const double tau = __ldg(static_cast<const double*>(launder(CR ? a.frec2 : a.face2)) + 4LL * r + 3);
+  double omA, tA;
+  if (CR) {
+    const double2 w = __ldg(reinterpret_cast<const double2*>(a.frec_relax) + r);
+    omA = w.x;
+    tA = w.y;
+  } else {
+    const double tau = __ldg(static_cast<const double*>(launder(a.face2)) + 4LL * r + 3);
+    omA = (1.0 - tau) * area;
+    tA = tau * area;
+  }
   const double mn = m[0] * nf[0] + m[1] * nf[1] + m[2] * nf[2];
   const double Pn[3] = {P[0] * nf[0] + P[3] * nf[1] + P[4] * nf[2],
                         P[3] * nf[0] + P[1] * nf[1] + P[5] * nf[2],
@@ -434,9 +448,9 @@ __device__ __forceinline__ void face_flux_out(const KernelArgs& a, const int f, 
   const double p3 = rhoI * (1.0 / 3.0);
   const double mnr = mn / rhoI * pg;
   d4 out;
-  out.x = ((1.0 - tau) * fma(m[0], mnr, p3 * nf[0]) + tau * Pn[0]) * area;
-  out.y = ((1.0 - tau) * fma(m[1], mnr, p3 * nf[1]) + tau * Pn[1]) * area;
-  out.z = ((1.0 - tau) * fma(m[2], mnr, p3 * nf[2]) + tau * Pn[2]) * area;
+  out.x = fma(omA, fma(m[0], mnr, p3 * nf[0]), tA * Pn[0]);
+  out.y = fma(omA, fma(m[1], mnr, p3 * nf[1]), tA * Pn[1]);
+  out.z = fma(omA, fma(m[2], mnr, p3 * nf[2]), tA * Pn[2]);
   out.w = mn * area;
   st4(a.flux, f, out);
 }
@@ -486,8 +500,7 @@ __device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, cons
         // velocity 1 the value, velocity 8 (u, 0, w) of the owner, otherwise
         // extrapolated with the ghost gradient
         const bool dirichlet = (k == 0) ? (rt == 1) : (FL == 1 ? vt == 1 : vt != 2);
-        const double ext =
-            qov[k] - (t1[0] * g2[3 * k] + t1[1] * g2[3 * k + 1] + t1[2] * g2[3 * k + 2]);
+        const double ext = reconstruct(qov[k], t1, g2 + 3 * k);
         sc[k] = dirichlet ? bvv[k] : (FL == 1 && k > 0 && vt == 8) ? (k == 2 ? 0.0 : qov[k]) : ext;
         si[k] = sc[k];
         sn[k] = sc[k];
@@ -504,8 +517,8 @@ __device__ __forceinline__ void flux_face(const KernelArgs& a, const int f, cons
     const double qnv[4] = {qn.w, qn.x, qn.y, qn.z};
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      si[k] = qov[k] - (t1[0] * g1[3 * k] + t1[1] * g1[3 * k + 1] + t1[2] * g1[3 * k + 2]);
-      sn[k] = qnv[k] - (t2[0] * g2[3 * k] + t2[1] * g2[3 * k + 1] + t2[2] * g2[3 * k + 2]);
+      si[k] = reconstruct(qov[k], t1, g1 + 3 * k);
+      sn[k] = reconstruct(qnv[k], t2, g2 + 3 * k);
       sc[k] = (si[k] + sn[k]) * 0.5;
     }
   }
@@ -685,8 +698,8 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     double si[4], sn[4], sc[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-      si[q] = qov[q] - (t1[0] * g1[3 * q] + t1[1] * g1[3 * q + 1] + t1[2] * g1[3 * q + 2]);
-      sn[q] = qnv[q] - (t2[0] * g2[3 * q] + t2[1] * g2[3 * q + 1] + t2[2] * g2[3 * q + 2]);
+      si[q] = reconstruct(qov[q], t1, g1 + 3 * q);
+      sn[q] = reconstruct(qnv[q], t2, g2 + 3 * q);
       sc[q] = (si[q] + sn[q]) * 0.5;
     }
     face_flux_out<0, false>(a, f, f, n, dt, si, sn, sc, g1, g2);
@@ -1062,9 +1075,12 @@ inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 // The seven branch decisions of each unique face record of the compact
 // layout, as face_flux_out computes them.
 template <int FL>
-__global__ void k_record_sides(const void* frec0, const void* frec1, int n, int32_t* out) {
+__global__ void k_record_sides(const void* frec0, const void* frec1, const void* frec2, int n,
+                               int32_t* out, double2* relax) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    const d4 f0 = ld4(frec0, r), f1 = ld4(frec1, r);
+    const d4 f0 = ld4(frec0, r), f1 = ld4(frec1, r), f2 = ld4(frec2, r);
+    // the pair face_flux_out forms per face without the compact layout
+    relax[r] = make_double2((1.0 - f2.w) * f0.w, f2.w * f0.w);
     const double nv[3] = {f0.x, f0.y, f0.z};
     const double d1 = 0.001 * f1.x;
     out[r] = (int32_t)(pair_side<1, 0, 0, FL>(nv, d1) | pair_side<0, 1, 0, FL>(nv, d1) << 2 |
@@ -1077,14 +1093,15 @@ __global__ void k_record_sides(const void* frec0, const void* frec1, int n, int3
 
 }  // namespace
 
-void launch_record_sides(const void* frec0, const void* frec1, int n, int flavour, int32_t* out,
-                         cudaStream_t s) {
+void launch_record_sides(const void* frec0, const void* frec1, const void* frec2, int n,
+                         int flavour, int32_t* out, double* relax, cudaStream_t s) {
   if (n <= 0) return;
   const int nb = (int)blocks_for(n, kBlock);
+  double2* rl = reinterpret_cast<double2*>(relax);
   if (flavour == PLFBS_FLAVOUR_CPU_SOLVER)
-    k_record_sides<1><<<nb, kBlock, 0, s>>>(frec0, frec1, n, out);
+    k_record_sides<1><<<nb, kBlock, 0, s>>>(frec0, frec1, frec2, n, out, rl);
   else
-    k_record_sides<0><<<nb, kBlock, 0, s>>>(frec0, frec1, n, out);
+    k_record_sides<0><<<nb, kBlock, 0, s>>>(frec0, frec1, frec2, n, out, rl);
 }
 
 void launch_gradient(const KernelArgs& a, int precision, cudaStream_t s) {

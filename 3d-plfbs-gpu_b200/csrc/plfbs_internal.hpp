@@ -278,6 +278,9 @@ struct KernelArgs {
   // scalars
   double dt;            // RK time step
   double pg;            // 1 / gamma
+  // equilibrium constants of the flux kernel per weight class (centre 2/9,
+  // axis 1/9, diagonal 1/72): (w, 3 w, 4.5 w / gamma, 1.5 w / gamma)
+  double eq[3][4];
   double visc3;         // 3 nu (relaxation factor is 3 nu / (dt_s gamma))
   double pressure_gradient;
   double tolerance;
@@ -320,6 +323,7 @@ struct KernelArgs {
   const int32_t* cell_wset;                       // [C] index into wtab
   const void* wtab;                               // [unique sets][K][3] double (FP32: float)
   const int32_t* frec_sides;                      // [unique records] branch bits (FP64)
+  const double* frec_relax;                       // [2 x unique records] (1 - tau) A, tau A (FP64)
   int compact;                                    // 1: the kernels read the tables
 };
 
@@ -341,9 +345,10 @@ void launch_wall_forces(const KernelArgs& a, int precision, const int* walls, in
                         double visc_gamma, double gamma, double* out, cudaStream_t stream);
 void launch_ibm32(const KernelArgs& a, cudaStream_t stream);
 // Branch bits (the flux kernel's seven lattice-pair sides) of n unique FP64
-// face records of the compact layout.
-void launch_record_sides(const void* frec0, const void* frec1, int n, int flavour, int32_t* out,
-                         cudaStream_t stream);
+// face records of the compact layout, and their relaxation pairs
+// relax[2r] = (1 - tau) A, relax[2r + 1] = tau A.
+void launch_record_sides(const void* frec0, const void* frec1, const void* frec2, int n,
+                         int flavour, int32_t* out, double* relax, cudaStream_t stream);
 void launch_gradient32(const KernelArgs& a, cudaStream_t stream);
 void launch_flux32(const KernelArgs& a, cudaStream_t stream);
 void launch_update32(const KernelArgs& a, int rk, cudaStream_t stream, bool finish = true);

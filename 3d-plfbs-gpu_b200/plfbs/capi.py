@@ -404,7 +404,8 @@ class Solver:
                                            _d(nx) if nx is not None else None, self.N))
 
     def set_flux_kernel(self, kind):
-        """0: per-thread gathers (default); 1: TMA-staged internal faces (FP64)."""
+        """0: one thread per face (default); 1: TMA-staged internal faces (FP64;
+        both give the same bits)."""
         self._check(lib().plfbs_set_flux_kernel(self.h, int(kind)))
 
     def set_layout_compression(self, on):

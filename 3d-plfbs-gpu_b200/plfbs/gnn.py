@@ -189,3 +189,46 @@ class GraphNet:
             self.close()
         except Exception:
             pass
+
+
+def main(argv=None):
+    """Times training steps of the network (forward, backward, Adam) on the
+    face graph of the warm start's 64 x 32 x 32 channel (65,536 nodes, 8
+    message-passing layers, 6 node / 4 edge features, 4 outputs) with seeded
+    synthetic features and targets; prints one JSON line. The command behind
+    the committed ncu summary of the network's kernels:
+
+        python -m plfbs.gnn --steps 5 [--tensor-cores 0|1]
+    """
+    import argparse
+    import json
+    import time
+
+    from . import cases
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--tensor-cores", type=int, default=1)
+    args = ap.parse_args(argv)
+    ma = cases.mesh_arrays(cases.uniform_box(64, 32, 32), 0.008, 1.0, 0.0)
+    src, dst, ef = mesh_graph(ma)
+    x = node_features(ma, (64, 32, 32), (16.0, 16.0, 16.0), 8.0, 100.0)
+    rng = np.random.Generator(np.random.PCG64(0))
+    t = rng.standard_normal((ma.n_cells, 4)).astype(np.float32)
+    net = GraphNet(src, dst, ef, ma.n_cells, x.shape[1], 8, 4)
+    net.set_params(init_params(x.shape[1], ef.shape[1], 8, 4, seed=1))
+    net.set_tensor_cores(args.tensor_cores)
+    net.train_step(x, t, 1e-4)  # warm-up
+    t0 = time.perf_counter()
+    losses = [net.train_step(x, t, 1e-4) for _ in range(args.steps)]
+    dt = (time.perf_counter() - t0) / max(args.steps, 1)
+    t1 = time.perf_counter()
+    net.forward(x)
+    fwd = time.perf_counter() - t1
+    net.close()
+    print(json.dumps({"graph_nodes": int(ma.n_cells), "graph_edges": int(len(src)), "layers": 8,
+                      "train_step_s": dt, "forward_s": fwd, "loss_first": losses[0],
+                      "loss_last": losses[-1], "tensor_cores": args.tensor_cores}))
+
+
+if __name__ == "__main__":
+    main()

@@ -417,7 +417,7 @@ def reference_cpu_aggregate(pm, c, nodes):
         "%d concurrent instances of the serial reference CPU Solver (the host threads "
         "available, within half of MemAvailable and of the free temporary disk space), each "
         "%d steps of the same %d-cell mesh and boundary conditions (no IBM: the CPU Solver has "
-        "none) of which the last %d are timed between its console lines with its text output "
+        "none), the last %d of them timed between its console lines with its text output "
         "left out (%.3g-%.3g s per step); %s"
         % (P, CPU_STEPS, pm.n_cells, CPU_STEPS - 2, min(per_step), max(per_step), how)), \
         CPU_STEPS - 2
@@ -678,15 +678,20 @@ def pinned_mesh(ma):
     return dataclasses.replace(ma, **kw)
 
 
-def kernel_table(kt, ms_per_step, alg, peak):
-    """Per-kernel device time (back-to-back launches) and the HBM fraction of
-    the algorithmic bytes; `sum_over_step` = the kernels of one step over the
+def kernel_table(kt, ms_per_step, alg, peak, workload):
+    """Per-kernel device time (back-to-back launches), the HBM fraction of the
+    algorithmic bytes (`frac`) and of the DRAM bytes of the committed ncu
+    capture (`dram_frac`); `sum_over_step` = the kernels of one step over the
     step's measured time."""
     kern = {}
     for k in ("gradient", "flux", "update"):
         gbs = alg[k] / (kt[k] / 1e3) / 1e9
         kern[k] = {"ms_per_launch": kt[k], "algorithmic_bytes": alg[k], "achieved_gbs": gbs,
                    "frac": gbs / peak}
+        dram = load_profile("traffic", k, workload)
+        if dram:
+            kern[k]["dram_bytes"] = dram
+            kern[k]["dram_frac"] = dram / (kt[k] / 1e3) / 1e9 / peak
     kern["ibm"] = {"ms_per_launch": kt["ibm"]}
     kern["finish"] = {"ms_per_launch": kt["finish"]}
     per_step = kt["ibm"] + 4 * (kt["gradient"] + kt["flux"] + kt["update"]) + kt["finish"]
@@ -739,7 +744,7 @@ def secondary_channel(w: Channel, steps, warmup, device, peak, peak_kind, fp64_g
     wl = w.name + "_fp64"
     return {"workload": wl, "cells": ma.n_cells, "faces": ma.n_faces, "nodes": w.nodes,
             "steps": steps, "ms_per_step": ms, "value": ma.n_cells / ms / 1e3, "unit": METRIC,
-            "kernels": kernel_table(kt, ms, alg, peak),
+            "kernels": kernel_table(kt, ms, alg, peak, wl),
             "roofline": flux_roofline(kt, alg, peak, peak_kind, wl, fp64_gflops, ma.n_faces)}
 
 
@@ -764,7 +769,7 @@ def secondary_tets(warmup, device, peak, peak_kind, fp64_gflops):
                     "jitter the method diverges near t = 4.5, the reference CPU Solver "
                     "included" % (steps, warmup, (steps + warmup) * TETS["dt"]),
             "ms_per_step": ms, "value": ma.n_cells / ms / 1e3, "unit": METRIC,
-            "kernels": kernel_table(kt, ms, alg, peak),
+            "kernels": kernel_table(kt, ms, alg, peak, wl),
             "roofline": flux_roofline(kt, alg, peak, peak_kind, wl, fp64_gflops, ma.n_faces)}
 
 
@@ -775,8 +780,10 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="scale", choices=["scale", "sphere"],
-                    help="scale: 256x128x128, 12,869 nodes (the headline); sphere: 128x64x64")
+    ap.add_argument("--workload", default="scale", choices=["scale", "sphere", "tets"],
+                    help="scale: 256x128x128, 12,869 nodes (the headline); sphere: 128x64x64; "
+                         "tets: 64^3 hexes jittered +-20%% as 6 tets each (keep steps + warmup "
+                         "under about 80: the method diverges on that mesh near step 90)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--renumber", type=int, default=0, choices=[0, 1, 2],
                     help="cell order: 0 the mesh's (blockMesh), 1 RCM on the host, 2 on the device")
@@ -819,13 +826,26 @@ def main():
 
     from plfbs import capi
 
-    w = SCALE if args.workload == "scale" else SPHERE
-    pm, c, ma, nodes, state0 = build_channel(w)
-    rt, vt, val = cases.bc_arrays(ma, c)
-    log("case built: %s, %d cells, %d faces" % (w.name, ma.n_cells, ma.n_faces))
     prec = capi.FP32_DEVIATION if args.precision == "fp32" else capi.FP64
-    solver = capi.Solver(ma, rt, vt, val, solver_cfg(c, prec, args.renumber),
-                         ibm=ibm_cfg(w, nodes), device=local_rank)
+    if args.workload == "tets":  # the unstructured stress mesh (no IBM, exact-inverse LS)
+        w = None
+        pm, c, ma, state0 = build_tets()
+        nodes = np.zeros((0, 3))
+        name = TETS["name"]
+        scfg = solver_cfg(c, prec, args.renumber)
+        scfg["gradient_mode"] = capi.GRAD_EXACT_INVERSE
+    else:
+        w = SCALE if args.workload == "scale" else SPHERE
+        pm, c, ma, nodes, state0 = build_channel(w)
+        name = w.name
+        scfg = solver_cfg(c, prec, args.renumber)
+
+    def ibm_of(n):
+        return ibm_cfg(w, n) if w is not None else None
+
+    rt, vt, val = cases.bc_arrays(ma, c)
+    log("case built: %s, %d cells, %d faces" % (name, ma.n_cells, ma.n_faces))
+    solver = capi.Solver(ma, rt, vt, val, scfg, ibm=ibm_of(nodes), device=local_rank)
 
     def barrier():
         if dist:
@@ -853,12 +873,12 @@ def main():
     kt = solver.profile_kernels(args.profile_launches)
     log("kernels: %r" % kt)
     fp64_gflops = capi.fp64_fma_peak(local_rank) if rank == 0 else None
-    workload = w.name + ("_fp64" if args.precision == "fp64" else "_fp32dev")
+    workload = name + ("_fp64" if args.precision == "fp64" else "_fp32dev")
     if args.renumber:  # another cell order: the committed ncu figures do not apply
         workload += "_rcm"
     alg = algorithmic_bytes(ma.n_cells, ma.n_faces, ma.n_bc, fp32=args.precision == "fp32")
     peak, peak_kind = load_peaks()
-    kern = kernel_table(kt, ms / args.steps, alg, peak)
+    kern = kernel_table(kt, ms / args.steps, alg, peak, workload)
     roof = flux_roofline(kt, alg, peak, peak_kind, workload, fp64_gflops, ma.n_faces)
 
     # end to end through the C ABI from pinned host buffers; the median of
@@ -874,8 +894,7 @@ def main():
         for _ in range(E2E_REPS):
             barrier()
             t0 = time.perf_counter()
-            s2 = capi.Solver(pma, rt, vt, val, solver_cfg(c, prec, args.renumber),
-                             ibm=ibm_cfg(w, nodes_p), device=local_rank)
+            s2 = capi.Solver(pma, rt, vt, val, scfg, ibm=ibm_of(nodes_p), device=local_rank)
             t1 = time.perf_counter()
             s2.set_fields(*fields_in)
             t2 = time.perf_counter()
@@ -909,7 +928,7 @@ def main():
     # the reference CPU Solver (one instance, CPU only) runs while the other
     # GPU measurements below do
     cpu, cpu_thread = {}, None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and w is not None:
         def cpu_job():
             v, sample = reference_cpu_throughput(pm, c, nodes, w)
             if v is not None:
@@ -920,7 +939,8 @@ def main():
         cpu_thread.start()
 
     secondary = None
-    if rank == 0 and world == 1 and not args.no_secondary and args.precision == "fp64":
+    if (rank == 0 and world == 1 and not args.no_secondary and args.precision == "fp64" and
+            w is not None):
         secondary = {}
         if w is not SPHERE:
             secondary["sphere"] = secondary_channel(SPHERE, 200, 20, local_rank, peak, peak_kind,
@@ -930,7 +950,8 @@ def main():
         log("secondary tets: %.1f Mcell/s" % secondary["tets"]["value"])
 
     ref_gpu = None
-    if rank == 0 and world == 1 and not args.no_reference_gpu and args.precision == "fp64":
+    if (rank == 0 and world == 1 and not args.no_reference_gpu and args.precision == "fp64" and
+            w is not None):  # the reference's GPU path takes hexahedra only
         v, sample = reference_gpu_throughput(pm, c, nodes)
         ref_gpu = {"value": v, "unit": METRIC, "sample": sample}
         log("reference GPU: %r" % ref_gpu)
@@ -939,7 +960,13 @@ def main():
         log("reference CPU: %r" % cpu)
 
     if rank == 0:
-        cfg = line_config(w, ma, world, args.renumber)
+        if w is not None:
+            cfg = line_config(w, ma, world, args.renumber)
+        else:
+            cfg = {"cells": ma.n_cells, "faces": ma.n_faces, "jitter": TETS["jitter"],
+                   "re": TETS["re"], "dt": TETS["dt"], "l2": "working set > L2 (no flush)",
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "renumber": args.renumber}
         cfg["workload"] = workload
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -949,6 +976,7 @@ def main():
                 "per_rk_stage": {"value": 4 * value, "unit": "Mcell-stage-updates/s"},
                 "roofline": roof, "kernels": kern, "cpu_baseline": cpu if cpu else None,
                 "reference_gpu": ref_gpu, "e2e": e2e, "secondary": secondary,
+                "fp64_fma_peak_gflops": fp64_gflops,
                 "gpu_launches": KERNELS_PER_STEP * args.steps, "clocks": clk.summary(),
                 "final_max_error": float(hist[-1, 1]) if len(hist) else None}
         print(json.dumps(line))
