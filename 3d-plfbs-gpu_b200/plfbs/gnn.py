@@ -101,16 +101,21 @@ def mesh_graph(ma):
     return src, dst, feat.astype(np.float32)
 
 
-def node_features(ma, lengths, centre, diameter, re):
-    """[n_cells][6]: x, y, z / box lengths, signed distance to the sphere in
-    diameters, 1 / (1 + that^2), Re / 200."""
+def node_features(ma, lengths, centre, diameter, re, relative=True):
+    """[n_cells][9]: x, y, z / box lengths, signed distance to the sphere in
+    diameters, 1 / (1 + that^2), Re / 200 and, with `relative`, the offset from
+    the sphere centre in units of 4 diameters (which side of the sphere a cell
+    lies on: a cell downstream sits in the wake); [n_cells][6] without."""
     c = np.asarray(ma.cell_centroid, np.float64).reshape(-1, 3)[: ma.n_cells]
-    sd = (np.linalg.norm(c - np.asarray(centre, np.float64), axis=1) - diameter / 2) / diameter
-    f = np.empty((ma.n_cells, 6))
+    d = c - np.asarray(centre, np.float64)
+    sd = (np.linalg.norm(d, axis=1) - diameter / 2) / diameter
+    f = np.empty((ma.n_cells, 9 if relative else 6))
     f[:, :3] = c / np.asarray(lengths, np.float64)
     f[:, 3] = sd
     f[:, 4] = 1.0 / (1.0 + sd * sd)
     f[:, 5] = re / 200.0
+    if relative:
+        f[:, 6:9] = d / (4.0 * diameter)
     return f.astype(np.float32)
 
 

@@ -26,13 +26,17 @@ def test_graph_has_two_edges_per_internal_face():
 def test_node_features():
     ma = _small_mesh()
     f = gnn.node_features(ma, (6, 5, 4), (3.0, 2.5, 2.0), 2.0, 100.0)
-    assert f.shape == (ma.n_cells, 6) and f.dtype == np.float32
+    assert f.shape == (ma.n_cells, 9) and f.dtype == np.float32
     assert f[:, 3].min() < 0 < f[:, 3].max()  # cells inside and outside the sphere
     np.testing.assert_allclose(f[:, 5], 0.5)
+    c = np.asarray(ma.cell_centroid).reshape(-1, 3)[: ma.n_cells]
+    np.testing.assert_allclose(f[:, 6:9], (c - [3.0, 2.5, 2.0]) / 8.0, rtol=1e-6)
+    f6 = gnn.node_features(ma, (6, 5, 4), (3.0, 2.5, 2.0), 2.0, 100.0, relative=False)
+    np.testing.assert_array_equal(f6, f[:, :6])
 
 
 def test_param_layout_and_reference_model():
-    nf, ef_, L, out = 6, 4, 2, 4
+    nf, ef_, L, out = 9, 4, 2, 4
     p = gnn.init_params(nf, ef_, L, out, seed=1)
     assert p.size == gnn.param_count(nf, ef_, L, out)
     ma = _small_mesh()

@@ -11,7 +11,7 @@ from plfbs import cases, gnn
 
 pytestmark = pytest.mark.gpu
 
-NF, EF, OUT = 6, 4, 4
+NF, EF, OUT = 9, 4, 4
 
 
 def _graph(nx=9, ny=7, nz=5):
