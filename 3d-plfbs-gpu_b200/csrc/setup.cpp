@@ -256,7 +256,7 @@ std::vector<int32_t> cell_order(int C, int Fi, const int32_t* owner, const int32
                                 int renumber) {
   if (renumber == 1 || renumber == 2) return rcm_order(C, Fi, owner, nb);
   std::vector<int32_t> order(C);
-  std::iota(order.begin(), order.end(), 0);
+  parallel_for(C, [&](int i) { order[i] = i; });
   return order;
 }
 
@@ -346,8 +346,14 @@ int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out) {
       }
     }
   }
-  int K = 0;
-  for (int i = 0; i < C; i++) K = std::max(K, m.stencil_offsets[i + 1] - m.stencil_offsets[i]);
+  std::atomic<int> Kmax(0);
+  parallel_for(C, [&](int i) {
+    const int k = m.stencil_offsets[i + 1] - m.stencil_offsets[i];
+    int cur = Kmax.load(std::memory_order_relaxed);
+    while (k > cur && !Kmax.compare_exchange_weak(cur, k, std::memory_order_relaxed)) {
+    }
+  });
+  const int K = Kmax.load();
   if (K == 0) {
     err = "empty gradient stencil";
     return PLFBS_ERR_MESH;
@@ -408,21 +414,23 @@ int order_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
   const bool cpu = cfg.flavour == PLFBS_FLAVOUR_CPU_SOLVER;
   L.cell_old_of_new = std::move(order);
   L.cell_new_of_old.resize(C);
-  for (int i = 0; i < C; i++) L.cell_new_of_old[L.cell_old_of_new[i]] = i;
+  parallel_for(C, [&](int i) { L.cell_new_of_old[L.cell_old_of_new[i]] = i; });
 
-  // Boundary faces by new owner (stable). The internal faces are ordered on
-  // the device (layout.cu).
-  std::vector<int32_t> fbnd(B);
-  std::iota(fbnd.begin(), fbnd.end(), Fi);
-  std::stable_sort(fbnd.begin(), fbnd.end(), [&](int a, int b) {
-    return L.cell_new_of_old[m.owner[a]] < L.cell_new_of_old[m.owner[b]];
+  // Boundary faces by new owner, ties in face order (a stable sort by owner):
+  // one sort of packed (new owner, boundary index) keys. The internal faces
+  // are ordered on the device (layout.cu).
+  std::vector<uint64_t> key(B);
+  parallel_for(B, [&](int b) {
+    key[b] = (uint64_t)(uint32_t)L.cell_new_of_old[m.owner[Fi + b]] << 32 | (uint32_t)b;
   });
+  std::sort(key.begin(), key.end());
   L.bc_old_of_new.resize(B);
   L.bc_new_of_old.resize(B);
-  for (int b = 0; b < B; b++) {
-    L.bc_old_of_new[b] = fbnd[b] - Fi;
-    L.bc_new_of_old[fbnd[b] - Fi] = b;
-  }
+  parallel_for(B, [&](int b) {
+    const int bo = (int)(uint32_t)key[b];
+    L.bc_old_of_new[b] = bo;
+    L.bc_new_of_old[bo] = b;
+  });
   L.quirk_b = B > 0 ? L.bc_new_of_old[0] : -1;
 
   // --- boundary records --------------------------------------------------------
@@ -431,7 +439,9 @@ int order_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
   L.bc2.assign(4 * (size_t)B, 0.0);
   L.bc3.assign(4 * (size_t)B, 0.0);
   const double H = cfg.channel_height, H2 = H * 0.5, H4 = H * H * H * H;
-  for (int bn = 0; bn < B; bn++) {
+  // records of the boundary faces in the new order, on the host threads; the
+  // first face (new order) whose ghost sits on its owner is reported
+  const int bad = first_bad(B, [&](int bn) {
     const int bo = L.bc_old_of_new[bn];
     const int f = Fi + bo;
     const int own = m.owner[f];
@@ -460,10 +470,12 @@ int order_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
     t[1] = cpu ? 1 - n[1] : 1 - std::fabs(n[1]);
     t[2] = cpu ? 1 - n[2] : 1 - std::fabs(n[2]);
     t[3] = (double)(bcv.rho_type[bo] | (bcv.vel_type[bo] << 8));
-    if (!(dmag > 0)) {
-      err = msg("ghost centroid coincides with its owner's", bo, own);
-      return PLFBS_ERR_MESH;
-    }
+    return !(dmag > 0);
+  });
+  if (bad < B) {
+    const int bo = L.bc_old_of_new[bad];
+    err = msg("ghost centroid coincides with its owner's", bo, m.owner[Fi + bo]);
+    return PLFBS_ERR_MESH;
   }
   return PLFBS_OK;
 }
