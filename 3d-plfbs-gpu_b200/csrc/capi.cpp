@@ -370,37 +370,45 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   ctx->cfg = *cfg;
   std::string err;
   int rc;
+  // With the device present, the mesh's face and cell arrays start on their
+  // way to it now and the host validates them meanwhile (from page-locked
+  // memory the copies run alongside); without it, the validation comes first
+  // as always and its errors are reported before the missing device.
+  const bool have_device = check_device(device) == PLFBS_OK;
+  auto drop = [&](int code, const std::string& m) {
+    if (ctx->stream)
+      plfbs_destroy(ctx);  // waits for the copies, returns the staged memory
+    else
+      delete ctx;  // nothing on a device
+    return set_err(nullptr, code, m);
+  };
+  if (have_device) {
+    NvtxRange r("mesh upload");
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+      return drop(PLFBS_ERR_CUDA, "cudaSetDevice / stream creation failed");
+    if (stage_mesh(ctx, *mesh)) return drop(PLFBS_ERR_CUDA, ctx->err);
+  }
   {
     NvtxRange r("prepare_layout (host)");
     rc = plfbs::prepare_layout(*cfg, *mesh, *bc, ctx->L, err);
   }
-  if (rc) {
-    delete ctx;
-    return set_err(nullptr, rc, err);
-  }
+  if (rc) return drop(rc, err);
   const Layout& L = ctx->L;
   const bool fp32 = cfg->precision == PLFBS_FP32_DEVIATION;
   const int N = (ibm && ibm->n_nodes > 0) ? ibm->n_nodes : 0;
   if (N > 0) {
     if (!ibm->x || !ibm->x_ref || ibm->object_nodes <= 0 || !(cfg->domain_dt > 0) ||
         !(cfg->lengths[0] > 0) || !(cfg->lengths[1] > 0)) {
-      delete ctx;
-      return set_err(nullptr, PLFBS_ERR_ARG,
-                     "IBM needs node arrays, object_nodes > 0, domain_dt > 0 and lengths > 0");
+      return drop(PLFBS_ERR_ARG,
+                  "IBM needs node arrays, object_nodes > 0, domain_dt > 0 and lengths > 0");
     }
   }
   // validation needs no GPU; the device is checked before the layout is built
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) {
-    delete ctx;
-    return set_err(nullptr, PLFBS_ERR_NO_DEVICE, "no CUDA device with that index");
-  }
-  int major = 0;  // one attribute (cudaGetDeviceProperties fills every field and can be slow)
-  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess ||
-      major != 10) {
-    delete ctx;
-    return set_err(nullptr, PLFBS_ERR_NO_DEVICE,
-                   "this library is built for sm_100a (B200); device major != 10");
+  if (!have_device) {
+    check_device(device);  // sets the message
+    const std::string m = g_err;
+    return drop(PLFBS_ERR_NO_DEVICE, m);
   }
   ctx->N = N;
   auto fail = [&](int code) {
@@ -409,10 +417,8 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     g_err = m;
     return code;
   };
-  if (cudaSetDevice(device) != cudaSuccess) return fail(set_err(ctx, PLFBS_ERR_CUDA, "cudaSetDevice"));
-  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
-    return fail(set_err(ctx, PLFBS_ERR_CUDA, "stream/event creation failed"));
+  if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
+    return fail(set_err(ctx, PLFBS_ERR_CUDA, "event creation failed"));
   if (!(ctx->stats_host = take_pinned_stats()))
     return fail(set_err(ctx, PLFBS_ERR_CUDA, "cudaMallocHost failed"));
   if (cfg->renumber == 2) {  // the order on the device, then the host's order-dependent part
@@ -480,6 +486,7 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   {
     NvtxRange r("device layout");
     if ((rc = build_device_layout(ctx, *mesh))) return fail(rc);
+    free_stage(ctx);  // stream-ordered: after the layout kernels that read it
   }
   {
     NvtxRange r("compact layout");
@@ -574,7 +581,11 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     if ((rc = reset_force(ctx))) return fail(rc);
   }
   if ((rc = capture_step(ctx))) return fail(rc);
-  if (cudaDeviceSynchronize() != cudaSuccess) return fail(set_err(ctx, PLFBS_ERR_CUDA, "setup failed"));
+  // this context's stream only: a device-wide synchronise would also wait on
+  // a stream another thread is capturing into its step graph, which ends that
+  // capture with an error
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+    return fail(set_err(ctx, PLFBS_ERR_CUDA, "setup failed"));
   *out = ctx;
   return PLFBS_OK;
 }
@@ -584,6 +595,7 @@ void plfbs_destroy(plfbs_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
+  if (ctx->stream) free_stage(ctx);
   for (void* p : ctx->allocs) cudaFreeAsync(p, ctx->stream);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->stats_host) give_pinned_stats(ctx->stats_host);

@@ -38,6 +38,18 @@ struct plfbs_ctx {
   int compact_faces = 0;          // unique face records in the compact layout (0: none)
   int compact_cells = 0;          // unique cell weight sets in the compact layout (0: none)
   bool flux_maps_ok = false;
+  // The caller's face and cell arrays, copied to the device at the start of
+  // plfbs_create while the host validates them (read only after it has):
+  // owner, neighbour [F] int; area, sdt [F], normal, fcen [3F], vol [C],
+  // ccen [3(C+B)] double. Freed once the layout is built.
+  struct MeshStage {
+    bool ok = false;
+    const int32_t* owner = nullptr;
+    const int32_t* neighbour = nullptr;
+    const double *area = nullptr, *normal = nullptr, *fcen = nullptr, *sdt = nullptr,
+                 *vol = nullptr, *ccen = nullptr;
+    std::vector<void*> bufs;
+  } stage;
   double timeout_s = 0;  // bound on plfbs_run's waits for its step batches (0: none)
   bool busy = false;     // a timed-out run's steps are still in flight (ev1 marks their end)
   std::string err;
@@ -73,6 +85,11 @@ int check_device(int device);
 // The face, stencil and gather arrays of a context on the device, and the
 // compact layout (capi_layout.cpp).
 int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m);
+// Starts the copies of the mesh's face and cell arrays (sizes from the view's
+// counts, checked positive first) into ctx->stage; returns without staging
+// when the counts or pointers are not usable (the layout then uploads them).
+int stage_mesh(plfbs_ctx* ctx, const plfbs_mesh_view& m);
+void free_stage(plfbs_ctx* ctx);
 int build_compact_layout(plfbs_ctx* ctx);
 
 // The renumber-1 cell order (reverse Cuthill-McKee, order[new] = caller cell)

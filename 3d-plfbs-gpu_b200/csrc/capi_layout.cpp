@@ -47,6 +47,52 @@ struct ScratchList {
   }
 };
 
+int stage_mesh(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
+  auto& g = ctx->stage;
+  g.ok = false;
+  const long long C = m.n_cells, F = m.n_faces, Fi = m.n_internal;
+  if (C <= 0 || F <= 0 || Fi < 0 || Fi > F || 2 * F >= (1LL << 31) || !m.owner ||
+      !m.neighbour || !m.face_area || !m.face_normal || !m.face_centroid || !m.streaming_dt ||
+      !m.cell_volume || !m.cell_centroid)
+    return PLFBS_OK;  // validation reports it
+  const long long T = C + (F - Fi);
+  cudaMemPool_t pool = device_pool(ctx->device);
+  if (!pool) return set_err(ctx, PLFBS_ERR_CUDA, "device memory pool creation failed");
+  auto up = [&](const void* src, size_t bytes, const void** dst) -> int {
+    void* p = nullptr;
+    CK(cudaMallocFromPoolAsync(&p, std::max<size_t>(bytes, 16), pool, ctx->stream));
+    g.bufs.push_back(p);
+    CK(cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    *dst = p;
+    return PLFBS_OK;
+  };
+  const void* q = nullptr;
+  TRY(up(m.owner, 4 * (size_t)F, &q));
+  g.owner = static_cast<const int32_t*>(q);
+  TRY(up(m.neighbour, 4 * (size_t)F, &q));
+  g.neighbour = static_cast<const int32_t*>(q);
+  TRY(up(m.face_area, 8 * (size_t)F, &q));
+  g.area = static_cast<const double*>(q);
+  TRY(up(m.face_normal, 24 * (size_t)F, &q));
+  g.normal = static_cast<const double*>(q);
+  TRY(up(m.face_centroid, 24 * (size_t)F, &q));
+  g.fcen = static_cast<const double*>(q);
+  TRY(up(m.streaming_dt, 8 * (size_t)F, &q));
+  g.sdt = static_cast<const double*>(q);
+  TRY(up(m.cell_volume, 8 * (size_t)C, &q));
+  g.vol = static_cast<const double*>(q);
+  TRY(up(m.cell_centroid, 24 * (size_t)T, &q));
+  g.ccen = static_cast<const double*>(q);
+  g.ok = true;
+  return PLFBS_OK;
+}
+
+void free_stage(plfbs_ctx* ctx) {
+  for (void* p : ctx->stage.bufs) cudaFreeAsync(p, ctx->stream);
+  ctx->stage.bufs.clear();
+  ctx->stage.ok = false;
+}
+
 // The face, stencil and gather arrays of a context, built on the device from
 // the caller's mesh arrays (layout.cu); sets args' layout pointers, L.K2 and
 // the mesh fingerprint.
@@ -64,14 +110,26 @@ int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
   d.F = L.F;
   d.Fi = L.Fi;
   d.B = L.B;
-  TRY(S.upload(&d.owner, m.owner, F));
-  TRY(S.upload(&d.neighbour, m.neighbour, F));
-  TRY(S.upload(&d.area, m.face_area, F));
-  TRY(S.upload(&d.normal, m.face_normal, 3 * F));
-  TRY(S.upload(&d.fcen, m.face_centroid, 3 * F));
-  TRY(S.upload(&d.sdt, m.streaming_dt, F));
-  TRY(S.upload(&d.vol, m.cell_volume, C));
-  TRY(S.upload(&d.ccen, m.cell_centroid, 3 * T));
+  if (ctx->stage.ok) {  // copied at the start of plfbs_create
+    const auto& g = ctx->stage;
+    d.owner = g.owner;
+    d.neighbour = g.neighbour;
+    d.area = g.area;
+    d.normal = g.normal;
+    d.fcen = g.fcen;
+    d.sdt = g.sdt;
+    d.vol = g.vol;
+    d.ccen = g.ccen;
+  } else {
+    TRY(S.upload(&d.owner, m.owner, F));
+    TRY(S.upload(&d.neighbour, m.neighbour, F));
+    TRY(S.upload(&d.area, m.face_area, F));
+    TRY(S.upload(&d.normal, m.face_normal, 3 * F));
+    TRY(S.upload(&d.fcen, m.face_centroid, 3 * F));
+    TRY(S.upload(&d.sdt, m.streaming_dt, F));
+    TRY(S.upload(&d.vol, m.cell_volume, C));
+    TRY(S.upload(&d.ccen, m.cell_centroid, 3 * T));
+  }
   TRY(S.upload(&d.st_off, m.stencil_offsets, C + 1));
   TRY(S.upload(&d.st_cells, m.stencil_cells, nnz));
   TRY(S.upload(&d.st_faces, m.stencil_faces, nnz));

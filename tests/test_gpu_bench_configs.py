@@ -128,3 +128,32 @@ def test_scale_channel_2_steps_against_oracle(plfbs_lib):
         assert rel_l2(got[:, k], o.state[:, k]) < RUN_TOL, k
     assert rel_err(hist, o.history) < 1e-10
     assert rel_err(x, o.node_x) < 1e-12
+
+
+def test_sphere_channel_20000_steps_against_reference_cuda(plfbs_lib, tmp_path):
+    """The 128 x 64 x 64 channel with its 3,217-node sphere over the full
+    length its configuration names, 20,000 steps (t = 4,000, about three
+    flow-through times of the sphere's wake), against the reference's own CUDA
+    path run here for the same steps: every field to 1e-10 relative L2, the
+    IBM nodes to 1e-10. Drag and lift of the sphere from the node forces
+    (C = -sum F / (rho U^2 pi D^2 / 8)) are printed for the record; the
+    reference never reduces the IBM force, so they have no reference value."""
+    if not os.path.exists(BIN_GPU):
+        pytest.skip("oracle/_ref/plfbs_ref_gpu not built (needs the reference sources)")
+    w, steps = bench.SPHERE, 20000
+    pm, c, ma, nodes, state0, bcs = _channel(w)
+    s = capi.Solver(ma, *bcs, bench.solver_cfg(c, renumber=1), ibm=bench.ibm_cfg(w, nodes))
+    s.set_state(state0)
+    st, hist = s.run(steps)
+    assert st["rc"] == 0 and st["steps_done"] == steps
+    got = s.get_state()
+    cd, cl = s.body_force(np.pi * w.diam ** 2 / 4)
+    s.close()
+    print("cfg 2, %d steps: Cd %.6f Cl %.3e, max_error %.3e" % (steps, cd, cl, hist[-1, 1]))
+    c.steps = steps
+    dumps = refrun.run_reference(str(tmp_path), pm, c, nodes=nodes, init_state=state0,
+                                 binary=BIN_GPU, timeout=1500)
+    ref = dumps["ref_gpu_final_state"]
+    for k in range(4):
+        assert rel_l2(got[:, k], ref[:, k]) < RUN_TOL, k
+    assert 0.5 < cd < 5.0 and abs(cl) < 0.1 * cd  # a sphere's drag, lift near zero
