@@ -12,10 +12,12 @@
 //             X1^T dZ1, relu(Z1)^T dY and the bias sums accumulated per block
 //             across its tiles; a second kernel adds the block partials in a
 //             fixed order, so gradients are deterministic.
-// The products run on the tensor cores as mma.sync m16n8k16 BF16 x BF16 ->
-// FP32, operands fetched with ldmatrix (.trans for the transposed products),
-// one warp per 16 rows. Aggregation over edges goes through CSR lists (no
-// atomics). Activations and master weights are FP32; Adam runs on the device.
+// The products run on the tensor cores: by default as tcgen05 MMAs (one
+// thread issuing 128 x N x 16 BF16 products from shared-memory descriptors,
+// FP32 accumulators in tensor memory; the backward's transposed operands read
+// through MN-major descriptors), or as mma.sync m16n8k16 BF16 x BF16 -> FP32
+// with ldmatrix operands (.trans for the transposed products), one warp per
+// 16 rows. Aggregation over edges goes through CSR lists (no atomics). Activations and master weights are FP32; Adam runs on the device.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -313,6 +315,19 @@ __device__ __forceinline__ uint64_t smem_desc(const void* base, int K) {
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
          ((uint32_t)(M >> 4) << 24);
+}
+// The same canonical [rows][C] tile read MN-major (the backward's transposed
+// operands): its C columns are the M (or N) dimension and its rows the K
+// dimension, so the 8-column groups (128 B apart) are the stride byte offset
+// and the 8-row groups (C * 16 B apart) the leading byte offset.
+__device__ __forceinline__ uint64_t smem_desc_mn(const void* base, int C) {
+  const uint64_t addr = su32(base);
+  return ((addr & 0x3FFFFull) >> 4) | ((uint64_t)((C * 16) >> 4) << 16) |
+         ((uint64_t)(128 >> 4) << 32) | (1ull << 46);
+}
+// idesc_bf16 with A (bit 15) and B (bit 16) read MN-major.
+__host__ __device__ constexpr uint32_t idesc_bf16_mn(int M, int N) {
+  return idesc_bf16(M, N) | (1u << 15) | (1u << 16);
 }
 __device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
                                      int accumulate) {
@@ -718,13 +733,292 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_bwd(const Bwd a) {
   }
 }
 
-// Sum of the block partials (fixed order) into the flat gradient of one MLP:
-// W1 [kin][64], b1 [64], W2 [64][out], b2 [out].
-__global__ void k_reduce_parts(const float* part, int nblk, int K1, int NOUT, int kin, int out,
-                               float* grad) {
+// ---------------------------------------------------------------------------
+// backward, tcgen05 form. Per 128-row tile, five products on the tensor cores
+// with FP32 accumulators in tensor memory:
+//   dA   = dY W2^T          A = dY [128][NOUT], B = W2 [64][NOUT]        (K-major)
+//   dW2 += relu(Z1)^T dY     A = relu(Z1), B = dY, both read MN-major
+//   dZ1  = dA where Z1 > 0   (epilogue: tensor memory -> shared memory)
+//   dX1  = dZ1 W1^T          A = dZ1 [128][64], B = W1 [K1][64]          (K-major)
+//   dW1 += X1^T dZ1          A = X1 read MN-major (128 features per MMA), B = dZ1 MN-major
+// The transposed operands are the K-major tiles themselves, read through
+// MN-major descriptors, so nothing is transposed in memory. dW1 and dW2 stay
+// in tensor memory over all of the block's tiles and are written once as the
+// block's partials, like k_mlp_bwd's; db1 and db2 are per-thread sums added
+// in a fixed order. An MMA's rows past a matrix's last feature read the
+// operand buffer that follows it and land in accumulator rows nobody reads.
+// Tensor memory: dA and then dX1 in columns [0, K1), dW1 in [192, 192 + 64 *
+// ceil(K1 / 128)), dW2 after it; 512 columns, one block per SM.
+// ---------------------------------------------------------------------------
+constexpr int kBwdCols = 512;
+
+template <int K1, int NOUT>
+constexpr size_t bwd_tc_smem() {
+  // the operands and the mbarrier; at least 116 KB so that an SM holds one
+  // block (two blocks' 2 x 512 tensor-memory columns would not fit), which
+  // also covers the end-of-kernel bias reduction buffers (66 KB)
+  return std::max<size_t>(
+      2 * (size_t)(TM * K1 + TM * NOUT + 2 * TM * H + K1 * H + H * NOUT) + 16, 118784);
+}
+
+template <int MODE, int K1, int NOUT>
+__global__ void __launch_bounds__(kTcThreads, 1) k_mlp_bwd_tc(const Bwd a, int* err) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned char* Xs = smem;                 // X1 [128][K1]
+  unsigned char* Ds = Xs + TM * K1 * 2;     // dY [128][NOUT] (BF16)
+  unsigned char* As = Ds + TM * NOUT * 2;   // relu(Z1) [128][64]
+  unsigned char* Zs = As + TM * H * 2;      // dZ1 [128][64]
+  unsigned char* W1c = Zs + TM * H * 2;     // W1 [K1][64]
+  unsigned char* W2c = W1c + K1 * H * 2;    // W2 [64][NOUT]
+  // the mbarrier and the tensor-memory address at the end, clear of the
+  // bias reduction buffers that reuse the operands' space
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + bwd_tc_smem<K1, NOUT>() - 16);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(mbar + 1);
+  constexpr int MT = (K1 + TM - 1) / TM;    // 128-feature row blocks of dW1
+  constexpr uint32_t cX = 0, cW1 = 192, cW2 = cW1 + 64 * MT;
+  static_assert(K1 <= 192 && H <= 192 && cW2 + NOUT <= kBwdCols, "tensor-memory columns");
+  static_assert(NOUT % 16 == 0 && K1 % 16 == 0, "MMA shapes");
+  constexpr int GB2 = (TM * (NOUT / 8) + kTcThreads - 1) / kTcThreads * 8;  // dY columns a thread sums
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < K1 * H; i += kTcThreads)
+    *reinterpret_cast<bf16*>(W1c + canon_off(i / H, i % H, H)) = a.W1[i];
+  for (int i = tid; i < H * NOUT; i += kTcThreads)
+    *reinterpret_cast<bf16*>(W2c + canon_off(i / NOUT, i % NOUT, NOUT)) = a.W2[i];
+  if (tid == 0) mbar_init(mbar, 1);
+  if (warp == 0) tmem_alloc(slot, kBwdCols);
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *slot;
+  const int quarter = warp & 3, half = warp >> 2;
+  const uint32_t lanes = (uint32_t)(quarter * 32) << 16;  // this warp's 32 accumulator rows
+  const int r = quarter * 32 + lane;                       // this thread's row of the tile
+  float gb1[32], gb2[GB2];
+#pragma unroll
+  for (int i = 0; i < 32; i++) gb1[i] = 0.f;
+#pragma unroll
+  for (int i = 0; i < GB2; i++) gb2[i] = 0.f;
+  uint32_t parity = 0;
+  bool ok = true, any = false;
+  const int ntiles = (a.x.M + TM - 1) / TM;
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int row0 = tile * TM, m = row0 + r;
+    load_x_canon<MODE, K1>(a.x, row0, Xs);
+    // dY (plus the node aggregate's gradient at dst for an edge MLP) as BF16,
+    // its column sums (db2) kept per thread: thread tid holds row tid % 128 of
+    // the 8-column chunks tid / 128 + 2 j
+#pragma unroll
+    for (int j = 0; j < GB2 / 8; j++) {
+      const int q = tid + kTcThreads * j, rr = q % TM, k = 8 * (q / TM), mm = row0 + rr;
+      float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (mm < a.x.M) {
+        if (a.dy) ldg8(a.dy + (size_t)mm * NOUT + k, v);
+        if (MODE == EDGE && a.dadd) {
+          float d[8];
+          ldg8(a.dadd + (size_t)a.x.dst[mm] * H + k, d);
+#pragma unroll
+          for (int i = 0; i < 8; i++) v[i] += d[i];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; i++) gb2[8 * j + i] += v[i];
+      __nv_bfloat162 b[4] = {__floats2bfloat162_rn(v[0], v[1]), __floats2bfloat162_rn(v[2], v[3]),
+                             __floats2bfloat162_rn(v[4], v[5]), __floats2bfloat162_rn(v[6], v[7])};
+      *reinterpret_cast<uint4*>(Ds + canon_off(rr, k, NOUT)) = *reinterpret_cast<const uint4*>(b);
+    }
+    for (int q = tid; q < TM * (H / 8); q += kTcThreads) {
+      const int rr = q % TM, k = 8 * (q / TM), mm = row0 + rr;
+      float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (mm < a.x.M) ldg8(a.z1 + (size_t)mm * H + k, v);
+      __nv_bfloat162 b[4] = {
+          __floats2bfloat162_rn(fmaxf(v[0], 0.f), fmaxf(v[1], 0.f)),
+          __floats2bfloat162_rn(fmaxf(v[2], 0.f), fmaxf(v[3], 0.f)),
+          __floats2bfloat162_rn(fmaxf(v[4], 0.f), fmaxf(v[5], 0.f)),
+          __floats2bfloat162_rn(fmaxf(v[6], 0.f), fmaxf(v[7], 0.f))};
+      *reinterpret_cast<uint4*>(As + canon_off(rr, k, H)) = *reinterpret_cast<const uint4*>(b);
+    }
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int k0 = 0; k0 < NOUT; k0 += 16)
+        umma(tmem + cX, smem_desc(Ds + k0 * 16, NOUT), smem_desc(W2c + k0 * 16, NOUT),
+             idesc_bf16(TM, H), k0 > 0);
+#pragma unroll
+      for (int k0 = 0; k0 < TM; k0 += 16)
+        umma(tmem + cW2, smem_desc_mn(As + k0 * H * 2, H), smem_desc_mn(Ds + k0 * NOUT * 2, NOUT),
+             idesc_bf16_mn(TM, NOUT), any || k0 > 0);
+      umma_commit(mbar);
+    }
+    __syncwarp();
+    ok = mbar_wait(mbar, parity);
+    parity ^= 1u;
+    tc_fence_after();
+    // dZ1 = dA where Z1 > 0, into shared memory; db1 per thread
+#pragma unroll
+    for (int c = 0; c < 32; c += 16) {
+      const int c0 = 32 * half + c;
+      float v[16];
+      tmem_ld16(tmem + cX + lanes + c0, v);
+      __align__(16) bf16 av[16];
+      *reinterpret_cast<uint4*>(av) = *reinterpret_cast<const uint4*>(As + canon_off(r, c0, H));
+      *reinterpret_cast<uint4*>(av + 8) =
+          *reinterpret_cast<const uint4*>(As + canon_off(r, c0 + 8, H));
+      __align__(16) bf16 zb[16];
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        const float z = __bfloat162float(av[i]) > 0.f ? v[i] : 0.f;
+        gb1[c + i] += z;
+        zb[i] = __float2bfloat16_rn(z);
+      }
+      *reinterpret_cast<uint4*>(Zs + canon_off(r, c0, H)) = *reinterpret_cast<const uint4*>(zb);
+      *reinterpret_cast<uint4*>(Zs + canon_off(r, c0 + 8, H)) =
+          *reinterpret_cast<const uint4*>(zb + 8);
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      if (MODE != ENC) {
+#pragma unroll
+        for (int k0 = 0; k0 < H; k0 += 16)
+          umma(tmem + cX, smem_desc(Zs + k0 * 16, H), smem_desc(W1c + k0 * 16, H),
+               idesc_bf16(TM, K1), k0 > 0);
+      }
+#pragma unroll
+      for (int t = 0; t < MT; t++)
+#pragma unroll
+        for (int k0 = 0; k0 < TM; k0 += 16)
+          umma(tmem + cW1 + 64 * t, smem_desc_mn(Xs + k0 * K1 * 2 + t * 2048, K1),
+               smem_desc_mn(Zs + k0 * H * 2, H), idesc_bf16_mn(TM, H), any || k0 > 0);
+      umma_commit(mbar);
+    }
+    __syncwarp();
+    ok = mbar_wait(mbar, parity) && ok;
+    parity ^= 1u;
+    tc_fence_after();
+    any = true;
+    if (MODE != ENC) {
+      // dX1 by input segment of 64 columns; the residual path passes dY through
+      // to segment 0 (not for the decoder)
+      constexpr int HALF = K1 / 2;
+#pragma unroll
+      for (int c0 = HALF * half; c0 < HALF * half + HALF; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + cX + lanes + c0, v);
+        const int seg = c0 / H, col = c0 % H;
+        if (m < a.x.M) {
+          if (seg == 0 && MODE != DEC) {
+            float d0[8] = {}, d1[8] = {};
+            if (a.dy) {
+              ldg8(a.dy + (size_t)m * NOUT + col, d0);
+              ldg8(a.dy + (size_t)m * NOUT + col + 8, d1);
+            }
+            if (MODE == EDGE && a.dadd) {
+              float e0[8], e1[8];
+              ldg8(a.dadd + (size_t)a.x.dst[m] * H + col, e0);
+              ldg8(a.dadd + (size_t)a.x.dst[m] * H + col + 8, e1);
+#pragma unroll
+              for (int i = 0; i < 8; i++) {
+                d0[i] += e0[i];
+                d1[i] += e1[i];
+              }
+            }
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+              v[i] += d0[i];
+              v[8 + i] += d1[i];
+            }
+          }
+          float* out = seg == 0 ? a.dx0 : (seg == 1 ? a.dseg1 : a.dseg2);
+          stg8(out + (size_t)m * H + col, v);
+          stg8(out + (size_t)m * H + col + 8, v + 8);
+        }
+      }
+    }
+    tc_fence_before();
+    ok = __syncthreads_and(ok);  // operands and accumulators free for the next tile
+  }
+  tc_fence_after();
+  // block partials: [dW1 K1 x 64][db1 64][dW2 64 x NOUT][db2 NOUT]
+  float* P = a.part + (size_t)blockIdx.x * (K1 * H + H + H * NOUT + NOUT);
+  float* P2 = P + K1 * H + H;
+#pragma unroll
+  for (int t = 0; t < MT; t++) {
+    const int f = TM * t + r;  // feature of this accumulator row
+#pragma unroll
+    for (int c = 0; c < 32; c += 16) {
+      const int c0 = 32 * half + c;
+      float v[16];
+      if (any) {
+        tmem_ld16(tmem + cW1 + 64 * t + lanes + c0, v);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; i++) v[i] = 0.f;
+      }
+      if (f < K1) {
+        stg8(P + (size_t)f * H + c0, v);
+        stg8(P + (size_t)f * H + c0 + 8, v + 8);
+      }
+    }
+  }
+  for (int c0 = 16 * half; c0 < NOUT; c0 += 32) {  // dW2: rows are the 64 hidden units
+    float v[16];
+    if (any) {
+      tmem_ld16(tmem + cW2 + lanes + c0, v);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 16; i++) v[i] = 0.f;
+    }
+    if (r < H) {
+      stg8(P2 + (size_t)r * NOUT + c0, v);
+      stg8(P2 + (size_t)r * NOUT + c0 + 8, v + 8);
+    }
+  }
+  // db1 and db2: the per-thread sums through shared memory (the operands are
+  // no longer read: every MMA has completed), added over rows in order
+  float* red = reinterpret_cast<float*>(smem);  // [128][65]
+  float* red2 = red + TM * (H + 1);             // [256][GB2 + 1]
+#pragma unroll
+  for (int i = 0; i < 32; i++) red[r * (H + 1) + 32 * half + i] = gb1[i];
+#pragma unroll
+  for (int i = 0; i < GB2; i++) red2[tid * (GB2 + 1) + i] = gb2[i];
+  __syncthreads();
+  if (tid < H) {
+    float s = 0.f;
+    for (int rr = 0; rr < TM; rr++) s += red[rr * (H + 1) + tid];
+    P[K1 * H + tid] = s;
+  } else if (tid >= 128 && tid < 128 + NOUT) {
+    const int c = tid - 128, ch = c / 8, t0 = (ch % 2) * TM, j = ch / 2;
+    float s = 0.f;
+    for (int rr = 0; rr < TM; rr++) s += red2[(t0 + rr) * (GB2 + 1) + 8 * j + c % 8];
+    P2[H * NOUT + c] = s;
+  }
+  if (!ok && tid == 0) atomicExch(err, 1);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc(tmem, kBwdCols);
+}
+
+// Sum of the block partials into the flat gradient of one MLP:
+// W1 [kin][64], b1 [64], W2 [64][out], b2 [out]. A block takes 32 gradient
+// entries (consecutive, so each warp's loads are coalesced) and its 8 warps
+// split the partials: warp w sums blocks w, w + 8, ... in order, and the 8 sums
+// are added in warp order, a fixed order whatever the launch.
+constexpr int kReduceWarps = 8;
+__global__ void __launch_bounds__(32 * kReduceWarps)
+    k_reduce_parts(const float* part, int nblk, int K1, int NOUT, int kin, int out, float* grad) {
+  __shared__ float sums[kReduceWarps][32];
   const int stride = K1 * H + H + H * NOUT + NOUT;
   const int n1 = kin * H, n2 = n1 + H, n3 = n2 + H * out, n4 = n3 + out;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = blockIdx.x * 32 + lane;
+  float s = 0.f;
+  if (i < n4) {
     int po;
     if (i < n1)
       po = i;
@@ -734,9 +1028,16 @@ __global__ void k_reduce_parts(const float* part, int nblk, int K1, int NOUT, in
       po = K1 * H + H + ((i - n2) / out) * NOUT + (i - n2) % out;
     else
       po = K1 * H + H + H * NOUT + (i - n3);
-    float s = 0.f;
-    for (int b = 0; b < nblk; b++) s += part[(size_t)b * stride + po];
-    grad[i] = s;
+#pragma unroll 4
+    for (int b = w; b < nblk; b += kReduceWarps) s += part[(size_t)b * stride + po];
+  }
+  sums[w][lane] = s;
+  __syncthreads();
+  if (w == 0 && i < n4) {
+    float t = sums[0][lane];
+#pragma unroll
+    for (int k = 1; k < kReduceWarps; k++) t += sums[k][lane];
+    grad[i] = t;
   }
 }
 
@@ -853,7 +1154,7 @@ struct plfbs_gnn {
         *ddst = nullptr, *dagg = nullptr, *part = nullptr;
   double* loss_part = nullptr;
   int loss_blocks = 0;
-  int use_tc = 1;           // forward on tcgen05 (1, measured faster) or mma.sync (0)
+  int use_tc = 1;           // MLPs on tcgen05 (1) or mma.sync (0)
   int* tc_err = nullptr;    // set by the tcgen05 kernel if an MMA wait gave up
   std::string err;
 };
@@ -906,6 +1207,9 @@ template <int MODE, int K1, int NOUT>
 int set_smem_tc(plfbs_gnn* g) {
   GCK(cudaFuncSetAttribute(k_mlp_fwd_tc<MODE, K1, NOUT>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem<K1, NOUT>()));
+  GCK(cudaFuncSetAttribute(k_mlp_bwd_tc<MODE, K1, NOUT>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)bwd_tc_smem<K1, NOUT>()));
   return 0;
 }
 
@@ -935,10 +1239,15 @@ int launch_bwd(plfbs_gnn* g, const Mlp& p, const Rows& x, const float* dy, const
                const float* z1, float* dx0, float* dseg1, float* dseg2) {
   const int grid = grid_for(g, x.M, 1);
   Bwd a{x, dy, dadd, z1, p.W1, p.W2, dx0, dseg1, dseg2, g->part};
-  k_mlp_bwd<MODE, K1, NOUT><<<grid, kThreads, bwd_smem<K1, NOUT>(), g->stream>>>(a);
+  if (g->use_tc)
+    k_mlp_bwd_tc<MODE, K1, NOUT><<<grid, kTcThreads, bwd_tc_smem<K1, NOUT>(), g->stream>>>(
+        a, g->tc_err);
+  else
+    k_mlp_bwd<MODE, K1, NOUT><<<grid, kThreads, bwd_smem<K1, NOUT>(), g->stream>>>(a);
   GCK(cudaGetLastError());
-  k_reduce_parts<<<64, 256, 0, g->stream>>>(g->part, grid, K1, NOUT, p.kin, p.out,
-                                            g->grad + p.off);
+  const int n = p.kin * H + H + H * p.out + p.out;
+  k_reduce_parts<<<(n + 31) / 32, 32 * kReduceWarps, 0, g->stream>>>(g->part, grid, K1, NOUT,
+                                                                    p.kin, p.out, g->grad + p.off);
   GCK(cudaGetLastError());
   return 0;
 }
@@ -950,6 +1259,19 @@ int pack_all(plfbs_gnn* g) {
     k_pack<<<64, 256, 0, g->stream>>>(g->params + p.off, p.K1, p.NOUT, p.kin, p.out, p.W1, p.b1,
                                       p.W2, p.b2);
     GCK(cudaGetLastError());
+  }
+  return 0;
+}
+
+// The tcgen05 kernels' error flag: set when an MMA wait gave up.
+int check_tc(plfbs_gnn* g) {
+  if (!g->use_tc) return 0;
+  int flag = 0;
+  GCK(cudaMemcpyAsync(&flag, g->tc_err, sizeof flag, cudaMemcpyDeviceToHost, g->stream));
+  GCK(cudaStreamSynchronize(g->stream));
+  if (flag) {
+    GCK(cudaMemsetAsync(g->tc_err, 0, sizeof flag, g->stream));
+    return gerr(g, PLFBS_ERR_CUDA, "a tensor-core MMA did not complete within its wait limit");
   }
   return 0;
 }
@@ -971,16 +1293,7 @@ int forward(plfbs_gnn* g, bool train) {
   }
   Rows rd{N, g->h[L], nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   GTRY((launch_fwd<DEC, H, FP>(g, g->mlps[2 * L + 2], rd, train ? g->z_dec : nullptr, g->y)));
-  if (g->use_tc) {
-    int flag = 0;
-    GCK(cudaMemcpyAsync(&flag, g->tc_err, sizeof flag, cudaMemcpyDeviceToHost, g->stream));
-    GCK(cudaStreamSynchronize(g->stream));
-    if (flag) {
-      GCK(cudaMemsetAsync(g->tc_err, 0, sizeof flag, g->stream));
-      return gerr(g, PLFBS_ERR_CUDA, "a tensor-core MMA did not complete within its wait limit");
-    }
-  }
-  return 0;
+  return check_tc(g);
 }
 
 int loss_and_grad(plfbs_gnn* g, double* loss) {
@@ -1016,6 +1329,7 @@ int loss_and_grad(plfbs_gnn* g, double* loss) {
   GTRY((launch_bwd<ENC, FP, H>(g, g->mlps[1], rows_enc(E, g->feat_e), g->de, nullptr, g->z_enc_e,
                                nullptr, nullptr, nullptr)));
   GCK(cudaStreamSynchronize(g->stream));
+  GTRY(check_tc(g));
   double s = 0.0;
   for (double v : lp) s += v;
   *loss = s / ((double)N * g->s.outputs);

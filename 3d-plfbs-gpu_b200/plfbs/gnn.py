@@ -199,7 +199,7 @@ class GraphNet:
 def main(argv=None):
     """Times training steps of the network (forward, backward, Adam) on the
     face graph of the warm start's 64 x 32 x 32 channel (65,536 nodes, 8
-    message-passing layers, 6 node / 4 edge features, 4 outputs) with seeded
+    message-passing layers, 9 node / 4 edge features, 4 outputs) with seeded
     synthetic features and targets; prints one JSON line. The command behind
     the committed ncu summary of the network's kernels:
 

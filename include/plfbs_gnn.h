@@ -61,9 +61,10 @@ int plfbs_gnn_gradients(plfbs_gnn* g, const float* node_features, const float* t
 int plfbs_gnn_train_step(plfbs_gnn* g, const float* node_features, const float* target,
                          float learning_rate, double* loss);
 
-/* Which tensor-core instructions the forward MLPs use: 1 = tcgen05
- * (accumulators in tensor memory, one thread issuing the MMAs; the default),
- * 0 = warp-level mma.sync. The backward pass always uses mma.sync. */
+/* Which tensor-core instructions the MLPs use, forward and backward: 1 =
+ * tcgen05 (accumulators in tensor memory, one thread issuing the MMAs; the
+ * backward's weight gradients accumulated in tensor memory over a block's
+ * tiles; the default), 0 = warp-level mma.sync. */
 int plfbs_gnn_set_tensor_cores(plfbs_gnn* g, int32_t kind);
 
 const char* plfbs_gnn_last_error(const plfbs_gnn* g);

@@ -1,7 +1,9 @@
 """Learned warm start on the GPU: the mesh graph network's forward pass,
 loss and every parameter gradient against the torch reference (CPU, same
 BF16 rounding of the matrix-product operands), on a mesh graph whose row
-counts are not multiples of the 128-row tiles; and a short training run."""
+counts are not multiples of the 128-row tiles, with both tensor-core paths
+(mma.sync and tcgen05, forward and backward); the two paths against each
+other on a graph with several tiles per block; and a short training run."""
 
 import numpy as np
 import pytest
@@ -93,3 +95,30 @@ def test_tcgen05_forward_matches_mma_sync(plfbs_lib):
     assert _rel(y1, y0) < 2e-3
     with pytest.raises(gnn.GnnError):
         net.set_tensor_cores(2)
+
+
+def test_tcgen05_gradients_match_mma_sync(plfbs_lib):
+    """Forward and backward on tcgen05 against the mma.sync kernels: the same
+    BF16 operands, FP32 sums in another order; every MLP's gradient block,
+    deterministic from run to run. Several 128-row tiles per block, so the
+    weight gradients accumulate in tensor memory over tiles."""
+    ma, src, dst, ef, x = _graph(24, 20, 18)
+    p = gnn.init_params(NF, EF, 3, OUT, seed=11, residual_scale=0.5)
+    net = gnn.GraphNet(src, dst, ef, ma.n_cells, NF, 3, OUT)
+    net.set_params(p)
+    t = _target(ma)
+    net.set_tensor_cores(0)
+    loss0, g0 = net.gradients(x, t)
+    net.set_tensor_cores(1)
+    loss1, g1 = net.gradients(x, t)
+    loss2, g2 = net.gradients(x, t)
+    net.close()
+    np.testing.assert_array_equal(g1, g2)
+    assert loss1 == loss2
+    assert abs(loss1 - loss0) / loss0 < 1e-3
+    assert _rel(g1, g0) < 5e-3
+    off = 0
+    for k, o in gnn.mlp_sizes(NF, EF, 3, OUT):
+        n = k * 64 + 64 + 64 * o + o
+        assert _rel(g1[off:off + n], g0[off:off + n]) < 2e-2, off
+        off += n
