@@ -409,38 +409,72 @@ __device__ __forceinline__ void stg8(float* p, const float* v) {
                : "memory");
 }
 
-// As load_x, into the canonical layout: each thread moves one 8-element
-// (16-byte) core-matrix row, consecutive threads taking consecutive rows, so
-// that a warp's stores fill four whole core matrices (no bank conflicts) and
-// each thread reads one full 32-byte sector.
+// As load_x, into the canonical layout. Thread t takes row t % 128 of the tile
+// and its 8-element (16-byte) chunks t / 128, t / 128 + 2, ...: a warp's stores
+// fill whole core matrices (no bank conflicts) and each thread reads whole
+// 32-byte sectors. The row's sources (its node rows for an edge MLP, its CSR
+// range for a node MLP) are read once, and the chunks are loaded four at a
+// time, so that a thread has four independent gathers in flight rather than
+// one (the kernels are bound by the latency of these gathers); a group of
+// four chunks covers one 64-column input segment.
 template <int MODE, int K1>
 __device__ __forceinline__ void load_x_canon(const Rows& a, int row0, unsigned char* As) {
-  constexpr int C8 = K1 / 8;
-  for (int q = threadIdx.x; q < TM * C8; q += kTcThreads) {
-    const int r = q % TM, k = 8 * (q / TM), m = row0 + r;
-    float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (m < a.M) {
-      if (MODE == NODE && k >= H) {
-        for (int e = a.in_off[m]; e < a.in_off[m + 1]; e++) {
-          float u[8];
-          ldg8(a.eagg + (size_t)a.in_idx[e] * H + (k - H), u);
+  constexpr int C8 = K1 / 8, NQ = TM * C8 / kTcThreads, G = NQ < 4 ? NQ : 4;
+  static_assert(kTcThreads == 2 * TM && (TM * C8) % kTcThreads == 0 && NQ % G == 0,
+                "chunks per thread");
+  const int r = threadIdx.x % TM, kc0 = threadIdx.x / TM, m = row0 + r;
+  const bool valid = m < a.M;
+  const float *p0 = nullptr, *p1 = nullptr, *p2 = nullptr;
+  int e0 = 0, e1 = 0;
+  if (valid) {
+    p0 = a.x0 + (size_t)m * (MODE == ENC ? FP : H);
+    if (MODE == EDGE) {
+      p1 = a.hs + (size_t)a.src[m] * H;
+      p2 = a.hs + (size_t)a.dst[m] * H;
+    }
+    if (MODE == NODE) {
+      e0 = a.in_off[m];
+      e1 = a.in_off[m + 1];
+    }
+  }
 #pragma unroll
-          for (int i = 0; i < 8; i++) v[i] += u[i];
-        }
-      } else {
-        const float* p;
-        if (MODE == ENC)
-          p = a.x0 + (size_t)m * FP + k;
-        else if (MODE == EDGE && k >= H)
-          p = a.hs + (size_t)(k < 2 * H ? a.src[m] : a.dst[m]) * H + (k & (H - 1));
-        else
-          p = a.x0 + (size_t)m * H + k;
-        ldg8(p, v);
+  for (int g0 = 0; g0 < NQ; g0 += G) {
+    float v[G][8];
+#pragma unroll
+    for (int i = 0; i < G; i++) {
+      const int c = kc0 + 2 * (g0 + i);  // this chunk: columns 8c .. 8c + 7
+#pragma unroll
+      for (int j = 0; j < 8; j++) v[i][j] = 0.f;
+      if (valid && !(MODE == NODE && c >= 8)) {
+        const int seg = MODE == ENC ? 0 : c / 8;
+        const float* p = seg == 0 ? p0 : (seg == 1 ? p1 : p2);
+        ldg8(p + (MODE == ENC ? 8 * c : 8 * (c % 8)), v[i]);
       }
     }
-    __nv_bfloat162 b[4] = {__floats2bfloat162_rn(v[0], v[1]), __floats2bfloat162_rn(v[2], v[3]),
-                           __floats2bfloat162_rn(v[4], v[5]), __floats2bfloat162_rn(v[6], v[7])};
-    *reinterpret_cast<uint4*>(As + canon_off(r, k, K1)) = *reinterpret_cast<const uint4*>(b);
+    if (MODE == NODE && kc0 + 2 * g0 >= 8) {
+      // the aggregate segment: the sum of the edge states over the incoming
+      // edges, in CSR order
+#pragma unroll 2
+      for (int e = e0; e < e1; e++) {
+        const float* pe = a.eagg + (size_t)a.in_idx[e] * H;
+#pragma unroll
+        for (int i = 0; i < G; i++) {
+          float u[8];
+          ldg8(pe + 8 * (kc0 + 2 * (g0 + i) - 8), u);
+#pragma unroll
+          for (int j = 0; j < 8; j++) v[i][j] += u[j];
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < G; i++) {
+      const int c = kc0 + 2 * (g0 + i);
+      __nv_bfloat162 b[4] = {
+          __floats2bfloat162_rn(v[i][0], v[i][1]), __floats2bfloat162_rn(v[i][2], v[i][3]),
+          __floats2bfloat162_rn(v[i][4], v[i][5]), __floats2bfloat162_rn(v[i][6], v[i][7])};
+      *reinterpret_cast<uint4*>(As + canon_off(r, 8 * c, K1)) =
+          *reinterpret_cast<const uint4*>(b);
+    }
   }
 }
 
@@ -808,15 +842,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_bwd_tc(const Bwd a, int* 
     // dY (plus the node aggregate's gradient at dst for an edge MLP) as BF16,
     // its column sums (db2) kept per thread: thread tid holds row tid % 128 of
     // the 8-column chunks tid / 128 + 2 j
+    const int rr = tid % TM, mm = row0 + rr;  // this thread's row of dY and Z1
+    const float* pd = (MODE == EDGE && a.dadd && mm < a.x.M)
+                          ? a.dadd + (size_t)a.x.dst[mm] * H : nullptr;
 #pragma unroll
     for (int j = 0; j < GB2 / 8; j++) {
-      const int q = tid + kTcThreads * j, rr = q % TM, k = 8 * (q / TM), mm = row0 + rr;
+      const int k = 8 * (tid / TM + 2 * j);
       float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       if (mm < a.x.M) {
         if (a.dy) ldg8(a.dy + (size_t)mm * NOUT + k, v);
-        if (MODE == EDGE && a.dadd) {
+        if (MODE == EDGE && pd) {
           float d[8];
-          ldg8(a.dadd + (size_t)a.x.dst[mm] * H + k, d);
+          ldg8(pd + k, d);
 #pragma unroll
           for (int i = 0; i < 8; i++) v[i] += d[i];
         }
@@ -827,8 +864,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_bwd_tc(const Bwd a, int* 
                              __floats2bfloat162_rn(v[4], v[5]), __floats2bfloat162_rn(v[6], v[7])};
       *reinterpret_cast<uint4*>(Ds + canon_off(rr, k, NOUT)) = *reinterpret_cast<const uint4*>(b);
     }
-    for (int q = tid; q < TM * (H / 8); q += kTcThreads) {
-      const int rr = q % TM, k = 8 * (q / TM), mm = row0 + rr;
+#pragma unroll
+    for (int j = 0; j < TM * (H / 8) / kTcThreads; j++) {
+      const int k = 8 * (tid / TM + 2 * j);
       float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       if (mm < a.x.M) ldg8(a.z1 + (size_t)mm * H + k, v);
       __nv_bfloat162 b[4] = {
