@@ -370,10 +370,10 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   ctx->cfg = *cfg;
   std::string err;
   int rc;
-  // With the device present, the mesh's face and cell arrays start on their
-  // way to it now and the host validates them meanwhile (from page-locked
-  // memory the copies run alongside); without it, the validation comes first
-  // as always and its errors are reported before the missing device.
+  // With the device present, the mesh's arrays start on their way to it now
+  // and are checked there (launch_mesh_scan: the host's checks, the same
+  // first failing index and message); without it, the host threads check
+  // them, and their errors are reported before the missing device.
   const bool have_device = check_device(device) == PLFBS_OK;
   auto drop = [&](int code, const std::string& m) {
     if (ctx->stream)
@@ -390,8 +390,16 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     if (stage_mesh(ctx, *mesh)) return drop(PLFBS_ERR_CUDA, ctx->err);
   }
   {
+    // the mesh checks on the device when the arrays are there (their copies
+    // end first), else on the host threads
+    plfbs::MeshScan scan{};
+    bool scanned = false;
+    if (have_device) {
+      NvtxRange r("mesh checks (device)");
+      if (scan_mesh(ctx, &scan, &scanned)) return drop(PLFBS_ERR_CUDA, ctx->err);
+    }
     NvtxRange r("prepare_layout (host)");
-    rc = plfbs::prepare_layout(*cfg, *mesh, *bc, ctx->L, err);
+    rc = plfbs::prepare_layout(*cfg, *mesh, *bc, ctx->L, err, scanned ? &scan : nullptr);
   }
   if (rc) return drop(rc, err);
   const Layout& L = ctx->L;

@@ -38,16 +38,22 @@ struct plfbs_ctx {
   int compact_faces = 0;          // unique face records in the compact layout (0: none)
   int compact_cells = 0;          // unique cell weight sets in the compact layout (0: none)
   bool flux_maps_ok = false;
-  // The caller's face and cell arrays, copied to the device at the start of
-  // plfbs_create while the host validates them (read only after it has):
-  // owner, neighbour [F] int; area, sdt [F], normal, fcen [3F], vol [C],
-  // ccen [3(C+B)] double. Freed once the layout is built.
+  // The caller's mesh arrays, copied to the device at the start of
+  // plfbs_create, checked there (launch_mesh_scan) and read by the layout
+  // only after the checks passed: owner, neighbour [F] int; area, sdt [F],
+  // normal, fcen [3F], vol [C], ccen [3(C+B)] double; the stencil offsets
+  // [C+1], cells and faces [nnz] int (with `stencil` set). Freed once the
+  // layout is built.
   struct MeshStage {
-    bool ok = false;
+    bool ok = false, stencil = false;
     const int32_t* owner = nullptr;
     const int32_t* neighbour = nullptr;
     const double *area = nullptr, *normal = nullptr, *fcen = nullptr, *sdt = nullptr,
                  *vol = nullptr, *ccen = nullptr;
+    const int32_t *st_off = nullptr, *st_cells = nullptr, *st_faces = nullptr;
+    long long nnz = 0;
+    int C = 0, F = 0, Fi = 0;
+    plfbs::MeshScan* scan = nullptr;  // device
     std::vector<void*> bufs;
   } stage;
   double timeout_s = 0;  // bound on plfbs_run's waits for its step batches (0: none)
@@ -85,10 +91,13 @@ int check_device(int device);
 // The face, stencil and gather arrays of a context on the device, and the
 // compact layout (capi_layout.cpp).
 int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m);
-// Starts the copies of the mesh's face and cell arrays (sizes from the view's
-// counts, checked positive first) into ctx->stage; returns without staging
-// when the counts or pointers are not usable (the layout then uploads them).
+// Starts the copies of the mesh's arrays (sizes from the view's counts,
+// checked positive first) into ctx->stage; returns without staging when the
+// counts or pointers are not usable (the layout then uploads them).
 int stage_mesh(plfbs_ctx* ctx, const plfbs_mesh_view& m);
+// The checks of validate_mesh on the staged arrays (false: nothing staged to
+// check, the host scans instead).
+int scan_mesh(plfbs_ctx* ctx, plfbs::MeshScan* out, bool* done);
 void free_stage(plfbs_ctx* ctx);
 int build_compact_layout(plfbs_ctx* ctx);
 

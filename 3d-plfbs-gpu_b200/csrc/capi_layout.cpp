@@ -83,7 +83,41 @@ int stage_mesh(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
   g.vol = static_cast<const double*>(q);
   TRY(up(m.cell_centroid, 24 * (size_t)T, &q));
   g.ccen = static_cast<const double*>(q);
+  g.C = (int)C;
+  g.F = (int)F;
+  g.Fi = (int)Fi;
   g.ok = true;
+  // the stencil, when its size reads sanely (else the host checks and the
+  // layout uploads it)
+  if (m.stencil_offsets && m.stencil_cells && m.stencil_faces && m.stencil_offsets[0] == 0 &&
+      m.stencil_offsets[C] >= 0) {
+    const long long nnz = m.stencil_offsets[C];
+    TRY(up(m.stencil_offsets, 4 * (size_t)(C + 1), &q));
+    g.st_off = static_cast<const int32_t*>(q);
+    TRY(up(m.stencil_cells, 4 * (size_t)nnz, &q));
+    g.st_cells = static_cast<const int32_t*>(q);
+    TRY(up(m.stencil_faces, 4 * (size_t)nnz, &q));
+    g.st_faces = static_cast<const int32_t*>(q);
+    void* p = nullptr;
+    CK(cudaMallocFromPoolAsync(&p, sizeof(plfbs::MeshScan), pool, ctx->stream));
+    g.bufs.push_back(p);
+    g.scan = static_cast<plfbs::MeshScan*>(p);
+    g.nnz = nnz;
+    g.stencil = true;
+  }
+  return PLFBS_OK;
+}
+
+int scan_mesh(plfbs_ctx* ctx, plfbs::MeshScan* out, bool* done) {
+  const auto& g = ctx->stage;
+  *done = false;
+  if (!g.ok || !g.stencil) return PLFBS_OK;
+  plfbs::launch_mesh_scan(g.owner, g.neighbour, g.area, g.sdt, g.normal, g.vol, g.st_off,
+                          g.st_cells, g.st_faces, g.C, g.F, g.Fi, g.nnz, g.scan, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, g.scan, sizeof *out, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *done = true;
   return PLFBS_OK;
 }
 
@@ -91,6 +125,7 @@ void free_stage(plfbs_ctx* ctx) {
   for (void* p : ctx->stage.bufs) cudaFreeAsync(p, ctx->stream);
   ctx->stage.bufs.clear();
   ctx->stage.ok = false;
+  ctx->stage.stencil = false;
 }
 
 // The face, stencil and gather arrays of a context, built on the device from
@@ -130,9 +165,15 @@ int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
     TRY(S.upload(&d.vol, m.cell_volume, C));
     TRY(S.upload(&d.ccen, m.cell_centroid, 3 * T));
   }
-  TRY(S.upload(&d.st_off, m.stencil_offsets, C + 1));
-  TRY(S.upload(&d.st_cells, m.stencil_cells, nnz));
-  TRY(S.upload(&d.st_faces, m.stencil_faces, nnz));
+  if (ctx->stage.ok && ctx->stage.stencil) {
+    d.st_off = ctx->stage.st_off;
+    d.st_cells = ctx->stage.st_cells;
+    d.st_faces = ctx->stage.st_faces;
+  } else {
+    TRY(S.upload(&d.st_off, m.stencil_offsets, C + 1));
+    TRY(S.upload(&d.st_cells, m.stencil_cells, nnz));
+    TRY(S.upload(&d.st_faces, m.stencil_faces, nnz));
+  }
   TRY(S.upload(&d.bc_new, L.bc_new_of_old.data(), B));
   TRY(S.upload(&d.bc_old, L.bc_old_of_new.data(), B));
   void* p = nullptr;

@@ -212,7 +212,24 @@ void boundary_records32(const Layout& L, double rho0, double uref, BoundaryRecor
 
 // The checks of a caller's mesh arrays that everything indexing with them
 // relies on (setup.cpp); *K_out (may be null) receives the largest stencil.
-int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out);
+// First failing index of each mesh check (the count where none fails) and the
+// largest stencil, found on the device by launch_mesh_scan; validate_mesh
+// takes them in place of its own scans.
+struct MeshScan {
+  int bad_face;     // face checks: owner / neighbour ranges, area, dt, normal
+  int bad_volume;   // cell volume positive and finite
+  int bad_offset;   // stencil_offsets[i + 1] < stencil_offsets[i]
+  int bad_stencil;  // a cell with a stencil entry out of range or not a face neighbour
+  int kmax;         // largest stencil
+};
+int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out,
+                  const MeshScan* scan = nullptr);
+// the checks of validate_mesh over the copies of the mesh arrays on the
+// device, into *out (device memory) on stream s
+void launch_mesh_scan(const int32_t* owner, const int32_t* nb, const double* area,
+                      const double* sdt, const double* normal, const double* vol,
+                      const int32_t* off, const int32_t* cells, const int32_t* faces, int C, int F,
+                      int Fi, long long nnz, MeshScan* out, cudaStream_t s);
 
 // Least-squares weights exactly as gradients::pre_fill_LHS_and_RHS_matrix
 // (gradients.cpp:214-313): lhs_inv [9C], rhs [3 nnz], caller numbering. The
@@ -232,7 +249,7 @@ std::vector<int32_t> cell_order(int C, int Fi, const int32_t* owner, const int32
 // their records (setup.cpp). For renumber 2 it stops after the validation:
 // the caller builds the order on the device and calls order_layout.
 int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bc,
-                   Layout& L, std::string& err);
+                   Layout& L, std::string& err, const MeshScan* scan = nullptr);
 
 // The order-dependent part of prepare_layout for a given cell order (a
 // permutation of the cells): boundary face order and records.

@@ -265,7 +265,7 @@ std::vector<int32_t> cell_order(int C, int Fi, const int32_t* owner, const int32
 // cell volumes, stencil offsets and entries. Everything that indexes with the
 // caller's indices (the layout, the least-squares export) runs after them.
 // *K_out receives the largest stencil.
-int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out) {
+int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out, const MeshScan* scan) {
   const int C = m.n_cells, F = m.n_faces, Fi = m.n_internal;
   if (C <= 0 || F <= 0 || Fi < 0 || Fi > F) {
     err = "mesh sizes must satisfy n_cells > 0, n_faces > 0, 0 <= n_internal <= n_faces";
@@ -297,7 +297,7 @@ int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out) {
       return 4;
     return 0;
   };
-  const int bf = first_bad(F, [&](int f) { return face_problem(f) != 0; });
+  const int bf = scan ? scan->bad_face : first_bad(F, [&](int f) { return face_problem(f) != 0; });
   if (bf < F) {
     static const char* what[5] = {"", "face owner out of range",
                                   "internal face neighbour out of range",
@@ -307,7 +307,9 @@ int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out) {
     err = msg(what[code], bf, code == 1 ? m.owner[bf] : code == 4 ? 0 : m.neighbour[bf]);
     return PLFBS_ERR_MESH;
   }
-  const int bv = first_bad(C, [&](int i) { return !(m.cell_volume[i] > 0) || !finite(m.cell_volume[i]); });
+  const int bv = scan ? scan->bad_volume : first_bad(C, [&](int i) {
+    return !(m.cell_volume[i] > 0) || !finite(m.cell_volume[i]);
+  });
   if (bv < C) {
     err = msg("cell volume not positive", bv, 0);
     return PLFBS_ERR_MESH;
@@ -316,7 +318,9 @@ int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out) {
     err = "stencil_offsets[0] must be 0";
     return PLFBS_ERR_MESH;
   }
-  const int bo = first_bad(C, [&](int i) { return m.stencil_offsets[i + 1] < m.stencil_offsets[i]; });
+  const int bo = scan ? scan->bad_offset : first_bad(C, [&](int i) {
+    return m.stencil_offsets[i + 1] < m.stencil_offsets[i];
+  });
   if (bo < C) {
     err = msg("stencil offsets decrease", bo, m.stencil_offsets[bo + 1]);
     return PLFBS_ERR_MESH;
@@ -331,7 +335,7 @@ int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out) {
                     (f < Fi && m.neighbour[f] == i && m.owner[f] == j);
     return ok ? 0 : 2;
   };
-  const int bs = first_bad(C, [&](int i) {
+  const int bs = scan ? scan->bad_stencil : first_bad(C, [&](int i) {
     for (int e = m.stencil_offsets[i]; e < m.stencil_offsets[i + 1]; e++)
       if (entry_problem(e, i)) return true;
     return false;
@@ -346,13 +350,14 @@ int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out) {
       }
     }
   }
-  std::atomic<int> Kmax(0);
-  parallel_for(C, [&](int i) {
-    const int k = m.stencil_offsets[i + 1] - m.stencil_offsets[i];
-    int cur = Kmax.load(std::memory_order_relaxed);
-    while (k > cur && !Kmax.compare_exchange_weak(cur, k, std::memory_order_relaxed)) {
-    }
-  });
+  std::atomic<int> Kmax(scan ? scan->kmax : 0);
+  if (!scan)
+    parallel_for(C, [&](int i) {
+      const int k = m.stencil_offsets[i + 1] - m.stencil_offsets[i];
+      int cur = Kmax.load(std::memory_order_relaxed);
+      while (k > cur && !Kmax.compare_exchange_weak(cur, k, std::memory_order_relaxed)) {
+      }
+    });
   const int K = Kmax.load();
   if (K == 0) {
     err = "empty gradient stencil";
@@ -363,9 +368,9 @@ int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out) {
 }
 
 int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bcv,
-                   Layout& L, std::string& err) {
+                   Layout& L, std::string& err, const MeshScan* scan) {
   int K = 0;
-  const int vrc = validate_mesh(m, err, &K);
+  const int vrc = validate_mesh(m, err, &K, scan);
   if (vrc) return vrc;
   const int C = m.n_cells, F = m.n_faces, Fi = m.n_internal, B = F - Fi;
   if (B > 0 && (!bcv.rho_type || !bcv.vel_type || !bcv.value)) {
