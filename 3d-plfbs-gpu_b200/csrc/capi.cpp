@@ -390,16 +390,34 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     if (stage_mesh(ctx, *mesh)) return drop(PLFBS_ERR_CUDA, ctx->err);
   }
   {
-    // the mesh checks on the device when the arrays are there (their copies
-    // end first), else on the host threads
-    plfbs::MeshScan scan{};
+    // The mesh checks on the device when the arrays are there, their results
+    // copied to page-locked memory (the stats buffer, not in use yet); the
+    // host's part of the layout runs while the copies and checks proceed
+    // (prepare_layout's wait_scan path), else the host threads check.
     bool scanned = false;
+    plfbs::MeshScan* scan = nullptr;
     if (have_device) {
       NvtxRange r("mesh checks (device)");
-      if (scan_mesh(ctx, &scan, &scanned)) return drop(PLFBS_ERR_CUDA, ctx->err);
+      if (!(ctx->stats_host = take_pinned_stats()))
+        return drop(PLFBS_ERR_CUDA, "cudaMallocHost failed");
+      static_assert(sizeof(plfbs::MeshScan) <= sizeof(DevStats), "scan results fit");
+      scan = reinterpret_cast<plfbs::MeshScan*>(ctx->stats_host);
+      if (scan_mesh(ctx, scan, &scanned)) return drop(PLFBS_ERR_CUDA, ctx->err);
     }
     NvtxRange r("prepare_layout (host)");
-    rc = plfbs::prepare_layout(*cfg, *mesh, *bc, ctx->L, err, scanned ? &scan : nullptr);
+    if (scanned && cfg->renumber != 1) {
+      rc = plfbs::prepare_layout(*cfg, *mesh, *bc, ctx->L, err, nullptr,
+                                 [&](plfbs::MeshScan& out) -> int {
+                                   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+                                     return PLFBS_ERR_CUDA;
+                                   out = *scan;
+                                   return PLFBS_OK;
+                                 });
+    } else {
+      if (scanned && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return drop(PLFBS_ERR_CUDA, "the device mesh checks failed");
+      rc = plfbs::prepare_layout(*cfg, *mesh, *bc, ctx->L, err, scanned ? scan : nullptr);
+    }
   }
   if (rc) return drop(rc, err);
   const Layout& L = ctx->L;
@@ -427,7 +445,7 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   };
   if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
     return fail(set_err(ctx, PLFBS_ERR_CUDA, "event creation failed"));
-  if (!(ctx->stats_host = take_pinned_stats()))
+  if (!ctx->stats_host && !(ctx->stats_host = take_pinned_stats()))
     return fail(set_err(ctx, PLFBS_ERR_CUDA, "cudaMallocHost failed"));
   if (cfg->renumber == 2) {  // the order on the device, then the host's order-dependent part
     NvtxRange r("device cell order");
@@ -499,13 +517,6 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   {
     NvtxRange r("compact layout");
     if ((rc = build_compact_layout(ctx))) return fail(rc);
-  }
-  {  // caller index -> device index, cells then ghosts (state transfer)
-    std::vector<int32_t> perm((size_t)T);
-    for (long long o = 0; o < L.C; o++) perm[o] = L.cell_new_of_old[o];
-    for (long long b = 0; b < L.B; b++) perm[L.C + b] = L.C + L.bc_new_of_old[b];
-    if ((rc = dev_upload(ctx, &p, perm))) return fail(rc);
-    ctx->perm = static_cast<int32_t*>(p);
   }
   if (fp32) {
     plfbs::BoundaryRecords32 b32;

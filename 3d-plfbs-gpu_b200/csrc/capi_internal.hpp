@@ -95,9 +95,11 @@ int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m);
 // checked positive first) into ctx->stage; returns without staging when the
 // counts or pointers are not usable (the layout then uploads them).
 int stage_mesh(plfbs_ctx* ctx, const plfbs_mesh_view& m);
-// The checks of validate_mesh on the staged arrays (false: nothing staged to
-// check, the host scans instead).
-int scan_mesh(plfbs_ctx* ctx, plfbs::MeshScan* out, bool* done);
+// Launches the checks of validate_mesh on the staged arrays and the copy of
+// their results into *out (page-locked host memory; valid once the stream
+// has reached it). *launched false: nothing staged to check, the host scans
+// instead.
+int scan_mesh(plfbs_ctx* ctx, plfbs::MeshScan* out, bool* launched);
 void free_stage(plfbs_ctx* ctx);
 int build_compact_layout(plfbs_ctx* ctx);
 

@@ -108,16 +108,15 @@ int stage_mesh(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
   return PLFBS_OK;
 }
 
-int scan_mesh(plfbs_ctx* ctx, plfbs::MeshScan* out, bool* done) {
+int scan_mesh(plfbs_ctx* ctx, plfbs::MeshScan* out, bool* launched) {
   const auto& g = ctx->stage;
-  *done = false;
+  *launched = false;
   if (!g.ok || !g.stencil) return PLFBS_OK;
   plfbs::launch_mesh_scan(g.owner, g.neighbour, g.area, g.sdt, g.normal, g.vol, g.st_off,
                           g.st_cells, g.st_faces, g.C, g.F, g.Fi, g.nnz, g.scan, ctx->stream);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, g.scan, sizeof *out, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  *done = true;
+  *launched = true;
   return PLFBS_OK;
 }
 
@@ -179,6 +178,11 @@ int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
   void* p = nullptr;
   TRY(dev_upload(ctx, &p, L.cell_new_of_old));  // kept: the IBM kernels map caller cells with it
   d.cell_new = static_cast<const int32_t*>(p);
+  // caller index -> device index, cells then ghosts (state transfer)
+  TRY(pool_alloc(ctx, &p, 4 * T));
+  ctx->perm = static_cast<int32_t*>(p);
+  plfbs::launch_perm(d.cell_new, d.bc_new, L.C, L.B, ctx->perm, ctx->stream);
+  CK(cudaGetLastError());
   plfbs::LayoutScratch s{};
   TRY(S.alloc(&s.own_cnt, 4 * C, true));
   TRY(S.alloc(&s.own_off, 4 * C, false));

@@ -7,6 +7,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -248,8 +249,12 @@ std::vector<int32_t> cell_order(int C, int Fi, const int32_t* owner, const int32
 // Validate the views, renumber the cells, order the boundary faces and build
 // their records (setup.cpp). For renumber 2 it stops after the validation:
 // the caller builds the order on the device and calls order_layout.
+// With `scan`, the mesh checks' results found on the device; with
+// `wait_scan` (renumber 0 and 2), they are still being found: the host work
+// that is safe on unchecked arrays runs first, then wait_scan blocks for them.
 int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bc,
-                   Layout& L, std::string& err, const MeshScan* scan = nullptr);
+                   Layout& L, std::string& err, const MeshScan* scan = nullptr,
+                   const std::function<int(MeshScan&)>& wait_scan = nullptr);
 
 // The order-dependent part of prepare_layout for a given cell order (a
 // permutation of the cells): boundary face order and records.
@@ -385,6 +390,9 @@ void launch_state_out(const int32_t* perm, long long T, const void* state, int p
                       cudaStream_t stream);
 void launch_records(const int32_t* perm, long long n, int rec_bytes, const void* src, void* dst,
                     bool to_caller, cudaStream_t stream);
+// perm[C + B]: the device index of each caller cell (cell_new) and ghost (C + bc_new)
+void launch_perm(const int32_t* cell_new, const int32_t* bc_new, int C, int B, int32_t* perm,
+                 cudaStream_t stream);
 // p[0, n) = value
 void launch_fill(double* p, long long n, double value, cudaStream_t stream);
 void launch_fill(float* p, long long n, float value, cudaStream_t stream);

@@ -2,6 +2,7 @@
 // renumbering, boundary order and records, and the host-only least-squares
 // weights export. The O(faces) layout is built on the device (layout.cu).
 #include <algorithm>
+#include <functional>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -108,6 +109,41 @@ void parallel_for(int n, const Body& body, int serial_below = 32768) {
   }
   for (int i = lo; i < n; i++) body(i);
   for (auto& t : th) t.join();
+}
+
+// Sorts distinct keys: chunks sorted on the host threads, then merged
+// pairwise (in parallel within a round); std::sort below 64 K keys.
+void parallel_sort(std::vector<uint64_t>& v) {
+  const size_t n = v.size();
+  const unsigned hw = std::thread::hardware_concurrency();
+  const size_t nt = std::min<size_t>(16, hw ? hw : 1);
+  if (nt <= 1 || n < 65536) {
+    std::sort(v.begin(), v.end());
+    return;
+  }
+  std::vector<size_t> cut(nt + 1);
+  for (size_t k = 0; k <= nt; k++) cut[k] = n * k / nt;
+  {
+    std::vector<std::thread> th;
+    for (size_t k = 0; k < nt; k++)
+      th.emplace_back([&, k] { std::sort(v.begin() + cut[k], v.begin() + cut[k + 1]); });
+    for (auto& t : th) t.join();
+  }
+  std::vector<uint64_t> tmp(n);
+  std::vector<uint64_t>*src = &v, *dst = &tmp;
+  for (size_t width = 1; width < nt; width *= 2) {
+    std::vector<std::thread> th;
+    for (size_t k = 0; k < nt; k += 2 * width) {
+      const size_t a = cut[k], m = cut[std::min(nt, k + width)], b = cut[std::min(nt, k + 2 * width)];
+      th.emplace_back([=] {
+        std::merge(src->begin() + a, src->begin() + m, src->begin() + m, src->begin() + b,
+                   dst->begin() + a);
+      });
+    }
+    for (auto& t : th) t.join();
+    std::swap(src, dst);
+  }
+  if (src != &v) v.swap(tmp);
 }
 
 }  // namespace
@@ -367,21 +403,12 @@ int validate_mesh(const plfbs_mesh_view& m, std::string& err, int* K_out, const 
   return PLFBS_OK;
 }
 
-int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bcv,
-                   Layout& L, std::string& err, const MeshScan* scan) {
-  int K = 0;
-  const int vrc = validate_mesh(m, err, &K, scan);
-  if (vrc) return vrc;
-  const int C = m.n_cells, F = m.n_faces, Fi = m.n_internal, B = F - Fi;
+// The boundary arrays: present, and types the flavour defines, finite values.
+static int check_bcs(const plfbs_config& cfg, const plfbs_bc_view& bcv, int B, std::string& err) {
   if (B > 0 && (!bcv.rho_type || !bcv.vel_type || !bcv.value)) {
     err = "null boundary array";
     return PLFBS_ERR_ARG;
   }
-  L.C = C;
-  L.F = F;
-  L.Fi = Fi;
-  L.B = B;
-  L.K = K;
   const bool cpu = cfg.flavour == PLFBS_FLAVOUR_CPU_SOLVER;
   for (int b = 0; b < B; b++) {
     const int rt = bcv.rho_type[b], vt = bcv.vel_type[b];
@@ -405,6 +432,52 @@ int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfb
         return PLFBS_ERR_BC;
       }
   }
+  return PLFBS_OK;
+}
+
+int prepare_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_bc_view& bcv,
+                   Layout& L, std::string& err, const MeshScan* scan,
+                   const std::function<int(MeshScan&)>& wait_scan) {
+  const int C = m.n_cells, F = m.n_faces, Fi = m.n_internal, B = F - Fi;
+  if (wait_scan && cfg.renumber != 1) {
+    // The mesh checks run on the device meanwhile (the caller has checked the
+    // sizes and pointers). The boundary checks, the identity order and the
+    // boundary order and records (which guard the owners they index with)
+    // go first; the errors come out in the order of the path below: the
+    // mesh's, then the boundary arrays', then the order's.
+    L.C = C;
+    L.F = F;
+    L.Fi = Fi;
+    L.B = B;
+    std::string berr, oerr;
+    const int brc = check_bcs(cfg, bcv, B, berr);
+    int orc = PLFBS_OK;
+    if (!brc && cfg.renumber == 0)
+      orc = order_layout(cfg, m, bcv, cell_order(C, Fi, m.owner, m.neighbour, 0), L, oerr);
+    MeshScan s{};
+    if (const int wrc = wait_scan(s)) {
+      err = "the device mesh checks failed";
+      return wrc;
+    }
+    int K = 0;
+    if (const int vrc = validate_mesh(m, err, &K, &s)) return vrc;
+    L.K = K;
+    if (brc) {
+      err = berr;
+      return brc;
+    }
+    if (orc) err = oerr;
+    return orc;
+  }
+  int K = 0;
+  const int vrc = validate_mesh(m, err, &K, scan);
+  if (vrc) return vrc;
+  L.C = C;
+  L.F = F;
+  L.Fi = Fi;
+  L.B = B;
+  L.K = K;
+  if (const int brc = check_bcs(cfg, bcv, B, err)) return brc;
 
   // --- renumbering ---------------------------------------------------------
   // renumber 2: the device builds the order, then plfbs_create calls
@@ -424,11 +497,15 @@ int order_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
   // Boundary faces by new owner, ties in face order (a stable sort by owner):
   // one sort of packed (new owner, boundary index) keys. The internal faces
   // are ordered on the device (layout.cu).
+  // An owner out of range (arrays not checked yet: see prepare_layout) sorts
+  // last; the checks then report it and this order is dropped.
   std::vector<uint64_t> key(B);
   parallel_for(B, [&](int b) {
-    key[b] = (uint64_t)(uint32_t)L.cell_new_of_old[m.owner[Fi + b]] << 32 | (uint32_t)b;
+    const int o = m.owner[Fi + b];
+    const uint32_t no = (o >= 0 && o < C) ? (uint32_t)L.cell_new_of_old[o] : 0xffffffffu;
+    key[b] = (uint64_t)no << 32 | (uint32_t)b;
   });
-  std::sort(key.begin(), key.end());
+  parallel_sort(key);
   L.bc_old_of_new.resize(B);
   L.bc_new_of_old.resize(B);
   parallel_for(B, [&](int b) {
@@ -449,7 +526,7 @@ int order_layout(const plfbs_config& cfg, const plfbs_mesh_view& m, const plfbs_
   const int bad = first_bad(B, [&](int bn) {
     const int bo = L.bc_old_of_new[bn];
     const int f = Fi + bo;
-    const int own = m.owner[f];
+    const int own = std::min(std::max(m.owner[f], 0), C - 1);  // in range once checked
     const double* val = bcv.value + 4 * (size_t)bo;
     const double* cg = m.cell_centroid + 3 * ((size_t)C + bo);
     const double* cn = m.cell_centroid + 3 * (size_t)own;

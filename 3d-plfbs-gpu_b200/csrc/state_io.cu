@@ -128,6 +128,21 @@ __global__ void __launch_bounds__(kIoBlock) k_fill(T* __restrict__ p, long long 
 
 }  // namespace
 
+// perm[o] = device index of caller cell o (o < C) and of caller ghost C + b
+__global__ void __launch_bounds__(kIoBlock)
+    k_perm(const int32_t* __restrict__ cell_new, const int32_t* __restrict__ bc_new, int C,
+           long long T, int32_t* __restrict__ perm) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T) return;
+  perm[i] = i < C ? cell_new[i] : C + bc_new[i - C];
+}
+
+void launch_perm(const int32_t* cell_new, const int32_t* bc_new, int C, int B, int32_t* perm,
+                 cudaStream_t s) {
+  const long long T = (long long)C + B;
+  if (T > 0) k_perm<<<(unsigned)((T + kIoBlock - 1) / kIoBlock), kIoBlock, 0, s>>>(cell_new, bc_new, C, T, perm);
+}
+
 void launch_fill(double* p, long long n, double value, cudaStream_t s) {
   if (n > 0) k_fill<double><<<io_blocks(n), kIoBlock, 0, s>>>(p, n, value);
 }
