@@ -6,7 +6,8 @@
   * the 128 x 64 x 64 sphere channel (3,217 IBM nodes), 20 steps from the
     bench's uniform start, against the reference's own CUDA path run here
     (oracle/_ref/plfbs_ref_gpu) and against the C oracle;
-  * the 256 x 128 x 128 channel (12,869 nodes), 2 steps against the C oracle.
+  * the 256 x 128 x 128 channel (12,869 nodes), 2 steps against the C oracle
+    and 200 steps against the reference's own CUDA path.
 
 Bar: relative L2 <= 1e-10 per field (the reference itself is defined only up
 to the order of its FP64 atomic additions); residual histories to 1e-10.
@@ -128,6 +129,24 @@ def test_scale_channel_2_steps_against_oracle(plfbs_lib):
         assert rel_l2(got[:, k], o.state[:, k]) < RUN_TOL, k
     assert rel_err(hist, o.history) < 1e-10
     assert rel_err(x, o.node_x) < 1e-12
+
+
+def test_scale_channel_200_steps_against_reference_cuda(plfbs_lib, tmp_path):
+    """The headline 256 x 128 x 128 channel with its 12,869-node sphere, 200
+    steps from the bench's uniform start, against the reference's own CUDA
+    path run here on the same polyMesh: every field to 1e-10 relative L2."""
+    if not os.path.exists(BIN_GPU):
+        pytest.skip("oracle/_ref/plfbs_ref_gpu not built (needs the reference sources)")
+    w, steps = bench.SCALE, 200
+    pm, c, ma, nodes, state0, bcs = _channel(w)
+    got, hist, x = _run_ours(w, c, ma, nodes, state0, bcs, steps, renumber=0)
+    assert np.abs(got[: ma.n_cells, 1:3]).max() > 1e-4  # the sphere has deflected the flow
+    c.steps = steps
+    dumps = refrun.run_reference(str(tmp_path), pm, c, nodes=nodes, init_state=state0,
+                                 binary=BIN_GPU, timeout=1500)
+    ref = dumps["ref_gpu_final_state"]
+    for k in range(4):
+        assert rel_l2(got[:, k], ref[:, k]) < RUN_TOL, k
 
 
 def test_sphere_channel_20000_steps_against_reference_cuda(plfbs_lib, tmp_path):

@@ -2,9 +2,9 @@
 over the plain method, on members of its family it was not trained on: the
 first six held-out cases of plfbs/data/warmstart_results.json, taken in order.
 The start field's error against the converged field (held-out case 1, Re
-137.4: measured 0.062), and the steps the FP32 solver needs to bring the
+137.4: measured 0.053), and the steps the FP32 solver needs to bring the
 residual below 1e-5 from the network's start versus from uniform flow
-(measured over the six: 80,112 vs 87,199, fewer in each). The evaluation over
+(measured over the six: 66,964 vs 87,199, fewer in each). The evaluation over
 all 20 held-out cases down to 1e-6 is in the same file."""
 
 import json
