@@ -43,6 +43,8 @@ CORRUPT = [
     ("owner", 40, 10 ** 6),
     ("neighbour", 3, "ghost"),              # internal face pointing at a ghost
     ("neighbour", "boundary", 0),           # boundary face not n_cells + face - n_internal
+    ("owner", "boundary", -1),              # a boundary face's owner out of range: the host's
+    ("owner", "boundary", 10 ** 6),         # boundary order meanwhile guards its indexing
     ("face_area", 17, 0.0),                 # area not positive
     ("face_area", 2, np.nan),
     ("streaming_dt", 9, -0.5),
