@@ -203,7 +203,11 @@ int plfbs_polymesh_geometry(const plfbs_polymesh_view* mesh, double visc, double
 /* Replaces the setup half of Solver_gpu.cu:150-662: validates the views,
  * builds the least-squares weights (gradients.cpp:214-313), renumbers for
  * locality, uploads everything to `device` and captures one time step in a
- * CUDA graph. The initial state is all zeros until plfbs_set_state. */
+ * CUDA graph. The mesh arrays are copied to the device first and checked
+ * there (the same checks, first failing index and message as on the host
+ * threads, which check them when `device` is absent); from page-locked host
+ * memory the copies set the pace. The initial state is all zeros until
+ * plfbs_set_state. */
 int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh,
                  const plfbs_bc_view* bc, const plfbs_ibm_view* ibm, int device,
                  plfbs_ctx** out);
