@@ -123,24 +123,38 @@ void parallel_sort(std::vector<uint64_t>& v) {
   }
   std::vector<size_t> cut(nt + 1);
   for (size_t k = 0; k <= nt; k++) cut[k] = n * k / nt;
-  {
+  // a job per thread where a thread can be started, else on this one
+  auto run_all = [](std::vector<std::function<void()>>& jobs) {
     std::vector<std::thread> th;
-    for (size_t k = 0; k < nt; k++)
-      th.emplace_back([&, k] { std::sort(v.begin() + cut[k], v.begin() + cut[k + 1]); });
+    size_t k = 0;
+    for (; k < jobs.size(); k++) {
+      try {
+        th.emplace_back(jobs[k]);
+      } catch (...) {
+        break;
+      }
+    }
+    for (; k < jobs.size(); k++) jobs[k]();
     for (auto& t : th) t.join();
+  };
+  {
+    std::vector<std::function<void()>> jobs;
+    for (size_t k = 0; k < nt; k++)
+      jobs.emplace_back([&, k] { std::sort(v.begin() + cut[k], v.begin() + cut[k + 1]); });
+    run_all(jobs);
   }
   std::vector<uint64_t> tmp(n);
   std::vector<uint64_t>*src = &v, *dst = &tmp;
   for (size_t width = 1; width < nt; width *= 2) {
-    std::vector<std::thread> th;
+    std::vector<std::function<void()>> jobs;
     for (size_t k = 0; k < nt; k += 2 * width) {
       const size_t a = cut[k], m = cut[std::min(nt, k + width)], b = cut[std::min(nt, k + 2 * width)];
-      th.emplace_back([=] {
+      jobs.emplace_back([=] {
         std::merge(src->begin() + a, src->begin() + m, src->begin() + m, src->begin() + b,
                    dst->begin() + a);
       });
     }
-    for (auto& t : th) t.join();
+    run_all(jobs);
     std::swap(src, dst);
   }
   if (src != &v) v.swap(tmp);
