@@ -5,6 +5,8 @@
 // Every array is a heap block of exactly the size the C ABI promises, so any
 // access past what the caller handed over ends the run with a sanitizer
 // report. Prints one line per case: the status of each call.
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <fstream>
 #include <string>
@@ -13,6 +15,44 @@
 #include "plfbs_internal.hpp"
 
 namespace {
+
+// The device mesh checks' results (csrc/mesh_scan.cu) computed here: the
+// smallest failing index of each check, the largest stencil.
+plfbs::MeshScan host_scan(const plfbs_mesh_view& m) {
+  const int C = m.n_cells, F = m.n_faces, Fi = m.n_internal;
+  const long long T = (long long)C + (F - Fi), nnz = m.stencil_offsets[C];
+  plfbs::MeshScan s{F, C, C, C, 0};
+  auto pf = [](double x) { return x > 0.0 && std::isfinite(x); };
+  for (int f = 0; f < F && s.bad_face == F; f++) {
+    const int o = m.owner[f], n = m.neighbour[f];
+    bool bad = o < 0 || o >= C;
+    bad = bad || (f < Fi ? (n < 0 || n >= C || n == o) : n != C + (f - Fi));
+    bad = bad || !pf(m.face_area[f]) || !(m.streaming_dt[f] > 0.0);
+    for (int c = 0; c < 3; c++) bad = bad || !std::isfinite(m.face_normal[3 * (size_t)f + c]);
+    if (bad) s.bad_face = f;
+  }
+  for (int i = 0; i < C; i++) {
+    if (s.bad_volume == C && !pf(m.cell_volume[i])) s.bad_volume = i;
+    const int k = m.stencil_offsets[i + 1] - m.stencil_offsets[i];
+    if (s.bad_offset == C && k < 0) s.bad_offset = i;
+    s.kmax = std::max(s.kmax, k);
+  }
+  for (int i = 0; i < C && s.bad_stencil == C; i++) {
+    const int e0 = m.stencil_offsets[i], e1 = m.stencil_offsets[i + 1];
+    if (e0 < 0 || e1 < e0 || e1 > nnz) continue;
+    for (int e = e0; e < e1; e++) {
+      const int j = m.stencil_cells[e], f = m.stencil_faces[e];
+      const bool bad = j < 0 || j >= T || f < 0 || f >= F ||
+                       !((m.owner[f] == i && m.neighbour[f] == j) ||
+                         (f < Fi && m.neighbour[f] == i && m.owner[f] == j));
+      if (bad) {
+        s.bad_stencil = i;
+        break;
+      }
+    }
+  }
+  return s;
+}
 
 template <typename T>
 std::vector<T> load(const std::string& dir, const char* name, size_t n) {
@@ -79,6 +119,23 @@ int main(int argc, char** argv) {
         plfbs::Layout L;
         std::string err;
         int rc = plfbs::prepare_layout(cfg, m, b, L, err);
+        if (renumber != 1) {
+          // the path plfbs_create takes when the device checks the mesh: the
+          // host's share first on unchecked arrays, then the checks' results
+          plfbs::Layout L2;
+          std::string err2;
+          const int rc2 = plfbs::prepare_layout(cfg, m, b, L2, err2, nullptr,
+                                                [&](plfbs::MeshScan& out) {
+                                                  out = host_scan(m);
+                                                  return PLFBS_OK;
+                                                });
+          bool same = rc2 == rc && err2 == err;
+          if (same && rc == PLFBS_OK && renumber == 0)
+            same = L2.bc_old_of_new == L.bc_old_of_new && L2.bc0 == L.bc0 && L2.bc1 == L.bc1 &&
+                   L2.bc2 == L.bc2 && L2.bc3 == L.bc3 && L2.quirk_b == L.quirk_b &&
+                   L2.K == L.K && L2.cell_new_of_old == L.cell_new_of_old;
+          std::printf(" deferred%d%d=%d", flavour, renumber, same ? 1 : 0);
+        }
         if (rc == PLFBS_OK && renumber == 2)  // the device order is the host RCM
           rc = plfbs::order_layout(cfg, m, b, plfbs::cell_order(m.n_cells, m.n_internal,
                                                                 m.owner, m.neighbour, 1),

@@ -1,9 +1,13 @@
 """The library's host-side setup (csrc/setup.cpp) under AddressSanitizer
 (tests/asan_setup_check.cpp): the layout's checks, the cell orders, the
 boundary records and the least-squares export on valid meshes (one large
-enough for the multi-threaded checks) and on corrupt ones of every kind the
-checks reject. The arrays are exactly the sizes the C ABI promises, so any
-access beyond what a caller hands over ends the run with a report."""
+enough for the multi-threaded checks, one with enough boundary faces for the
+multi-threaded key sort) and on corrupt ones of every kind the checks reject.
+The path plfbs_create takes with a device (the host's share of the layout on
+unchecked arrays, then the checks' results) must give the same status,
+message and boundary records as the checks-first path. The arrays are exactly
+the sizes the C ABI promises, so any access beyond what a caller hands over
+ends the run with a report."""
 
 import copy
 import os
@@ -92,6 +96,10 @@ def _corrupt(ma, rt, vt, val, kind):
         arr("face_area")[0] = np.nan
     elif kind == "bc_type":
         rt[0] = 5
+    elif kind == "owner_boundary_low":  # the deferred boundary order guards these
+        arr("owner")[Fi + 3] = -5
+    elif kind == "owner_boundary_high":
+        arr("owner")[Fi + 3] = C + 1000
     return ma, rt, vt, val
 
 
@@ -111,6 +119,11 @@ def test_setup_is_memory_clean_on_valid_and_corrupt_meshes(checker, tmp_path):
     runs["box"] = (box, *cases.bc_arrays(box, c))
     tets = cases.mesh_arrays(cases.jittered_tet_box(4, jitter=0.2, seed=3), 0.01, 1.0, 0.0)
     runs["tets"] = (tets, *cases.bc_arrays(tets, c))
+    slab = cases.mesh_arrays(cases.uniform_box(256, 256, 2), 0.01, 1.0, 0.0)
+    assert slab.n_faces - slab.n_internal > 65536  # the boundary keys sort on several threads
+    runs["slab"] = (slab, *cases.bc_arrays(slab, c))
+    for kind in ("owner_boundary_low", "owner_boundary_high"):
+        runs[kind] = _corrupt(ma0, rt0, vt0, val0, kind)
     for kind in KINDS + ("bc_type",):
         runs[kind] = _corrupt(ma0, rt0, vt0, val0, kind)
     dirs = []
@@ -125,12 +138,16 @@ def test_setup_is_memory_clean_on_valid_and_corrupt_meshes(checker, tmp_path):
         name, *kv = line.split()
         got[os.path.basename(name)] = {k: int(v) for k, v in (x.split("=") for x in kv)}
     assert set(got) == set(runs)
-    for name in ("cavity", "box"):  # hexes: every call succeeds
-        assert all(v == capi.OK for v in got[name].values()), (name, got[name])
+    for name in ("cavity", "box", "slab"):  # hexes: every call succeeds
+        assert all(v == capi.OK for k, v in got[name].items() if not k.startswith("deferred")), (
+            name, got[name])
     assert all(v == capi.OK for k, v in got["tets"].items() if k.startswith("layout"))
-    for kind in KINDS:  # rejected by the checks, by every call
-        assert all(v in (capi.ERR_ARG, capi.ERR_MESH) for v in got[kind].values()), (kind,
-                                                                                   got[kind])
+    for kind in KINDS + ("owner_boundary_low", "owner_boundary_high"):  # rejected by every call
+        assert all(v in (capi.ERR_ARG, capi.ERR_MESH) for k, v in got[kind].items()
+                   if not k.startswith("deferred")), (kind, got[kind])
+    for name, g in got.items():  # the deferred path: the same status, message and records
+        assert all(v == 1 for k, v in g.items() if k.startswith("deferred")), (name, g)
+        assert sum(k.startswith("deferred") for k in g) == 4, (name, g)
     bc = got["bc_type"]  # a boundary type neither flavour takes: the layout only
     assert all(bc[k] == capi.ERR_BC for k in bc if k.startswith("layout"))
     assert all(bc[k] == capi.OK for k in bc if k.startswith("ls"))
