@@ -96,3 +96,36 @@ def test_fp32_cavity_32cubed(plfbs_lib):
     errs = _field_errors(s.get_state(), o.state)
     print("fp32 vs fp64, 32^3 cavity, 50 steps:", errs)
     assert max(errs.values()) < RUN_TOL, errs
+
+
+# thousands of steps with IBM, relative L2 per field (measured on the B200 at
+# 2,000 steps: u 9.1e-7, v and w 1.1e-5, rho - rho0 8.7e-5; Cd 2.0e-5)
+LONG_TOL = {"u": 5e-6, "v": 5e-5, "w": 5e-5, "rho-rho0": 3e-4}
+
+
+def test_fp32_sphere_channel_2000_steps(plfbs_lib):
+    """The 128 x 64 x 64 channel with its 3,217-node sphere (the benchmarked
+    configuration), 2,000 steps from the bench's uniform start in both
+    precisions: the FP32 deviation form against the FP64 path (itself held to
+    the reference's CUDA path at 1e-10 in test_gpu_bench_configs.py), per
+    field, and the sphere's drag and lift."""
+    import bench
+    w, steps = bench.SPHERE, 2000
+    pm, c, ma, nodes, s0 = bench.build_channel(w)
+    rt, vt, val = cases.bc_arrays(ma, c)
+    area = np.pi * w.diam ** 2 / 4
+    out = {}
+    for prec in (capi.FP64, capi.FP32_DEVIATION):
+        s = capi.Solver(ma, rt, vt, val, bench.solver_cfg(c, prec), ibm=bench.ibm_cfg(w, nodes))
+        s.set_state(s0)
+        st, _ = s.run(steps, history=False)
+        assert st["rc"] == 0 and st["steps_done"] == steps
+        out[prec] = (s.get_state(), s.body_force(area))
+        s.close()
+    (q64, (cd64, cl64)), (q32, (cd32, cl32)) = out[capi.FP64], out[capi.FP32_DEVIATION]
+    errs = _field_errors(q32[: ma.n_cells], q64[: ma.n_cells])
+    cd_err = abs(cd32 - cd64) / abs(cd64)
+    print("fp32 vs fp64, 128x64x64 channel, %d steps: %s; Cd %.6f vs %.6f (%.1e), Cl %.2e vs %.2e"
+          % (steps, errs, cd32, cd64, cd_err, cl32, cl64))
+    assert all(errs[k] < LONG_TOL[k] for k in LONG_TOL), errs
+    assert cd_err < 1e-4
