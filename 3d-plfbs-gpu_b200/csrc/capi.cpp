@@ -44,6 +44,10 @@ cudaMemPool_t g_pools[plfbs::kMaxDevices] = {};
 // returns the buffer here and only plfbs_release_cached frees them.
 std::vector<DevStats*> g_pinned_stats;
 
+// Page-locked staging buffers for the host-built layout arrays of
+// plfbs_create, recycled the same way (size in bytes beside each).
+std::vector<std::pair<void*, size_t>> g_pinned_staging;
+
 }  // namespace
 
 namespace plfbs_capi {
@@ -134,6 +138,39 @@ DevStats* take_pinned_stats() {
 void give_pinned_stats(DevStats* p) {
   std::lock_guard<std::mutex> g(g_pool_mutex);
   g_pinned_stats.push_back(p);
+}
+
+// A recycled page-locked buffer of at least `bytes` (the smallest that fits),
+// else a new one rounded up to 16 MiB; null when none can be had.
+void* take_pinned_staging(size_t bytes, size_t* got) {
+  {
+    std::lock_guard<std::mutex> g(g_pool_mutex);
+    size_t best = g_pinned_staging.size();
+    for (size_t k = 0; k < g_pinned_staging.size(); k++)
+      if (g_pinned_staging[k].second >= bytes &&
+          (best == g_pinned_staging.size() ||
+           g_pinned_staging[k].second < g_pinned_staging[best].second))
+        best = k;
+    if (best < g_pinned_staging.size()) {
+      const auto b = g_pinned_staging[best];
+      g_pinned_staging.erase(g_pinned_staging.begin() + best);
+      *got = b.second;
+      return b.first;
+    }
+  }
+  const size_t n = (bytes + (16u << 20) - 1) / (16u << 20) * (16u << 20);
+  void* p = nullptr;
+  if (cudaMallocHost(&p, n) != cudaSuccess) {
+    cudaGetLastError();  // a failed page-lock leaves the pageable path, not an error
+    return nullptr;
+  }
+  *got = n;
+  return p;
+}
+
+void give_pinned_staging(void* p, size_t n) {
+  std::lock_guard<std::mutex> g(g_pool_mutex);
+  g_pinned_staging.emplace_back(p, n);
 }
 
 
@@ -305,6 +342,57 @@ int check_ctx(plfbs_ctx* ctx) {
 
 }  // namespace
 
+namespace plfbs_capi {
+
+int prestage_layout(plfbs_ctx* ctx) {
+  const plfbs::Layout& L = ctx->L;
+  const size_t C = (size_t)L.C, B = (size_t)L.B;
+  if (C == 0 || L.cell_new_of_old.size() != C || L.bc_new_of_old.size() != B ||
+      L.bc_old_of_new.size() != B || L.bc0.size() != 4 * B || L.bc1.size() != 4 * B ||
+      L.bc2.size() != 4 * B || L.bc3.size() != 4 * B)
+    return PLFBS_OK;  // not built yet (or not at all): the later uploads run
+  const bool fp32 = ctx->cfg.precision == PLFBS_FP32_DEVIATION;
+  plfbs::BoundaryRecords32 b32;
+  if (fp32) plfbs::boundary_records32(L, ctx->cfg.ref_rho, ctx->cfg.max_velocity, b32);
+  const void* src[7] = {L.cell_new_of_old.data(), L.bc_new_of_old.data(), L.bc_old_of_new.data(),
+                        fp32 ? (const void*)b32.bc0.data() : L.bc0.data(),
+                        fp32 ? (const void*)b32.bc1.data() : L.bc1.data(),
+                        fp32 ? (const void*)b32.bc2.data() : L.bc2.data(),
+                        fp32 ? (const void*)b32.bc3.data() : L.bc3.data()};
+  const size_t rec = 4 * B * (fp32 ? sizeof(float) : sizeof(double));
+  const size_t len[7] = {4 * C, 4 * B, 4 * B, rec, rec, rec, rec};
+  size_t off[8] = {0};
+  for (int k = 0; k < 7; k++) off[k + 1] = off[k] + (len[k] + 255) / 256 * 256;
+  size_t got = 0;
+  void* host = take_pinned_staging(off[7], &got);
+  if (!host) return PLFBS_OK;
+  ctx->staging = host;
+  ctx->staging_bytes = got;
+  const void* dev[7];
+  for (int k = 0; k < 7; k++) {
+    unsigned char* h = static_cast<unsigned char*>(host) + off[k];
+    if (len[k]) std::memcpy(h, src[k], len[k]);
+    void* d = nullptr;
+    TRY(pool_alloc(ctx, &d, std::max<size_t>(len[k], 16)));
+    if (len[k]) CK(cudaMemcpyAsync(d, h, len[k], cudaMemcpyHostToDevice, ctx->stream));
+    dev[k] = d;
+  }
+  ctx->pre.cell_new = dev[0];
+  ctx->pre.bc_new = dev[1];
+  ctx->pre.bc_old = dev[2];
+  for (int k = 0; k < 4; k++) ctx->pre.bc[k] = dev[3 + k];
+  return PLFBS_OK;
+}
+
+void release_staging(plfbs_ctx* ctx) {
+  if (!ctx->staging) return;
+  give_pinned_staging(ctx->staging, ctx->staging_bytes);
+  ctx->staging = nullptr;
+  ctx->staging_bytes = 0;
+}
+
+}  // namespace plfbs_capi
+
 void plfbs::set_global_error(const std::string& m) { g_err = m; }
 
 extern "C" {
@@ -408,6 +496,9 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     if (scanned && cfg->renumber != 1) {
       rc = plfbs::prepare_layout(*cfg, *mesh, *bc, ctx->L, err, nullptr,
                                  [&](plfbs::MeshScan& out) -> int {
+                                   // the host would wait for the copies: the
+                                   // arrays it has built go up behind them
+                                   if (prestage_layout(ctx)) return PLFBS_ERR_CUDA;
                                    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
                                      return PLFBS_ERR_CUDA;
                                    out = *scan;
@@ -518,7 +609,12 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
     NvtxRange r("compact layout");
     if ((rc = build_compact_layout(ctx))) return fail(rc);
   }
-  if (fp32) {
+  if (ctx->pre.bc[0]) {  // copied while the mesh copies ran
+    a.bc0 = ctx->pre.bc[0];
+    a.bc1 = ctx->pre.bc[1];
+    a.bc2 = ctx->pre.bc[2];
+    a.bc3 = ctx->pre.bc[3];
+  } else if (fp32) {
     plfbs::BoundaryRecords32 b32;
     plfbs::boundary_records32(L, cfg->ref_rho, cfg->max_velocity, b32);
     if ((rc = dev_upload(ctx, &p, b32.bc0))) return fail(rc);
@@ -605,6 +701,7 @@ int plfbs_create(const plfbs_config* cfg, const plfbs_mesh_view* mesh, const plf
   // capture with an error
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
     return fail(set_err(ctx, PLFBS_ERR_CUDA, "setup failed"));
+  release_staging(ctx);  // the copies from it have ended
   *out = ctx;
   return PLFBS_OK;
 }
@@ -613,6 +710,7 @@ void plfbs_destroy(plfbs_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  release_staging(ctx);
   if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
   if (ctx->stream) free_stage(ctx);
   for (void* p : ctx->allocs) cudaFreeAsync(p, ctx->stream);
@@ -687,11 +785,14 @@ int plfbs_release_cached(int32_t device) {
     pool = g_pools[device];
   }
   std::vector<DevStats*> pinned;
+  std::vector<std::pair<void*, size_t>> staging;
   {
     std::lock_guard<std::mutex> g(g_pool_mutex);
     pinned.swap(g_pinned_stats);
+    staging.swap(g_pinned_staging);
   }
   for (DevStats* p : pinned) cudaFreeHost(p);
+  for (auto& b : staging) cudaFreeHost(b.first);
   if (!pool) return PLFBS_OK;
   cudaError_t e = cudaMemPoolTrimTo(pool, 0);
   if (e != cudaSuccess)

@@ -44,6 +44,19 @@ struct plfbs_ctx {
   // normal, fcen [3F], vol [C], ccen [3(C+B)] double; the stencil offsets
   // [C+1], cells and faces [nnz] int (with `stencil` set). Freed once the
   // layout is built.
+  // Host-built layout arrays copied to the device from a page-locked staging
+  // buffer while plfbs_create waits for the mesh copies (prestage_layout):
+  // the caller-to-device cell map [C], the boundary orders [B] (int32) and
+  // the boundary records [B] (FP64 double4, FP32 float4); null where they go
+  // up later from pageable memory instead.
+  struct Prestaged {
+    const void* cell_new = nullptr;
+    const void* bc_new = nullptr;
+    const void* bc_old = nullptr;
+    const void* bc[4] = {nullptr, nullptr, nullptr, nullptr};
+  } pre;
+  void* staging = nullptr;  // the page-locked buffer, held until plfbs_create ends
+  size_t staging_bytes = 0;
   struct MeshStage {
     bool ok = false, stencil = false;
     const int32_t* owner = nullptr;
@@ -100,6 +113,12 @@ int stage_mesh(plfbs_ctx* ctx, const plfbs_mesh_view& m);
 // has reached it). *launched false: nothing staged to check, the host scans
 // instead.
 int scan_mesh(plfbs_ctx* ctx, plfbs::MeshScan* out, bool* launched);
+// Copies the host-built layout arrays to the device through page-locked
+// staging (ctx->pre); leaves ctx->pre empty when they are not all built yet
+// or no staging buffer can be had. Returns the staging buffer with
+// release_staging once the stream has passed the copies.
+int prestage_layout(plfbs_ctx* ctx);
+void release_staging(plfbs_ctx* ctx);
 void free_stage(plfbs_ctx* ctx);
 int build_compact_layout(plfbs_ctx* ctx);
 

@@ -173,11 +173,17 @@ int build_device_layout(plfbs_ctx* ctx, const plfbs_mesh_view& m) {
     TRY(S.upload(&d.st_cells, m.stencil_cells, nnz));
     TRY(S.upload(&d.st_faces, m.stencil_faces, nnz));
   }
-  TRY(S.upload(&d.bc_new, L.bc_new_of_old.data(), B));
-  TRY(S.upload(&d.bc_old, L.bc_old_of_new.data(), B));
   void* p = nullptr;
-  TRY(dev_upload(ctx, &p, L.cell_new_of_old));  // kept: the IBM kernels map caller cells with it
-  d.cell_new = static_cast<const int32_t*>(p);
+  if (ctx->pre.cell_new) {  // copied while the mesh copies ran
+    d.bc_new = static_cast<const int32_t*>(ctx->pre.bc_new);
+    d.bc_old = static_cast<const int32_t*>(ctx->pre.bc_old);
+    d.cell_new = static_cast<const int32_t*>(ctx->pre.cell_new);
+  } else {
+    TRY(S.upload(&d.bc_new, L.bc_new_of_old.data(), B));
+    TRY(S.upload(&d.bc_old, L.bc_old_of_new.data(), B));
+    TRY(dev_upload(ctx, &p, L.cell_new_of_old));  // kept: the IBM kernels map caller cells with it
+    d.cell_new = static_cast<const int32_t*>(p);
+  }
   // caller index -> device index, cells then ghosts (state transfer)
   TRY(pool_alloc(ctx, &p, 4 * T));
   ctx->perm = static_cast<int32_t*>(p);

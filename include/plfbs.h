@@ -397,8 +397,9 @@ const char* plfbs_last_error(const plfbs_ctx* ctx);  /* ctx may be NULL: this th
 void plfbs_destroy(plfbs_ctx* ctx);
 
 /* Returns the memory cached in this library's pool for `device` to the driver
- * (contexts still alive keep theirs), and frees the pinned host status
- * buffers destroyed contexts left for reuse. No counterpart in the reference.
+ * (contexts still alive keep theirs), and frees the pinned host status and
+ * staging buffers destroyed contexts left for reuse. No counterpart in the
+ * reference.
  * Errors are reported through plfbs_last_error(NULL). */
 int plfbs_release_cached(int32_t device);
 
